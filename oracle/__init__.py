@@ -1,0 +1,361 @@
+"""Python access to the CPU oracle (TEST INFRASTRUCTURE ONLY).
+
+Two libraries, both built by ``oracle/Makefile``:
+
+* ``restatement`` -- ``_lib/liboracle.so``, the plain-C restatement of the
+  reference's FP64 path (oracle.c). Always available once built.
+* ``reference`` -- ``_ref/libref_orrery.so``, the reference's own CPU sources
+  compiled where they lie, behind a small C shim (ref_shim.cpp). Present only
+  where it was built (it travels with the repository snapshot as a built file).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package. The product never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT_PATH = os.path.join(HERE, "_lib", "liboracle.so")
+REFERENCE_PATH = os.path.join(HERE, "_ref", "libref_orrery.so")
+
+_dp = C.POINTER(C.c_double)
+_u64p = C.POINTER(C.c_uint64)
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp)
+
+
+def _u(a):
+    return a.ctypes.data_as(_u64p)
+
+
+def build(reference_root: str | None = None, with_reference: bool = True) -> None:
+    """Compile the restatement (and the reference library when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    root = reference_root or os.environ.get("ORRERY_REFERENCE_ROOT", "/root/reference")
+    if with_reference and os.path.isdir(os.path.join(root, "src", "solvers")):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={root}"], check=True)
+
+
+class Counts(C.Structure):
+    _fields_ = [("evaluations", C.c_uint64), ("particle_particle", C.c_uint64),
+                ("particle_cell", C.c_uint64)]
+
+
+class _Node(C.Structure):
+    _fields_ = [("mass", C.c_double), ("com_x", C.c_double), ("com_y", C.c_double),
+                ("com_z", C.c_double), ("acceptance_radius_squared", C.c_double),
+                ("next", C.c_uint64), ("first_particle", C.c_uint64),
+                ("particle_count", C.c_uint64)]
+
+
+class _Tree(C.Structure):
+    _fields_ = [("nodes", C.POINTER(_Node)), ("quadrupoles", C.POINTER(C.c_double)),
+                ("node_count", C.c_size_t), ("capacity", C.c_size_t),
+                ("leaf_count", C.c_size_t), ("depth", C.c_uint),
+                ("opening_angle", C.c_double), ("leaf_capacity", C.c_uint64)]
+
+
+class Tree:
+    """An octree as arrays: reals (n, 5) = mass, com xyz, r2; idx (n, 3) = next, first, count."""
+
+    def __init__(self, reals, idx, quads, leaf_count, depth):
+        self.reals = reals
+        self.idx = idx
+        self.quads = quads
+        self.leaf_count = int(leaf_count)
+        self.depth = int(depth)
+
+    @property
+    def node_count(self) -> int:
+        return int(self.reals.shape[0])
+
+
+class Restatement:
+    """ctypes binding of oracle.c."""
+
+    def __init__(self, path: str = RESTATEMENT_PATH):
+        if not os.path.exists(path):
+            build(with_reference=False)
+        lib = C.CDLL(path)
+        self.lib = lib
+        lib.oc_direct.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, _dp, _dp, _dp,
+                                  C.POINTER(Counts)]
+        lib.oc_reference_acceleration.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_size_t,
+                                                  C.c_double, _dp]
+        lib.oc_bounding_cube.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, _dp]
+        lib.oc_spread_bits.argtypes = [C.c_uint32]
+        lib.oc_spread_bits.restype = C.c_uint64
+        lib.oc_morton_code_grid.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
+        lib.oc_morton_code_grid.restype = C.c_uint64
+        lib.oc_morton_code.argtypes = [C.c_double, C.c_double, C.c_double, _dp, C.c_double]
+        lib.oc_morton_code.restype = C.c_uint64
+        lib.oc_morton_octant.argtypes = [C.c_uint64, C.c_uint]
+        lib.oc_morton_octant.restype = C.c_uint
+        lib.oc_morton_order.argtypes = [C.c_size_t, _dp, _dp, _dp, _u64p, _u64p, _dp, _dp]
+        lib.oc_tree_build.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, _u64p, _dp, C.c_double,
+                                      C.c_double, C.c_uint64, C.c_int, C.POINTER(_Tree)]
+        lib.oc_tree_free.argtypes = [C.POINTER(_Tree)]
+        lib.oc_barnes_hut.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                                      C.c_uint64, C.c_int, _dp, _dp, _dp, C.POINTER(Counts)]
+        for name in ("oc_vv_step_direct", "oc_yoshida_step_direct"):
+            getattr(lib, name).argtypes = [C.c_size_t] + [_dp] * 10 + [C.c_double, C.c_double,
+                                                                       C.POINTER(Counts)]
+        lib.oc_yoshida_weights.argtypes = [_dp, _dp]
+        lib.oc_kinetic_energy.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp]
+        lib.oc_kinetic_energy.restype = C.c_double
+        lib.oc_potential_energy.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double]
+        lib.oc_potential_energy.restype = C.c_double
+
+    # -- direct --------------------------------------------------------------
+    def direct(self, x, y, z, m, softening):
+        n = len(m)
+        a = [np.zeros(n) for _ in range(3)]
+        counts = Counts()
+        self.lib.oc_direct(n, _d(x), _d(y), _d(z), _d(m), softening, _d(a[0]), _d(a[1]),
+                           _d(a[2]), C.byref(counts))
+        return np.stack(a, axis=1), counts
+
+    def reference_acceleration(self, x, y, z, m, target, softening):
+        out = np.zeros(3)
+        self.lib.oc_reference_acceleration(len(m), _d(x), _d(y), _d(z), _d(m), target, softening,
+                                           _d(out))
+        return out
+
+    def reference_accelerations(self, x, y, z, m, softening, targets=None):
+        targets = range(len(m)) if targets is None else targets
+        return np.array([self.reference_acceleration(x, y, z, m, int(t), softening)
+                         for t in targets]).reshape(-1, 3)
+
+    # -- Morton --------------------------------------------------------------
+    def bounding_cube(self, x, y, z):
+        origin = np.zeros(3)
+        size = C.c_double()
+        self.lib.oc_bounding_cube(len(x), _d(x), _d(y), _d(z), _d(origin), C.byref(size))
+        return origin, size.value
+
+    def spread_bits(self, v):
+        return self.lib.oc_spread_bits(v)
+
+    def morton_code_grid(self, gx, gy, gz):
+        return self.lib.oc_morton_code_grid(gx, gy, gz)
+
+    def morton_code(self, p, origin, size):
+        origin = np.ascontiguousarray(origin, dtype=np.float64)
+        return self.lib.oc_morton_code(p[0], p[1], p[2], _d(origin), size)
+
+    def morton_octant(self, code, level):
+        return self.lib.oc_morton_octant(code, level)
+
+    def morton_order(self, x, y, z):
+        n = len(x)
+        codes = np.zeros(n, np.uint64)
+        idx = np.zeros(n, np.uint64)
+        origin = np.zeros(3)
+        size = C.c_double()
+        self.lib.oc_morton_order(n, _d(x), _d(y), _d(z), _u(codes), _u(idx), _d(origin),
+                                 C.byref(size))
+        return codes, idx, origin, size.value
+
+    # -- tree ----------------------------------------------------------------
+    def tree(self, x, y, z, m, opening_angle=0.5, leaf_capacity=32, quadrupole=False):
+        """Morton-order the particles and build the octree; returns (Tree, codes, idx)."""
+        codes, idx, origin, size = self.morton_order(x, y, z)
+        ii = idx.astype(np.int64)
+        sx, sy, sz, sm = (np.ascontiguousarray(a[ii]) for a in (x, y, z, m))
+        t = _Tree()
+        rc = self.lib.oc_tree_build(len(m), _d(sx), _d(sy), _d(sz), _d(sm), _u(codes),
+                                    _d(origin), size, opening_angle, leaf_capacity,
+                                    1 if quadrupole else 0, C.byref(t))
+        if rc != 0:
+            raise MemoryError("oracle tree build failed")
+        n = t.node_count
+        reals = np.zeros((n, 5))
+        ind = np.zeros((n, 3), np.uint64)
+        quads = np.zeros((n, 6)) if quadrupole else None
+        if n:
+            nodes = np.ctypeslib.as_array(C.cast(t.nodes, C.POINTER(C.c_uint8)),
+                                          shape=(n * C.sizeof(_Node),))
+            rec = np.frombuffer(nodes.tobytes(), dtype=np.dtype([
+                ("r", np.float64, 5), ("i", np.uint64, 3)]))
+            reals[:] = rec["r"]
+            ind[:] = rec["i"]
+            if quadrupole:
+                quads[:] = np.ctypeslib.as_array(t.quadrupoles, shape=(n * 6,)).reshape(n, 6)
+        tree = Tree(reals, ind, quads, t.leaf_count, t.depth)
+        self.lib.oc_tree_free(C.byref(t))
+        return tree, codes, idx
+
+    def barnes_hut(self, x, y, z, m, softening, opening_angle=0.5, leaf_capacity=32,
+                   quadrupole=False):
+        n = len(m)
+        a = [np.zeros(n) for _ in range(3)]
+        counts = Counts()
+        rc = self.lib.oc_barnes_hut(n, _d(x), _d(y), _d(z), _d(m), softening, opening_angle,
+                                    leaf_capacity, 1 if quadrupole else 0, _d(a[0]), _d(a[1]),
+                                    _d(a[2]), C.byref(counts))
+        if rc != 0:
+            raise MemoryError("oracle Barnes-Hut failed")
+        return np.stack(a, axis=1), counts
+
+    # -- integrators and energies -------------------------------------------
+    def integrate_direct(self, state, m, softening, dt, steps, integrator="vv"):
+        """Advance ``state`` (dict of x y z vx vy vz ax ay az arrays, copied) in place."""
+        s = {k: np.ascontiguousarray(v, dtype=np.float64).copy() for k, v in state.items()}
+        fn = self.lib.oc_yoshida_step_direct if integrator == "yoshida4" else \
+            self.lib.oc_vv_step_direct
+        counts = Counts()
+        for _ in range(steps):
+            fn(len(m), *(_d(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")),
+               _d(m), softening, dt, C.byref(counts))
+        return s, counts
+
+    def yoshida_weights(self):
+        a, b = C.c_double(), C.c_double()
+        self.lib.oc_yoshida_weights(C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def kinetic_energy(self, vx, vy, vz, m):
+        return self.lib.oc_kinetic_energy(len(m), _d(vx), _d(vy), _d(vz), _d(m))
+
+    def potential_energy(self, x, y, z, m, softening):
+        return self.lib.oc_potential_energy(len(m), _d(x), _d(y), _d(z), _d(m), softening)
+
+
+class Reference:
+    """ctypes binding of the reference's own CPU code (libref_orrery.so)."""
+
+    def __init__(self, path: str = REFERENCE_PATH):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        lib = C.CDLL(path)
+        self.lib = lib
+        lib.ref_default_worker_count.restype = C.c_uint
+        lib.ref_plummer.argtypes = [C.c_size_t, C.c_double, C.c_double, C.c_uint64] + [_dp] * 7
+        lib.ref_direct.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, C.c_int, C.c_int,
+                                   _dp, _dp, _dp, _u64p]
+        lib.ref_direct_timed.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, C.c_int,
+                                         C.c_int, C.c_int, _dp]
+        lib.ref_reference_acceleration.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_size_t,
+                                                   C.c_double, _dp]
+        lib.ref_morton.argtypes = [C.c_size_t, _dp, _dp, _dp, C.c_int, _u64p, _u64p, _dp, _dp]
+        lib.ref_spread_bits.argtypes = [C.c_uint32]
+        lib.ref_spread_bits.restype = C.c_uint64
+        lib.ref_morton_code_grid.argtypes = [C.c_uint32] * 3
+        lib.ref_morton_code_grid.restype = C.c_uint64
+        lib.ref_barnes_hut.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
+                                       C.c_uint64, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp,
+                                       _u64p, C.POINTER(C.c_void_p)]
+        lib.ref_barnes_hut_timed.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double,
+                                             C.c_double, C.c_uint64, C.c_int, C.c_int, C.c_int,
+                                             _dp]
+        lib.ref_tree_node_count.argtypes = [C.c_void_p]
+        lib.ref_tree_node_count.restype = C.c_size_t
+        lib.ref_tree_leaf_count.argtypes = [C.c_void_p]
+        lib.ref_tree_leaf_count.restype = C.c_size_t
+        lib.ref_tree_depth.argtypes = [C.c_void_p]
+        lib.ref_tree_depth.restype = C.c_uint
+        lib.ref_tree_copy.argtypes = [C.c_void_p, _dp, _u64p, _dp]
+        lib.ref_tree_free.argtypes = [C.c_void_p]
+        lib.ref_integrate_direct.argtypes = [C.c_size_t] + [_dp] * 10 + [
+            C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int]
+        lib.ref_potential_energy.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double]
+        lib.ref_potential_energy.restype = C.c_double
+        lib.ref_kinetic_energy.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp]
+        lib.ref_kinetic_energy.restype = C.c_double
+
+    @staticmethod
+    def available(path: str = REFERENCE_PATH) -> bool:
+        return os.path.exists(path)
+
+    def worker_count(self) -> int:
+        return int(self.lib.ref_default_worker_count())
+
+    def plummer(self, count, total_mass=1.0, scale_radius=1.0, seed=20260811):
+        arrs = [np.zeros(count) for _ in range(7)]
+        rc = self.lib.ref_plummer(count, total_mass, scale_radius, seed, *(_d(a) for a in arrs))
+        if rc != 0:
+            raise RuntimeError("reference Plummer sampler failed")
+        return dict(zip(("x", "y", "z", "vx", "vy", "vz", "m"), arrs))
+
+    def direct(self, x, y, z, m, softening, kernel="scalar", threads=1):
+        n = len(m)
+        a = [np.zeros(n) for _ in range(3)]
+        pairs = np.zeros(1, np.uint64)
+        self.lib.ref_direct(n, _d(x), _d(y), _d(z), _d(m), softening,
+                            1 if kernel == "avx2" else 0, threads, _d(a[0]), _d(a[1]), _d(a[2]),
+                            _u(pairs))
+        return np.stack(a, axis=1), int(pairs[0])
+
+    def direct_seconds(self, x, y, z, m, softening, threads, repeats=1, kernel="avx2"):
+        s = C.c_double()
+        self.lib.ref_direct_timed(len(m), _d(x), _d(y), _d(z), _d(m), softening,
+                                  1 if kernel == "avx2" else 0, threads, repeats, C.byref(s))
+        return s.value
+
+    def reference_acceleration(self, x, y, z, m, target, softening):
+        out = np.zeros(3)
+        self.lib.ref_reference_acceleration(len(m), _d(x), _d(y), _d(z), _d(m), target,
+                                            softening, _d(out))
+        return out
+
+    def morton(self, x, y, z, threads=1):
+        n = len(x)
+        codes = np.zeros(n, np.uint64)
+        idx = np.zeros(n, np.uint64)
+        origin = np.zeros(3)
+        size = np.zeros(1)
+        self.lib.ref_morton(n, _d(x), _d(y), _d(z), threads, _u(codes), _u(idx), _d(origin),
+                            _d(size))
+        return codes, idx, origin, float(size[0])
+
+    def barnes_hut(self, x, y, z, m, softening, opening_angle=0.5, leaf_capacity=32,
+                   quadrupole=False, kernel="scalar", threads=1, with_tree=True):
+        n = len(m)
+        a = [np.zeros(n) for _ in range(3)]
+        counts = np.zeros(3, np.uint64)
+        handle = C.c_void_p()
+        self.lib.ref_barnes_hut(n, _d(x), _d(y), _d(z), _d(m), softening, opening_angle,
+                                leaf_capacity, 1 if quadrupole else 0,
+                                1 if kernel == "avx2" else 0, threads, _d(a[0]), _d(a[1]),
+                                _d(a[2]), _u(counts), C.byref(handle) if with_tree else None)
+        tree = None
+        if with_tree:
+            nn = self.lib.ref_tree_node_count(handle)
+            reals = np.zeros((nn, 5))
+            ind = np.zeros((nn, 3), np.uint64)
+            quads = np.zeros((nn, 6)) if quadrupole else None
+            self.lib.ref_tree_copy(handle, _d(reals), _u(ind),
+                                   _d(quads) if quadrupole else None)
+            tree = Tree(reals, ind, quads, self.lib.ref_tree_leaf_count(handle),
+                        self.lib.ref_tree_depth(handle))
+            self.lib.ref_tree_free(handle)
+        return np.stack(a, axis=1), counts, tree
+
+    def barnes_hut_seconds(self, x, y, z, m, softening, opening_angle, leaf_capacity, quadrupole,
+                           threads, repeats=1):
+        s = C.c_double()
+        self.lib.ref_barnes_hut_timed(len(m), _d(x), _d(y), _d(z), _d(m), softening,
+                                      opening_angle, leaf_capacity, 1 if quadrupole else 0,
+                                      threads, repeats, C.byref(s))
+        return s.value
+
+    def integrate_direct(self, state, m, softening, dt, steps, integrator="vv", kernel="scalar"):
+        s = {k: np.ascontiguousarray(v, dtype=np.float64).copy() for k, v in state.items()}
+        self.lib.ref_integrate_direct(
+            len(m), *(_d(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")),
+            _d(m), softening, dt, steps, 1 if integrator == "yoshida4" else 0,
+            1 if kernel == "avx2" else 0)
+        return s
+
+    def potential_energy(self, x, y, z, m, softening):
+        return self.lib.ref_potential_energy(len(m), _d(x), _d(y), _d(z), _d(m), softening)
+
+    def kinetic_energy(self, vx, vy, vz, m):
+        return self.lib.ref_kinetic_energy(len(m), _d(vx), _d(vy), _d(vz), _d(m))
