@@ -1,0 +1,456 @@
+"""Benchmark of the force-evaluation path on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload NAME]
+                    [--impl b200|reference]
+
+Workloads (seeded synthetic inputs with the shapes of the measured configs):
+  bh-collision-2m          two disc galaxies, 2,000,000 particles, Barnes-Hut
+                           theta 0.5 with quadrupoles, leaf 32, eps 0.02, FP32
+                           force / FP64 state, velocity Verlet dt 5e-4; a step
+                           is one VV step (Morton order, tree, walk, kicks).
+                           Metric: BH ms/step at 2M (lower is better).
+  direct-plummer-4096      Plummer sphere N=4096, eps 0.01, FP32 direct, VV
+                           dt 1e-3. Metric: direct Gint/s, N(N-1) per step.
+  direct-plummer-262144    the same at N=262,144 with the split-precision
+                           kernel and Yoshida-4 dt 1e-3 (3 evaluations/step).
+
+Timing: W untimed warm-up steps, then exactly K steps bracketed by a barrier
+and torch.cuda.synchronize() on both sides, timed with CUDA events on the
+stream the work runs on, max over ranks. One step is a replayed CUDA graph.
+Per-phase device times inside the timed region come from event nodes in the
+graph (DeviceSystem.profile). Under torchrun every rank runs an independent
+replica on its own GPU (the path has no exchange step: replicas only).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 1024 * 1024
+
+
+# ---------------------------------------------------------------------------
+# Workloads
+# ---------------------------------------------------------------------------
+
+WORKLOADS = {
+    "bh-collision-2m": dict(kind="tree", n=2_000_000, eps=0.02, dt=5e-4, integrator="vv",
+                            theta=0.5, leaf=32, quadrupole=True, precision="fp32",
+                            metric="BH ms/step at 2M", unit="ms/step", higher=False,
+                            generator="collision"),
+    "direct-plummer-4096": dict(kind="direct", n=4096, eps=0.01, dt=1e-3, integrator="vv",
+                                precision="fp32", metric="direct Gint/s", unit="Gint/s",
+                                higher=True, generator="plummer"),
+    "direct-plummer-262144": dict(kind="direct", n=262_144, eps=0.01, dt=1e-3,
+                                  integrator="yoshida4", precision="split",
+                                  metric="direct Gint/s", unit="Gint/s", higher=True,
+                                  generator="plummer"),
+}
+DEFAULT_WORKLOAD = "direct-plummer-4096"
+
+
+def make_inputs(w, seed=20260811):
+    from orrery_b200 import initial_conditions as ic
+
+    if w["generator"] == "plummer":
+        return ic.plummer_sphere(w["n"], seed=seed)
+    return ic.galaxy_collision(w["n"], softening=w["eps"], seed=seed)
+
+
+def evaluations_per_step(w):
+    return 3 if w["integrator"] == "yoshida4" else 1
+
+
+def step_units(w):
+    """Units of the metric one step processes (interactions, or one step)."""
+    if w["kind"] == "direct":
+        return evaluations_per_step(w) * w["n"] * (w["n"] - 1)
+    return 1
+
+
+# ---------------------------------------------------------------------------
+# Clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    """nvidia-smi sampling every 200 ms while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device = device_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        rows = []
+        if self.path and os.path.exists(self.path):
+            with open(self.path) as fh:
+                for line in fh:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4)
+                          if r[5 + k].lower().startswith("active")})
+        load = [v for v in sm if mx and v > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(load) if load else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# Distributed plumbing
+# ---------------------------------------------------------------------------
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    import datetime
+
+    import torch.distributed as dist
+
+    if world > 1 and not dist.is_initialized():
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist if world > 1 else None
+
+
+def reduce_max(dist, value, device):
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's own CPU solvers on this host's cores
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(w, data, budget_s=20.0):
+    """Times the reference's CPU implementation (oracle/_ref) on a bounded
+    sample of the workload; returns the cpu_baseline object."""
+    import oracle
+
+    if not oracle.Reference.available():
+        r = oracle.Restatement()
+        kind = "port"
+        cores = 1
+        n = min(w["n"], 2048)
+        sub = {k: np.ascontiguousarray(v[:n]) for k, v in data.items()}
+        t0 = time.perf_counter()
+        if w["kind"] == "direct":
+            r.direct(sub["x"], sub["y"], sub["z"], sub["m"], w["eps"])
+            sec = time.perf_counter() - t0
+            value = n * (n - 1) / sec / 1e9
+            return dict(value=value, unit="Gint/s", cores=cores, kind=kind,
+                        sample=f"one scalar direct evaluation of {n} particles")
+        r.barnes_hut(sub["x"], sub["y"], sub["z"], sub["m"], w["eps"], w["theta"], w["leaf"],
+                     w["quadrupole"])
+        sec = time.perf_counter() - t0
+        return dict(value=sec * 1e3, unit="ms/step", cores=cores, kind=kind,
+                    sample=f"one scalar Barnes-Hut evaluation of {n} particles (not 2M)")
+    ref = oracle.Reference()
+    threads = ref.worker_count()
+    x, y, z, m = (np.ascontiguousarray(data[k]) for k in ("x", "y", "z", "m"))
+    if w["kind"] == "direct":
+        n = len(m)
+        # One evaluation first to size the sample to the budget.
+        one = ref.direct_seconds(x, y, z, m, w["eps"], threads, repeats=1)
+        reps = max(1, min(int(budget_s / max(one, 1e-6)),
+                          100 * evaluations_per_step(w)))
+        sec = ref.direct_seconds(x, y, z, m, w["eps"], threads, repeats=reps)
+        value = n * (n - 1) / sec / 1e9
+        return dict(value=value, unit="Gint/s", cores=threads, kind="reference",
+                    sample=f"{reps} DirectSolver evaluations (AVX2, {threads} threads) "
+                           f"of the full {n}-particle input")
+    sec = ref.barnes_hut_seconds(x, y, z, m, w["eps"], w["theta"], w["leaf"], w["quadrupole"],
+                                 threads, repeats=1)
+    return dict(value=sec * 1e3 * evaluations_per_step(w), unit="ms/step", cores=threads,
+                kind="reference",
+                sample=f"one BarnesHutSolver evaluation (AVX2 leaves, {threads} threads) of the "
+                       f"full {len(m)}-particle input = one VV step's force evaluation")
+
+
+def run_reference(args, w):
+    world, rank, local = dist_env()
+    dist = init_dist(world, "gloo")
+    if rank != 0:
+        barrier(dist)
+        return
+    data = make_inputs(w)
+    steps = max(1, args.steps)
+    base = cpu_baseline(w, data, budget_s=min(60.0, 10.0 * steps))
+    value = base["value"]
+    ms_per_step = value if w["unit"] == "ms/step" else \
+        step_units(w) / (value * 1e9) * 1e3
+    line = {
+        "impl": "reference", "metric": w["metric"], "value": value, "unit": w["unit"],
+        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": w["higher"], "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_of(args, w), "cpu_baseline": base,
+        "e2e": {"value": value, "unit": w["unit"], "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    barrier(dist)
+
+
+def config_of(args, w):
+    c = {"workload": args.workload, "n": w["n"], "solver": w["kind"],
+         "precision": w["precision"], "softening": w["eps"], "dt": w["dt"],
+         "integrator": w["integrator"], "replicas": args.gpus,
+         "l2": "inputs larger than L2" if w["n"] * 80 > L2_BYTES else
+               "L2 flushed between timed steps"}
+    if w["kind"] == "tree":
+        c.update(theta=w["theta"], leaf_capacity=w["leaf"], quadrupole=w["quadrupole"],
+                 morton_bits=63)
+    return c
+
+
+# ---------------------------------------------------------------------------
+# The B200 arm
+# ---------------------------------------------------------------------------
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as fh:
+            p = json.load(fh)
+        return p.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+def e2e_drop_in(ob, w, data, steps, torch):
+    """The drop-in path: the reference's host integrator arithmetic on FP64
+    arrays in pinned host memory, with the B200 solver's host-buffer evaluate
+    (H2D positions + masses, device pipeline, D2H accelerations) per step."""
+    n = w["n"]
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    x, y, z, m = (pin(data[k]) for k in ("x", "y", "z", "m"))
+    vx, vy, vz = (pin(data[k]) for k in ("vx", "vy", "vz"))
+    ax, ay, az = (pin(np.zeros(n)) for _ in range(3))
+    if w["kind"] == "direct":
+        solver = ob.B200DirectSolver(w["eps"], w["precision"])
+    else:
+        solver = ob.B200TreeSolver(w["eps"], w["theta"], w["leaf"], w["quadrupole"])
+    solver.evaluate((x, y, z), m, (ax, ay, az))
+    weights = [w["dt"]]
+    if w["integrator"] == "yoshida4":
+        c = 1.2599210498948731647672106
+        outer, inner = 1.0 / (2.0 - c), -c / (2.0 - c)
+        weights = [outer * w["dt"], inner * w["dt"], outer * w["dt"]]
+
+    def step():
+        for h in weights:
+            half = h / 2.0
+            for v, a in ((vx, ax), (vy, ay), (vz, az)):
+                v += half * a
+            for p, v in ((x, vx), (y, vy), (z, vz)):
+                p += h * v
+            solver.evaluate((x, y, z), m, (ax, ay, az))
+            for v, a in ((vx, ax), (vy, ay), (vz, az)):
+                v += half * a
+
+    step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        step()
+    sec = (time.perf_counter() - t0) / steps
+    evals = len(weights)
+    return sec, evals * 4 * 8 * n, evals * 3 * 8 * n
+
+
+def run_b200(args, w):
+    import torch
+
+    import orrery_b200 as ob
+
+    world, rank, local = dist_env()
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ob.load_library()
+
+    data = make_inputs(w)
+    n = w["n"]
+    kind = ob.SOLVER_DIRECT if w["kind"] == "direct" else ob.SOLVER_TREE
+    system = ob.DeviceSystem(n, w["eps"], kind=kind, precision=w["precision"],
+                             opening_angle=w.get("theta", 0.5), leaf_capacity=w.get("leaf", 32),
+                             quadrupole=w.get("quadrupole", False))
+    system.set_state(data["x"], data["y"], data["z"], data["vx"], data["vy"], data["vz"],
+                     data["m"])
+    system.step(w["dt"], max(args.warmup, 3), w["integrator"])
+    kernels_per_step = system.step_kernels(w["dt"], w["integrator"])
+    stream = torch.cuda.ExternalStream(system.stream(), device=device)
+    flush = None
+    if n * 80 <= L2_BYTES:
+        flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
+
+    K = args.steps
+    system.profile(K)
+    sampler = ClockSampler(local)
+    barrier(dist)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    total_ms = 0.0
+    if flush is None:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        system.step_async(w["dt"], K, w["integrator"])
+        end.record(stream)
+        end.synchronize()
+        total_ms = start.elapsed_time(end)
+    else:
+        pairs = []
+        for _ in range(K):
+            with torch.cuda.stream(stream):
+                flush.add_(1.0)
+            s = torch.cuda.Event(enable_timing=True)
+            e = torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            system.step_async(w["dt"], 1, w["integrator"])
+            e.record(stream)
+            pairs.append((s, e))
+        pairs[-1][1].synchronize()
+        total_ms = sum(s.elapsed_time(e) for s, e in pairs)
+    system.synchronize()
+    torch.cuda.synchronize()
+    barrier(dist)
+    clocks = sampler.stop()
+    total_ms = reduce_max(dist, total_ms, device)
+    phases, evals = system.phase_times()
+
+    ms_per_step = total_ms / K
+    if w["unit"] == "ms/step":
+        value = ms_per_step / world  # whole-job time per 2M step across replicas
+    else:
+        value = step_units(w) * K * world / (total_ms * 1e-3) / 1e9
+
+    # Roofline of the dominant kernel (the force kernel: walk or direct sum).
+    kernel_ms = phases["traversal_ms"]
+    if w["kind"] == "direct":
+        ffma, rsq = ob.probe_fp32()
+        peak_gint = min(ffma / 13.0, rsq) / 1e9
+        achieved = n * (n - 1) / (kernel_ms * 1e-3) / 1e9
+        roofline = {"bound": "fp32-issue", "achieved": achieved, "peak": peak_gint,
+                    "unit": "Gint/s", "frac": achieved / peak_gint, "traffic": None,
+                    "peak_source": "measured FFMA lane rate / 13 issue slots per interaction "
+                                   f"(FFMA {ffma / 1e12:.2f} T lane-op/s, SFU rsqrt "
+                                   f"{rsq / 1e12:.2f} T/s) on this GPU",
+                    "kernel_ms": kernel_ms}
+    else:
+        hbm, src = load_peaks()
+        bytes_per_target = 16 + 24 + 12
+        achieved = bytes_per_target * n / (kernel_ms * 1e-3) / 1e9
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                    "frac": achieved / hbm, "traffic": None,
+                    "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
+                    "kernel_ms": kernel_ms}
+
+    line = None
+    if rank == 0:
+        e2e_steps = max(2, min(K, 10 if w["kind"] == "tree" else 50))
+        sec, h2d, d2h = e2e_drop_in(ob, w, data, e2e_steps, torch)
+        if w["unit"] == "ms/step":
+            e2e_value = sec * 1e3
+        else:
+            e2e_value = step_units(w) / sec / 1e9
+        base = cpu_baseline(w, data) if world == 1 else None
+        line = {
+            "metric": w["metric"], "value": value, "unit": w["unit"], "n_gpus": world,
+            "steps": K, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
+            "higher_is_better": w["higher"], "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "state_dtype": "f64", "data": "synthetic",
+            "config": config_of(args, w),
+            "phases_ms": {k: phases[k] for k in ("ordering_ms", "construction_ms",
+                                                  "traversal_ms")},
+            "profiled_evaluations": evals,
+            "roofline": roofline,
+            "e2e": {"value": e2e_value, "unit": w["unit"], "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "reference host integrator arithmetic + ob_solver_evaluate on "
+                            "pinned host buffers"},
+            "gpu_launches": kernels_per_step * K,
+            "clocks": clocks,
+        }
+        if base is not None:
+            line["cpu_baseline"] = base
+        print(json.dumps(line), flush=True)
+    barrier(dist)
+    del system
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        run_reference(args, w)
+    else:
+        run_b200(args, w)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,215 @@
+/*
+ * orrery_b200 -- B200 (sm_100a) force-evaluation backend for the Orrery N-body
+ * simulator, behind a plain C ABI.
+ *
+ * Conventions (the same ones the reference's kernel boundary uses:
+ * include/orrery/solvers/cuda_kernels.hpp:102-111 returns cudaError_t and never
+ * throws):
+ *   - every function returns an int status, OB_OK on success;
+ *   - ob_last_error() gives a message for the calling thread's last failure;
+ *   - handles are opaque; arrays are plain pointers plus a count;
+ *   - particle data is FP64 structure-of-arrays, like the reference's
+ *     ParticleData (include/orrery/core/particle_data.hpp:43-149);
+ *   - accelerations are written, never accumulated
+ *     (include/orrery/integrators/acceleration_field.hpp:56-58).
+ * No CUDA or torch type appears in a signature; streams are passed as void*.
+ */
+#ifndef ORRERY_B200_H
+#define ORRERY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define OB_OK 0
+#define OB_ERROR_INVALID_ARGUMENT 1
+#define OB_ERROR_NO_DEVICE 2      /* no usable sm_100 device: the try_create -> null case */
+#define OB_ERROR_OUT_OF_MEMORY 3
+#define OB_ERROR_CUDA 4           /* a CUDA runtime error; the message names it */
+#define OB_ERROR_TIMEOUT 5        /* a bounded device-side wait ran out */
+#define OB_ERROR_CAPACITY 6       /* a size or budget limit was exceeded */
+#define OB_ERROR_UNSUPPORTED 7
+
+/* Solver kinds: the reference's DirectSolver and BarnesHutSolver
+ * (include/orrery/solvers/direct_solver.hpp:107,
+ *  include/orrery/solvers/barnes_hut_solver.hpp:108). */
+#define OB_SOLVER_DIRECT 0
+#define OB_SOLVER_TREE 1
+
+/* Arithmetic of the pair interactions.
+ *   FP32  -- positions rounded to FP32, FP32 pair math (the plain kernel);
+ *   SPLIT -- FP32 pair math on hi/lo-split FP64 positions, Kahan-compensated
+ *            FP32 partials, FP64 tile accumulation (the precision form);
+ *   FP64  -- FP64 pair math in the reference's order: bit-identical to the
+ *            reference's scalar DirectSolver (direct solver only). */
+#define OB_PRECISION_FP32 0
+#define OB_PRECISION_SPLIT 1
+#define OB_PRECISION_FP64 2
+
+/* Integrators (src/integrators/velocity_verlet.cpp:59-72,
+ * src/integrators/yoshida4.cpp:45-59). */
+#define OB_INTEGRATOR_VV 0
+#define OB_INTEGRATOR_YOSHIDA4 1
+
+/* Solver parameters. Mirrors core::Softening (softening.hpp:50-60, the
+ * length; the square is used) and solvers::TreeParameters (octree.hpp:147-191;
+ * defaults theta 0.5, leaf 32, no quadrupole; corrected like
+ * corrected_parameters, octree.cpp:189-194). */
+typedef struct ob_solver_params {
+    int32_t kind;           /* OB_SOLVER_* */
+    int32_t precision;      /* OB_PRECISION_* */
+    double softening;       /* softening length epsilon (>= 0) */
+    double opening_angle;   /* theta, clamped to [0, 1] (tree only) */
+    uint64_t leaf_capacity; /* at least 1 (tree only) */
+    int32_t quadrupole;     /* nonzero: carry traceless quadrupoles (tree only) */
+    int32_t reserved;
+} ob_solver_params;
+
+/* solvers::InteractionCount (interaction_count.hpp:37-76). */
+typedef struct ob_counts {
+    uint64_t evaluations;
+    uint64_t particle_particle;
+    uint64_t particle_cell;
+} ob_counts;
+
+/* Device-timed phases of the last evaluation, in milliseconds (CUDA events);
+ * the counterpart of EvaluationTimings / CudaTreeTimings
+ * (barnes_hut_solver.hpp:92-105, cuda_tree_solver.hpp:81-117). */
+typedef struct ob_timings {
+    double transfer_in_ms;  /* host -> device copies (host entry points only) */
+    double ordering_ms;     /* cube, Morton encode, radix sort, gather */
+    double construction_ms; /* octree layout and moments */
+    double traversal_ms;    /* the force kernel (direct sum or walk) */
+    double transfer_out_ms; /* device -> host copies (host entry points only) */
+} ob_timings;
+
+/* Library information and errors. */
+const char *ob_version(void);
+const char *ob_last_error(void);
+int ob_device_count(int *count);
+
+/* ------------------------------------------------------------------------ */
+/* Solver: the ForceSolver drop-in                                           */
+/* ------------------------------------------------------------------------ */
+typedef struct ob_solver ob_solver;
+
+/* Replaces CudaDirectSolver::try_create / CudaTreeSolver::try_create
+ * (src/solvers/cuda_direct_solver.cpp:140-164, cuda_tree_solver.cpp:205-221):
+ * returns OB_ERROR_NO_DEVICE (and *out = NULL) when no usable device exists. */
+int ob_solver_create(const ob_solver_params *params, ob_solver **out);
+void ob_solver_destroy(ob_solver *solver);
+int ob_solver_get_params(const ob_solver *solver, ob_solver_params *params);
+
+/* Replaces ForceSolver::evaluate on host spans
+ * (include/orrery/integrators/acceleration_field.hpp:56-58): synchronous,
+ * host FP64 SoA in, accelerations written to host FP64 SoA. n may be 0. */
+int ob_solver_evaluate(ob_solver *solver, uint64_t n, const double *x, const double *y,
+                       const double *z, const double *m, double *ax, double *ay, double *az);
+
+/* The same evaluation on device-resident FP64 arrays, enqueued on `stream`
+ * (a cudaStream_t, NULL = the default stream) without synchronising. Replaces
+ * launch_cuda_direct / launch_cuda_tree (cuda_kernels.hpp:111,228). */
+int ob_solver_evaluate_device(ob_solver *solver, uint64_t n, const double *x, const double *y,
+                              const double *z, const double *m, double *ax, double *ay,
+                              double *az, void *stream);
+
+/* ForceSolver::interaction_count / reset_interaction_count
+ * (force_solver.hpp:64-76). Tree counts are read back when asked for. */
+int ob_solver_counts(ob_solver *solver, ob_counts *counts);
+int ob_solver_reset_counts(ob_solver *solver);
+int ob_solver_timings(const ob_solver *solver, ob_timings *timings);
+
+/* Tile shape of the direct kernels: threads per CTA, targets per thread and
+ * the number of CTAs (one thread-block cluster) that split the sources of a
+ * target tile. No reference counterpart: the reference picks one block size
+ * (src/solvers/cuda_direct_solver.cpp:46-63). */
+typedef struct ob_direct_shape {
+    int32_t threads;
+    int32_t targets_per_thread;
+    int32_t split;
+    int32_t reserved;
+} ob_direct_shape;
+
+/* Lists the shapes the library implements for a precision (FP32 or SPLIT);
+ * *count receives the total even when it exceeds capacity. */
+int ob_direct_shapes(int32_t precision, ob_direct_shape *out, int32_t capacity, int32_t *count);
+
+/* Fixes the shape a direct solver uses for n particles. */
+int ob_solver_set_direct_shape(ob_solver *solver, uint64_t n, const ob_direct_shape *shape);
+
+/* Times every implemented shape on the device for n synthetic particles and
+ * keeps the fastest for n; returns it and its time per evaluation. */
+int ob_solver_autotune(ob_solver *solver, uint64_t n, ob_direct_shape *chosen, double *best_ms);
+
+/* ------------------------------------------------------------------------ */
+/* System: particle state resident in HBM, integrated on the device          */
+/* ------------------------------------------------------------------------ */
+typedef struct ob_system ob_system;
+
+/* A system of n particles with its own solver. The state is FP64 SoA in HBM
+ * and stays there between steps. */
+int ob_system_create(const ob_solver_params *params, uint64_t n, ob_system **out);
+void ob_system_destroy(ob_system *system);
+
+/* Uploads positions, velocities and masses (velocities may be NULL = zero)
+ * and evaluates the accelerations, as sim::Simulation's constructor does
+ * (src/sim/simulation.cpp:16-27). */
+int ob_system_set_state(ob_system *system, const double *x, const double *y, const double *z,
+                        const double *vx, const double *vy, const double *vz, const double *m);
+
+/* Overwrites the carried accelerations (as a restored checkpoint does). */
+int ob_system_set_accelerations(ob_system *system, const double *ax, const double *ay,
+                                const double *az);
+
+/* Downloads any of the arrays (NULL pointers are skipped). */
+int ob_system_get_state(ob_system *system, double *x, double *y, double *z, double *vx,
+                        double *vy, double *vz, double *ax, double *ay, double *az);
+
+/* Advances `steps` steps of the integrator with timestep dt (Integrator::step,
+ * integrator.hpp:65), entirely on the device; one step is replayed from a CUDA
+ * graph. Synchronous. */
+int ob_system_step(ob_system *system, int32_t integrator, double dt, uint64_t steps);
+
+/* The same, enqueued without waiting (sync with ob_system_synchronize). */
+int ob_system_step_async(ob_system *system, int32_t integrator, double dt, uint64_t steps);
+int ob_system_synchronize(ob_system *system);
+
+/* Energies in FP64 on the device (core::kinetic_energy / potential_energy,
+ * src/core/diagnostics.cpp:118-158); the O(N^2) potential uses the system's
+ * softening. Either pointer may be NULL. */
+int ob_system_energy(ob_system *system, double *kinetic, double *potential);
+
+/* The stream the system's work is enqueued on (a cudaStream_t), for callers
+ * that order their own work or events after it. */
+int ob_system_stream(ob_system *system, void **stream);
+
+/* Per-phase device timing inside graph replays: the next `steps` steps record
+ * CUDA events around each evaluation's phases (0 turns it off).
+ * ob_system_phase_times then gives the per-evaluation average of each phase
+ * (ordering, construction, traversal) over the recorded steps, and the number
+ * of evaluations averaged. Synchronises. */
+int ob_system_profile(ob_system *system, uint32_t steps);
+int ob_system_phase_times(ob_system *system, ob_timings *average, uint32_t *evaluations);
+
+/* Kernel launches one step of the integrator makes (kernel nodes of the
+ * captured step graph). */
+int ob_system_step_kernels(ob_system *system, int32_t integrator, double dt, uint32_t *kernels);
+
+int ob_system_counts(ob_system *system, ob_counts *counts);
+int ob_system_size(const ob_system *system, uint64_t *n);
+
+/* Measured FP32 FFMA and SFU rsqrt lane operations per second on the current
+ * device: the denominators of the direct kernel's roofline. No reference
+ * counterpart in the library (the reference's probes are benchmark code,
+ * benchmarks/cuda_probes.cu:15-115). */
+int ob_probe_fp32(double *ffma_lane_per_s, double *rsqrt_lane_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ORRERY_B200_H */

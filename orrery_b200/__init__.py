@@ -1,0 +1,438 @@
+"""orrery_b200: a B200 (sm_100a) force-evaluation backend for Orrery.
+
+Python view of the C ABI in ``include/orrery_b200.h``. The solver classes
+mirror the reference's ``ForceSolver`` surface
+(include/orrery/solvers/force_solver.hpp:41-87): ``evaluate(positions, masses,
+accelerations)`` writes accelerations for FP64 structure-of-arrays input,
+``name()``, ``softening()``, ``interaction_count()`` and
+``reset_interaction_count()``; construction goes through ``try_create``, which
+returns ``None`` when no usable device exists, as ``CudaDirectSolver::try_create``
+does (src/solvers/cuda_direct_solver.cpp:140-164). Runtime failures raise
+:class:`OrreryError` carrying the C status code.
+
+There is no CPU fallback: importing works without a GPU (so that host logic can
+be tested), but every call that needs the device goes through the CUDA library
+and fails with an error when the library or the device is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(HERE, "_lib", "liborrery_b200.so")
+
+OK = 0
+ERROR_INVALID_ARGUMENT = 1
+ERROR_NO_DEVICE = 2
+ERROR_OUT_OF_MEMORY = 3
+ERROR_CUDA = 4
+ERROR_TIMEOUT = 5
+ERROR_CAPACITY = 6
+ERROR_UNSUPPORTED = 7
+
+SOLVER_DIRECT = 0
+SOLVER_TREE = 1
+PRECISION_FP32 = 0
+PRECISION_SPLIT = 1
+PRECISION_FP64 = 2
+INTEGRATOR_VV = 0
+INTEGRATOR_YOSHIDA4 = 1
+
+_PRECISIONS = {"fp32": PRECISION_FP32, "split": PRECISION_SPLIT, "fp64": PRECISION_FP64}
+_INTEGRATORS = {"vv": INTEGRATOR_VV, "velocity-verlet": INTEGRATOR_VV,
+                "yoshida4": INTEGRATOR_YOSHIDA4}
+
+
+class OrreryError(RuntimeError):
+    """A failed C-ABI call: ``code`` is the OB_ERROR_* status."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("precision", C.c_int32), ("softening", C.c_double),
+                ("opening_angle", C.c_double), ("leaf_capacity", C.c_uint64),
+                ("quadrupole", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Counts(C.Structure):
+    _fields_ = [("evaluations", C.c_uint64), ("particle_particle", C.c_uint64),
+                ("particle_cell", C.c_uint64)]
+
+
+class DirectShape(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("targets_per_thread", C.c_int32),
+                ("split", C.c_int32), ("reserved", C.c_int32)]
+
+
+class Timings(C.Structure):
+    _fields_ = [("transfer_in_ms", C.c_double), ("ordering_ms", C.c_double),
+                ("construction_ms", C.c_double), ("traversal_ms", C.c_double),
+                ("transfer_out_ms", C.c_double)]
+
+
+@dataclass
+class InteractionCount:
+    """solvers::InteractionCount (include/orrery/solvers/interaction_count.hpp:37-76)."""
+    evaluations: int = 0
+    particle_particle: int = 0
+    particle_cell: int = 0
+
+
+_dp = C.POINTER(C.c_double)
+_lib = None
+
+
+def library_path() -> str:
+    return LIBRARY_PATH
+
+
+def load_library():
+    """Loads the CUDA library, raising if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBRARY_PATH):
+        raise OrreryError(ERROR_NO_DEVICE,
+                          f"the CUDA library is missing ({LIBRARY_PATH}); run "
+                          "`python -m orrery_b200.build`")
+    lib = C.CDLL(LIBRARY_PATH)
+    vp = C.c_void_p
+    lib.ob_version.restype = C.c_char_p
+    lib.ob_last_error.restype = C.c_char_p
+    lib.ob_device_count.argtypes = [C.POINTER(C.c_int)]
+    lib.ob_solver_create.argtypes = [C.POINTER(SolverParams), C.POINTER(vp)]
+    lib.ob_solver_destroy.argtypes = [vp]
+    lib.ob_solver_destroy.restype = None
+    lib.ob_solver_get_params.argtypes = [vp, C.POINTER(SolverParams)]
+    lib.ob_solver_evaluate.argtypes = [vp, C.c_uint64] + [_dp] * 7
+    lib.ob_solver_evaluate_device.argtypes = [vp, C.c_uint64] + [vp] * 7 + [vp]
+    lib.ob_solver_counts.argtypes = [vp, C.POINTER(Counts)]
+    lib.ob_solver_reset_counts.argtypes = [vp]
+    lib.ob_solver_timings.argtypes = [vp, C.POINTER(Timings)]
+    lib.ob_direct_shapes.argtypes = [C.c_int32, C.POINTER(DirectShape), C.c_int32,
+                                     C.POINTER(C.c_int32)]
+    lib.ob_solver_set_direct_shape.argtypes = [vp, C.c_uint64, C.POINTER(DirectShape)]
+    lib.ob_solver_autotune.argtypes = [vp, C.c_uint64, C.POINTER(DirectShape),
+                                       C.POINTER(C.c_double)]
+    lib.ob_system_create.argtypes = [C.POINTER(SolverParams), C.c_uint64, C.POINTER(vp)]
+    lib.ob_system_destroy.argtypes = [vp]
+    lib.ob_system_destroy.restype = None
+    lib.ob_system_set_state.argtypes = [vp] + [_dp] * 7
+    lib.ob_system_set_accelerations.argtypes = [vp] + [_dp] * 3
+    lib.ob_system_get_state.argtypes = [vp] + [_dp] * 9
+    lib.ob_system_step.argtypes = [vp, C.c_int32, C.c_double, C.c_uint64]
+    lib.ob_system_step_async.argtypes = [vp, C.c_int32, C.c_double, C.c_uint64]
+    lib.ob_system_synchronize.argtypes = [vp]
+    lib.ob_system_energy.argtypes = [vp, _dp, _dp]
+    lib.ob_system_counts.argtypes = [vp, C.POINTER(Counts)]
+    lib.ob_system_size.argtypes = [vp, C.POINTER(C.c_uint64)]
+    lib.ob_probe_fp32.argtypes = [_dp, _dp]
+    lib.ob_system_stream.argtypes = [vp, C.POINTER(vp)]
+    lib.ob_system_profile.argtypes = [vp, C.c_uint32]
+    lib.ob_system_phase_times.argtypes = [vp, C.POINTER(Timings), C.POINTER(C.c_uint32)]
+    lib.ob_system_step_kernels.argtypes = [vp, C.c_int32, C.c_double, C.POINTER(C.c_uint32)]
+    _lib = lib
+    return lib
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        raise OrreryError(rc, load_library().ob_last_error().decode())
+
+
+def version() -> str:
+    return load_library().ob_version().decode()
+
+
+def device_count() -> int:
+    n = C.c_int(0)
+    _check(load_library().ob_device_count(C.byref(n)))
+    return n.value
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def make_params(kind=SOLVER_DIRECT, precision="fp32", softening=0.0, opening_angle=0.5,
+                leaf_capacity=32, quadrupole=False) -> SolverParams:
+    prec = _PRECISIONS[precision] if isinstance(precision, str) else int(precision)
+    return SolverParams(kind, prec, float(softening), float(opening_angle), int(leaf_capacity),
+                        1 if quadrupole else 0, 0)
+
+
+class _Solver:
+    """Common body of the two ForceSolver counterparts."""
+
+    _name = ""
+
+    def __init__(self, params: SolverParams):
+        lib = load_library()
+        handle = C.c_void_p()
+        _check(lib.ob_solver_create(C.byref(params), C.byref(handle)))
+        self._handle = handle
+        self._lib = lib
+
+    @classmethod
+    def _try(cls, params: SolverParams):
+        try:
+            return cls(params)
+        except OrreryError as e:
+            if e.code == ERROR_NO_DEVICE:
+                return None
+            raise
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            self._lib.ob_solver_destroy(h)
+            self._handle = None
+
+    def name(self) -> str:
+        return self._name
+
+    def params(self) -> SolverParams:
+        p = SolverParams()
+        _check(self._lib.ob_solver_get_params(self._handle, C.byref(p)))
+        return p
+
+    def softening(self) -> float:
+        return self.params().softening
+
+    def evaluate(self, positions, masses, accelerations=None) -> np.ndarray:
+        """ForceSolver::evaluate: positions (3, N) or (N, 3) FP64, masses (N,).
+
+        Writes into ``accelerations`` (three arrays x, y, z) when given --
+        directly, without a copy, when they are contiguous FP64 of length N, in
+        which case nothing is returned -- and otherwise returns the
+        accelerations as an (N, 3) array."""
+        x, y, z = _split_xyz(positions)
+        m = _f64(masses)
+        n = len(m)
+        direct = accelerations is not None and all(
+            isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.c_contiguous
+            and a.shape == (n,) for a in accelerations)
+        out = list(accelerations) if direct else [np.empty(n) for _ in range(3)]
+        _check(self._lib.ob_solver_evaluate(self._handle, n, _ptr(x), _ptr(y), _ptr(z), _ptr(m),
+                                            _ptr(out[0]), _ptr(out[1]), _ptr(out[2])))
+        if accelerations is not None and not direct:
+            for k in range(3):
+                accelerations[k][...] = out[k]
+        if direct:
+            return None
+        return np.stack(out, axis=1)
+
+    def evaluate_device(self, n, x, y, z, m, ax, ay, az, stream=0) -> None:
+        """Device-pointer form (integers or objects with ``data_ptr()``)."""
+        ptrs = [p.data_ptr() if hasattr(p, "data_ptr") else int(p)
+                for p in (x, y, z, m, ax, ay, az)]
+        _check(self._lib.ob_solver_evaluate_device(self._handle, int(n), *ptrs, stream or None))
+
+    def interaction_count(self) -> InteractionCount:
+        c = Counts()
+        _check(self._lib.ob_solver_counts(self._handle, C.byref(c)))
+        return InteractionCount(c.evaluations, c.particle_particle, c.particle_cell)
+
+    def reset_interaction_count(self) -> None:
+        _check(self._lib.ob_solver_reset_counts(self._handle))
+
+    def set_shape(self, n: int, shape) -> None:
+        """Fixes the direct kernel shape (threads, targets_per_thread, split) for n."""
+        s = DirectShape(*shape, 0) if not isinstance(shape, DirectShape) else shape
+        _check(self._lib.ob_solver_set_direct_shape(self._handle, int(n), C.byref(s)))
+
+    def autotune(self, n: int):
+        """Times every direct kernel shape for n particles; keeps and returns the best."""
+        s = DirectShape()
+        ms = C.c_double()
+        _check(self._lib.ob_solver_autotune(self._handle, int(n), C.byref(s), C.byref(ms)))
+        return (s.threads, s.targets_per_thread, s.split), ms.value
+
+    def timings(self) -> dict:
+        t = Timings()
+        _check(self._lib.ob_solver_timings(self._handle, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in Timings._fields_}
+
+
+class B200DirectSolver(_Solver):
+    """Direct O(N^2) solver (the reference's DirectSolver / CudaDirectSolver)."""
+
+    _name = "b200-direct"
+
+    def __init__(self, softening: float = 0.0, precision: str = "fp32"):
+        super().__init__(make_params(SOLVER_DIRECT, precision, softening))
+
+    @classmethod
+    def try_create(cls, softening: float = 0.0, precision: str = "fp32"):
+        try:
+            return cls(softening, precision)
+        except OrreryError as e:
+            if e.code == ERROR_NO_DEVICE:
+                return None
+            raise
+
+
+class B200TreeSolver(_Solver):
+    """Barnes-Hut solver (the reference's BarnesHutSolver / CudaTreeSolver)."""
+
+    _name = "b200-tree"
+
+    def __init__(self, softening: float = 0.0, opening_angle: float = 0.5,
+                 leaf_capacity: int = 32, quadrupole: bool = False):
+        super().__init__(make_params(SOLVER_TREE, "fp32", softening, opening_angle,
+                                     leaf_capacity, quadrupole))
+
+    @classmethod
+    def try_create(cls, softening: float = 0.0, opening_angle: float = 0.5,
+                   leaf_capacity: int = 32, quadrupole: bool = False):
+        try:
+            return cls(softening, opening_angle, leaf_capacity, quadrupole)
+        except OrreryError as e:
+            if e.code == ERROR_NO_DEVICE:
+                return None
+            raise
+
+
+def direct_shapes(precision: str = "fp32"):
+    """Every (threads, targets_per_thread, split) shape of a direct kernel."""
+    lib = load_library()
+    count = C.c_int32()
+    _check(lib.ob_direct_shapes(_PRECISIONS[precision], None, 0, C.byref(count)))
+    arr = (DirectShape * count.value)()
+    _check(lib.ob_direct_shapes(_PRECISIONS[precision], arr, count.value, C.byref(count)))
+    return [(s.threads, s.targets_per_thread, s.split) for s in arr]
+
+
+def _split_xyz(positions):
+    p = np.asarray(positions, dtype=np.float64)
+    if isinstance(positions, (tuple, list)) and len(positions) == 3:
+        return tuple(_f64(a) for a in positions)
+    if p.ndim == 2 and p.shape[0] == 3 and p.shape[1] != 3:
+        return tuple(_f64(p[k]) for k in range(3))
+    if p.ndim == 2 and p.shape[1] == 3:
+        return tuple(_f64(p[:, k]) for k in range(3))
+    if p.ndim == 2 and p.shape == (3, 3):
+        return tuple(_f64(p[:, k]) for k in range(3))
+    raise ValueError("positions must be (N, 3), (3, N) or a tuple of three arrays")
+
+
+class DeviceSystem:
+    """A particle system resident in HBM, integrated on the device.
+
+    ``step(dt, steps, integrator)`` advances with velocity Verlet or Yoshida-4
+    (src/integrators/velocity_verlet.cpp:59-72, yoshida4.cpp:45-59); one step is
+    a replayed CUDA graph and no state crosses to the host between steps."""
+
+    def __init__(self, n: int, softening: float = 0.0, kind: int = SOLVER_DIRECT,
+                 precision: str = "fp32", opening_angle: float = 0.5, leaf_capacity: int = 32,
+                 quadrupole: bool = False):
+        lib = load_library()
+        handle = C.c_void_p()
+        params = make_params(kind, precision, softening, opening_angle, leaf_capacity,
+                             quadrupole)
+        _check(lib.ob_system_create(C.byref(params), int(n), C.byref(handle)))
+        self._lib = lib
+        self._handle = handle
+        self.n = int(n)
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            self._lib.ob_system_destroy(h)
+            self._handle = None
+
+    def set_state(self, x, y, z, vx=None, vy=None, vz=None, m=None) -> None:
+        arrs = [_f64(a) if a is not None else None for a in (x, y, z, vx, vy, vz, m)]
+        _check(self._lib.ob_system_set_state(self._handle, *(_ptr(a) for a in arrs)))
+
+    def set_accelerations(self, ax, ay, az) -> None:
+        arrs = [_f64(a) for a in (ax, ay, az)]
+        _check(self._lib.ob_system_set_accelerations(self._handle, *(_ptr(a) for a in arrs)))
+
+    def state(self) -> dict:
+        out = {k: np.empty(self.n) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")}
+        _check(self._lib.ob_system_get_state(self._handle, *(_ptr(out[k]) for k in (
+            "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az"))))
+        return out
+
+    def step(self, dt: float, steps: int = 1, integrator: str = "vv") -> None:
+        _check(self._lib.ob_system_step(self._handle, _INTEGRATORS[integrator], float(dt),
+                                        int(steps)))
+
+    def step_async(self, dt: float, steps: int = 1, integrator: str = "vv") -> None:
+        _check(self._lib.ob_system_step_async(self._handle, _INTEGRATORS[integrator], float(dt),
+                                              int(steps)))
+
+    def synchronize(self) -> None:
+        _check(self._lib.ob_system_synchronize(self._handle))
+
+    def energy(self):
+        ke, pe = C.c_double(), C.c_double()
+        _check(self._lib.ob_system_energy(self._handle, C.byref(ke), C.byref(pe)))
+        return ke.value, pe.value
+
+    def kinetic_energy(self) -> float:
+        ke = C.c_double()
+        _check(self._lib.ob_system_energy(self._handle, C.byref(ke), None))
+        return ke.value
+
+    def interaction_count(self) -> InteractionCount:
+        c = Counts()
+        _check(self._lib.ob_system_counts(self._handle, C.byref(c)))
+        return InteractionCount(c.evaluations, c.particle_particle, c.particle_cell)
+
+    def stream(self) -> int:
+        """The cudaStream_t (as an integer) the system enqueues its work on."""
+        s = C.c_void_p()
+        _check(self._lib.ob_system_stream(self._handle, C.byref(s)))
+        return s.value or 0
+
+    def profile(self, steps: int) -> None:
+        """Record per-phase events for the next ``steps`` steps."""
+        _check(self._lib.ob_system_profile(self._handle, int(steps)))
+
+    def phase_times(self):
+        """Per-evaluation average phase times (ms) over the profiled steps."""
+        t = Timings()
+        n = C.c_uint32()
+        _check(self._lib.ob_system_phase_times(self._handle, C.byref(t), C.byref(n)))
+        return {k: getattr(t, k) for k, _ in Timings._fields_}, n.value
+
+    def step_kernels(self, dt: float, integrator: str = "vv") -> int:
+        """Kernel launches in one captured step."""
+        k = C.c_uint32()
+        _check(self._lib.ob_system_step_kernels(self._handle, _INTEGRATORS[integrator],
+                                                float(dt), C.byref(k)))
+        return k.value
+
+
+def probe_fp32():
+    """Measured (FFMA lane ops/s, SFU rsqrt lane ops/s) of the current device."""
+    a, b = C.c_double(), C.c_double()
+    _check(load_library().ob_probe_fp32(C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+def compute_accelerations(positions, masses, softening: float = 0.0, solver: str = "direct",
+                          precision: str = "fp32", opening_angle: float = 0.5,
+                          leaf_capacity: int = 32, quadrupole: bool = False) -> np.ndarray:
+    """One force evaluation, the counterpart of the reference's Python
+    ``orrery.compute_accelerations`` (python/src/sim_bindings.cpp:383-410)."""
+    if solver == "direct":
+        s = B200DirectSolver(softening, precision)
+    elif solver in ("tree", "barnes-hut"):
+        s = B200TreeSolver(softening, opening_angle, leaf_capacity, quadrupole)
+    else:
+        raise ValueError(f"unknown solver {solver!r}")
+    return s.evaluate(positions, masses)

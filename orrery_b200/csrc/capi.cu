@@ -1,0 +1,634 @@
+// The extern "C" boundary (include/orrery_b200.h) and the device-resident
+// system that integrates on the GPU.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "orrery_b200.h"
+#include "solver.hpp"
+#include "system.hpp"
+
+namespace ob {
+
+namespace {
+thread_local std::string g_last_error;
+
+template <typename F> int guarded(F &&body) {
+    try {
+        body();
+        return OB_OK;
+    } catch (const Error &e) {
+        return set_error(e.code(), e.what());
+    } catch (const std::bad_alloc &) {
+        return set_error(OB_ERROR_OUT_OF_MEMORY, "host allocation failed");
+    } catch (const std::exception &e) {
+        return set_error(OB_ERROR_INVALID_ARGUMENT, e.what());
+    }
+}
+
+// The try_create contract: OB_ERROR_NO_DEVICE when there is no usable
+// Blackwell device (src/solvers/cuda_direct_solver.cpp:140-164).
+void require_device() {
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        throw Error(OB_ERROR_NO_DEVICE, "no CUDA device is visible");
+    }
+    int device = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    int major = 0;
+    check(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device),
+          "querying the compute capability");
+    if (major != 10) {
+        throw Error(OB_ERROR_NO_DEVICE, "the device is not an sm_100 (Blackwell) GPU");
+    }
+}
+
+void require(bool condition, const char *message) {
+    if (!condition) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, message);
+    }
+}
+} // namespace
+
+int set_error(int code, const std::string &message) {
+    g_last_error = message;
+    return code;
+}
+
+// --------------------------------------------------------------------------
+// System
+// --------------------------------------------------------------------------
+
+System::System(const ob_solver_params &params, uint32_t n)
+    : solver_(std::make_unique<Solver>(params)), n_(n) {
+    state_.reserve(10ull * (n == 0 ? 1 : n));
+    check(cudaMemset(state_.data(), 0, state_.bytes()), "clearing state");
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a stream");
+}
+
+System::~System() {
+    drop_graph();
+    for (auto e : marks_) {
+        cudaEventDestroy(e);
+    }
+    for (auto e : ring_) {
+        cudaEventDestroy(e);
+    }
+    if (stream_ != nullptr) {
+        cudaStreamDestroy(stream_);
+    }
+}
+
+void System::drop_graph() {
+    if (graph_ != nullptr) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+    if (template_ != nullptr) {
+        cudaGraphDestroy(template_);
+        template_ = nullptr;
+    }
+    mark_nodes_.clear();
+    marks_retargeted_ = false;
+}
+
+void System::upload(int first, int count, const double *const *host) {
+    for (int k = 0; k < count; ++k) {
+        double *dst = array(first + k);
+        if (host[k] == nullptr) {
+            check(cudaMemsetAsync(dst, 0, sizeof(double) * n_, stream_), "clearing an array");
+        } else {
+            check(cudaMemcpyAsync(dst, host[k], sizeof(double) * n_, cudaMemcpyHostToDevice,
+                                  stream_),
+                  "uploading state");
+        }
+    }
+}
+
+void System::set_state(const double *x, const double *y, const double *z, const double *vx,
+                       const double *vy, const double *vz, const double *m) {
+    require(n_ == 0 || (x && y && z && m), "positions and masses are required");
+    const double *in[7] = {x, y, z, vx, vy, vz, nullptr};
+    upload(kX, 6, in);
+    upload(kM, 1, &m);
+    refresh();
+}
+
+void System::set_accelerations(const double *ax, const double *ay, const double *az) {
+    const double *in[3] = {ax, ay, az};
+    upload(kAx, 3, in);
+    check(cudaStreamSynchronize(stream_), "uploading accelerations");
+}
+
+void System::refresh() {
+    evaluate(true);
+    check(cudaStreamSynchronize(stream_), "evaluating accelerations");
+    solver_->check_status(stream_);
+}
+
+void System::evaluate(bool count, const cudaEvent_t *marks) {
+    solver_->evaluate_device(n_, array(kX), array(kY), array(kZ), array(kM), array(kAx),
+                             array(kAy), array(kAz), stream_, count, marks);
+}
+
+void System::get_state(double *const *out) {
+    for (int k = 0; k < 9; ++k) {
+        if (out[k] != nullptr && n_ > 0) {
+            check(cudaMemcpyAsync(out[k], array(k), sizeof(double) * n_, cudaMemcpyDeviceToHost,
+                                  stream_),
+                  "downloading state");
+        }
+    }
+    check(cudaStreamSynchronize(stream_), "downloading state");
+}
+
+// Yoshida-4 substep weights, computed as src/integrators/yoshida4.cpp:24-30.
+static void yoshida_weights(double &outer, double &inner) {
+    constexpr double cube_root_of_two = 1.2599210498948731647672106;
+    outer = 1.0 / (2.0 - cube_root_of_two);
+    inner = -cube_root_of_two / (2.0 - cube_root_of_two);
+}
+
+int System::evaluations_per_step(int integrator) {
+    return integrator == OB_INTEGRATOR_YOSHIDA4 ? 3 : 1;
+}
+
+void System::enqueue_substep(double timestep, const cudaEvent_t *marks) {
+    // velocity_verlet_step (src/integrators/velocity_verlet.cpp:59-72).
+    const double half = timestep / 2.0;
+    check(launch_kick_drift(array(kX), array(kY), array(kZ), array(kVx), array(kVy), array(kVz),
+                            array(kAx), array(kAy), array(kAz), n_, half, timestep, stream_),
+          "kick and drift");
+    evaluate(false, marks);
+    check(launch_kick(array(kVx), array(kVy), array(kVz), array(kAx), array(kAy), array(kAz), n_,
+                      half, stream_),
+          "kick");
+}
+
+void System::enqueue_step(int integrator, double dt) {
+    const cudaEvent_t *m = marks_.data();
+    if (integrator == OB_INTEGRATOR_YOSHIDA4) {
+        double outer = 0.0, inner = 0.0;
+        yoshida_weights(outer, inner);
+        enqueue_substep(outer * dt, m);
+        enqueue_substep(inner * dt, m + 4);
+        enqueue_substep(outer * dt, m + 8);
+    } else {
+        enqueue_substep(dt, m);
+    }
+}
+
+void System::ensure_graph(int integrator, double dt) {
+    if (graph_ != nullptr && graph_integrator_ == integrator && graph_dt_ == dt) {
+        return;
+    }
+    drop_graph();
+    const size_t needed = 4u * static_cast<size_t>(evaluations_per_step(integrator));
+    while (marks_.size() < needed) {
+        cudaEvent_t e = nullptr;
+        check(cudaEventCreate(&e), "creating an event");
+        marks_.push_back(e);
+    }
+    cudaGraph_t graph = nullptr;
+    check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed),
+          "beginning graph capture");
+    try {
+        enqueue_step(integrator, dt);
+    } catch (...) {
+        cudaStreamEndCapture(stream_, &graph);
+        if (graph != nullptr) {
+            cudaGraphDestroy(graph);
+        }
+        throw;
+    }
+    check(cudaStreamEndCapture(stream_, &graph), "ending graph capture");
+    template_ = graph;
+    check(cudaGraphInstantiate(&graph_, graph, 0), "instantiating the step graph");
+    graph_integrator_ = integrator;
+    graph_dt_ = dt;
+    // Find the event-record node of each placeholder, and count kernels.
+    size_t count = 0;
+    check(cudaGraphGetNodes(graph, nullptr, &count), "listing graph nodes");
+    std::vector<cudaGraphNode_t> nodes(count);
+    check(cudaGraphGetNodes(graph, nodes.data(), &count), "listing graph nodes");
+    mark_nodes_.assign(needed, nullptr);
+    graph_kernels_ = 0;
+    for (cudaGraphNode_t node : nodes) {
+        cudaGraphNodeType type;
+        check(cudaGraphNodeGetType(node, &type), "reading a node type");
+        if (type == cudaGraphNodeTypeKernel) {
+            ++graph_kernels_;
+        } else if (type == cudaGraphNodeTypeEventRecord) {
+            cudaEvent_t e = nullptr;
+            check(cudaGraphEventRecordNodeGetEvent(node, &e), "reading an event node");
+            for (size_t k = 0; k < needed; ++k) {
+                if (marks_[k] == e) {
+                    mark_nodes_[k] = node;
+                }
+            }
+        }
+    }
+}
+
+void System::set_marks(const std::vector<cudaEvent_t> &events, size_t offset) {
+    for (size_t k = 0; k < mark_nodes_.size(); ++k) {
+        if (mark_nodes_[k] != nullptr) {
+            check(cudaGraphExecEventRecordNodeSetEvent(graph_, mark_nodes_[k], events[offset + k]),
+                  "retargeting an event node");
+        }
+    }
+}
+
+void System::profile(uint32_t steps) {
+    synchronize();
+    for (auto e : ring_) {
+        cudaEventDestroy(e);
+    }
+    ring_.clear();
+    ring_steps_ = steps;
+    ring_used_ = 0;
+    const size_t per_step = 12; // enough for the largest step (Yoshida-4: 3 x 4)
+    ring_.resize(per_step * steps, nullptr);
+    for (auto &e : ring_) {
+        check(cudaEventCreate(&e), "creating an event");
+    }
+}
+
+ob_timings System::phase_times(uint32_t &evaluations) {
+    synchronize();
+    ob_timings t{};
+    evaluations = 0;
+    const size_t per_eval_marks = 4;
+    const size_t evals = mark_nodes_.size() / per_eval_marks;
+    for (uint32_t s = 0; s < ring_used_; ++s) {
+        for (size_t e = 0; e < evals; ++e) {
+            const cudaEvent_t *m = &ring_[s * 12 + e * 4];
+            float a = 0, b = 0, c = 0;
+            check(cudaEventElapsedTime(&a, m[0], m[1]), "phase timing");
+            check(cudaEventElapsedTime(&b, m[1], m[2]), "phase timing");
+            check(cudaEventElapsedTime(&c, m[2], m[3]), "phase timing");
+            t.ordering_ms += a;
+            t.construction_ms += b;
+            t.traversal_ms += c;
+            ++evaluations;
+        }
+    }
+    if (evaluations > 0) {
+        t.ordering_ms /= evaluations;
+        t.construction_ms /= evaluations;
+        t.traversal_ms /= evaluations;
+    }
+    return t;
+}
+
+uint32_t System::step_kernels(int integrator, double dt) {
+    require(integrator == OB_INTEGRATOR_VV || integrator == OB_INTEGRATOR_YOSHIDA4,
+            "unknown integrator");
+    ensure_graph(integrator, dt);
+    return graph_kernels_;
+}
+
+void System::step_async(int integrator, double dt, uint64_t steps) {
+    require(integrator == OB_INTEGRATOR_VV || integrator == OB_INTEGRATOR_YOSHIDA4,
+            "unknown integrator");
+    require(std::isfinite(dt), "the timestep must be finite");
+    if (steps == 0 || n_ == 0) {
+        solver_->account(steps * evaluations_per_step(integrator), n_);
+        return;
+    }
+    ensure_graph(integrator, dt);
+    for (uint64_t s = 0; s < steps; ++s) {
+        if (ring_used_ < ring_steps_) {
+            set_marks(ring_, static_cast<size_t>(ring_used_) * 12);
+            marks_retargeted_ = true;
+            ++ring_used_;
+        } else if (marks_retargeted_) {
+            set_marks(marks_, 0);
+            marks_retargeted_ = false;
+        }
+        check(cudaGraphLaunch(graph_, stream_), "launching the step graph");
+    }
+    solver_->account(steps * evaluations_per_step(integrator), n_);
+}
+
+void System::synchronize() {
+    check(cudaStreamSynchronize(stream_), "integrating");
+    solver_->check_status(stream_);
+}
+
+// Neumaier summation in index order, as core::CompensatedSum
+// (src/core/diagnostics.cpp:36-59).
+static double compensated_sum(const std::vector<double> &terms) {
+    double total = 0.0, correction = 0.0;
+    for (const double term : terms) {
+        const double updated = total + term;
+        if (std::fabs(total) >= std::fabs(term)) {
+            correction += (total - updated) + term;
+        } else {
+            correction += (term - updated) + total;
+        }
+        total = updated;
+    }
+    return total + correction;
+}
+
+void System::energy(double *kinetic, double *potential) {
+    if (n_ == 0) {
+        if (kinetic) *kinetic = 0.0;
+        if (potential) *potential = 0.0;
+        return;
+    }
+    terms_.reserve(n_);
+    std::vector<double> host(n_);
+    if (kinetic != nullptr) {
+        check(launch_kinetic_partials(array(kVx), array(kVy), array(kVz), array(kM), n_,
+                                      terms_.data(), stream_),
+              "kinetic energy terms");
+        check(cudaMemcpyAsync(host.data(), terms_.data(), sizeof(double) * n_,
+                              cudaMemcpyDeviceToHost, stream_),
+              "downloading kinetic terms");
+        check(cudaStreamSynchronize(stream_), "kinetic energy");
+        *kinetic = compensated_sum(host) / 2.0;
+    }
+    if (potential != nullptr) {
+        const double eps = solver_->params().softening;
+        check(launch_potential_rows(array(kX), array(kY), array(kZ), array(kM), n_, eps * eps,
+                                    terms_.data(), stream_),
+              "potential energy rows");
+        check(cudaMemcpyAsync(host.data(), terms_.data(), sizeof(double) * n_,
+                              cudaMemcpyDeviceToHost, stream_),
+              "downloading potential rows");
+        check(cudaStreamSynchronize(stream_), "potential energy");
+        *potential = compensated_sum(host);
+    }
+}
+
+} // namespace ob
+
+// ---------------------------------------------------------------------------
+// extern "C"
+// ---------------------------------------------------------------------------
+
+struct ob_solver {
+    std::unique_ptr<ob::Solver> impl;
+};
+
+struct ob_system {
+    std::unique_ptr<ob::System> impl;
+};
+
+using ob::guarded;
+using ob::require;
+
+extern "C" {
+
+const char *ob_version(void) { return "orrery_b200 0.1.0 (sm_100a)"; }
+
+const char *ob_last_error(void) { return ob::g_last_error.c_str(); }
+
+int ob_device_count(int *count) {
+    return guarded([&] {
+        require(count != nullptr, "count is NULL");
+        *count = 0;
+        if (cudaGetDeviceCount(count) != cudaSuccess) {
+            cudaGetLastError();
+            *count = 0;
+        }
+    });
+}
+
+int ob_solver_create(const ob_solver_params *params, ob_solver **out) {
+    return guarded([&] {
+        require(out != nullptr && params != nullptr, "NULL argument");
+        *out = nullptr;
+        const ob_solver_params checked = ob::corrected(*params);
+        ob::require_device();
+        auto s = std::make_unique<ob_solver>();
+        s->impl = std::make_unique<ob::Solver>(checked);
+        *out = s.release();
+    });
+}
+
+void ob_solver_destroy(ob_solver *solver) { delete solver; }
+
+int ob_solver_get_params(const ob_solver *solver, ob_solver_params *params) {
+    return guarded([&] {
+        require(solver != nullptr && params != nullptr, "NULL argument");
+        *params = solver->impl->params();
+    });
+}
+
+int ob_solver_evaluate(ob_solver *solver, uint64_t n, const double *x, const double *y,
+                       const double *z, const double *m, double *ax, double *ay, double *az) {
+    return guarded([&] {
+        require(solver != nullptr, "solver is NULL");
+        require(n == 0 || (x && y && z && m && ax && ay && az), "NULL array");
+        solver->impl->evaluate_host(n, x, y, z, m, ax, ay, az);
+    });
+}
+
+int ob_solver_evaluate_device(ob_solver *solver, uint64_t n, const double *x, const double *y,
+                              const double *z, const double *m, double *ax, double *ay,
+                              double *az, void *stream) {
+    return guarded([&] {
+        require(solver != nullptr, "solver is NULL");
+        require(n <= 0xffffffffull, "the B200 solvers index particles with 32 bits");
+        require(n == 0 || (x && y && z && m && ax && ay && az), "NULL array");
+        solver->impl->evaluate_device(static_cast<uint32_t>(n), x, y, z, m, ax, ay, az,
+                                      static_cast<cudaStream_t>(stream));
+    });
+}
+
+int ob_solver_counts(ob_solver *solver, ob_counts *counts) {
+    return guarded([&] {
+        require(solver != nullptr && counts != nullptr, "NULL argument");
+        *counts = solver->impl->counts();
+    });
+}
+
+int ob_solver_reset_counts(ob_solver *solver) {
+    return guarded([&] {
+        require(solver != nullptr, "solver is NULL");
+        solver->impl->reset_counts();
+    });
+}
+
+int ob_solver_timings(const ob_solver *solver, ob_timings *timings) {
+    return guarded([&] {
+        require(solver != nullptr && timings != nullptr, "NULL argument");
+        *timings = solver->impl->timings();
+    });
+}
+
+int ob_direct_shapes(int32_t precision, ob_direct_shape *out, int32_t capacity, int32_t *count) {
+    return guarded([&] {
+        require(count != nullptr, "count is NULL");
+        require(precision == OB_PRECISION_FP32 || precision == OB_PRECISION_SPLIT,
+                "shapes exist for the FP32 and split direct kernels");
+        ob::DirectConfig all[64];
+        const int total = ob::direct_candidates(precision == OB_PRECISION_SPLIT, all, 64);
+        for (int k = 0; k < total && k < capacity && out != nullptr; ++k) {
+            out[k] = ob_direct_shape{all[k].threads, all[k].targets_per_thread, all[k].split, 0};
+        }
+        *count = total;
+    });
+}
+
+int ob_solver_set_direct_shape(ob_solver *solver, uint64_t n, const ob_direct_shape *shape) {
+    return guarded([&] {
+        require(solver != nullptr && shape != nullptr, "NULL argument");
+        require(n <= 0xffffffffull, "the B200 solvers index particles with 32 bits");
+        const ob_solver_params &p = solver->impl->params();
+        require(p.kind == OB_SOLVER_DIRECT && p.precision != OB_PRECISION_FP64,
+                "only the FP32 and split direct kernels have shapes");
+        ob::DirectConfig all[64];
+        const int total = ob::direct_candidates(p.precision == OB_PRECISION_SPLIT, all, 64);
+        bool known = false;
+        for (int k = 0; k < total; ++k) {
+            known = known || (all[k].threads == shape->threads &&
+                              all[k].targets_per_thread == shape->targets_per_thread &&
+                              all[k].split == shape->split);
+        }
+        require(known, "the library implements no such direct kernel shape");
+        solver->impl->set_direct_config(
+            static_cast<uint32_t>(n),
+            ob::DirectConfig{shape->threads, shape->targets_per_thread, shape->split});
+    });
+}
+
+int ob_solver_autotune(ob_solver *solver, uint64_t n, ob_direct_shape *chosen, double *best_ms) {
+    return guarded([&] {
+        require(solver != nullptr, "solver is NULL");
+        require(n <= 0xffffffffull, "the B200 solvers index particles with 32 bits");
+        ob::DirectConfig c;
+        const double ms = solver->impl->autotune(static_cast<uint32_t>(n), c);
+        if (chosen != nullptr) {
+            *chosen = ob_direct_shape{c.threads, c.targets_per_thread, c.split, 0};
+        }
+        if (best_ms != nullptr) {
+            *best_ms = ms;
+        }
+    });
+}
+
+int ob_system_create(const ob_solver_params *params, uint64_t n, ob_system **out) {
+    return guarded([&] {
+        require(out != nullptr && params != nullptr, "NULL argument");
+        *out = nullptr;
+        require(n <= 0xffffffffull, "the B200 solvers index particles with 32 bits");
+        const ob_solver_params checked = ob::corrected(*params);
+        ob::require_device();
+        auto s = std::make_unique<ob_system>();
+        s->impl = std::make_unique<ob::System>(checked, static_cast<uint32_t>(n));
+        *out = s.release();
+    });
+}
+
+void ob_system_destroy(ob_system *system) { delete system; }
+
+int ob_system_set_state(ob_system *system, const double *x, const double *y, const double *z,
+                        const double *vx, const double *vy, const double *vz, const double *m) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        system->impl->set_state(x, y, z, vx, vy, vz, m);
+    });
+}
+
+int ob_system_set_accelerations(ob_system *system, const double *ax, const double *ay,
+                                const double *az) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        system->impl->set_accelerations(ax, ay, az);
+    });
+}
+
+int ob_system_get_state(ob_system *system, double *x, double *y, double *z, double *vx,
+                        double *vy, double *vz, double *ax, double *ay, double *az) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        double *out[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+        system->impl->get_state(out);
+    });
+}
+
+int ob_system_step(ob_system *system, int32_t integrator, double dt, uint64_t steps) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        system->impl->step_async(integrator, dt, steps);
+        system->impl->synchronize();
+    });
+}
+
+int ob_system_step_async(ob_system *system, int32_t integrator, double dt, uint64_t steps) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        system->impl->step_async(integrator, dt, steps);
+    });
+}
+
+int ob_system_synchronize(ob_system *system) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        system->impl->synchronize();
+    });
+}
+
+int ob_system_energy(ob_system *system, double *kinetic, double *potential) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        system->impl->energy(kinetic, potential);
+    });
+}
+
+int ob_system_counts(ob_system *system, ob_counts *counts) {
+    return guarded([&] {
+        require(system != nullptr && counts != nullptr, "NULL argument");
+        *counts = system->impl->solver().counts();
+    });
+}
+
+int ob_system_stream(ob_system *system, void **stream) {
+    return guarded([&] {
+        require(system != nullptr && stream != nullptr, "NULL argument");
+        *stream = system->impl->stream();
+    });
+}
+
+int ob_system_profile(ob_system *system, uint32_t steps) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        system->impl->profile(steps);
+    });
+}
+
+int ob_system_phase_times(ob_system *system, ob_timings *average, uint32_t *evaluations) {
+    return guarded([&] {
+        require(system != nullptr && average != nullptr, "NULL argument");
+        uint32_t count = 0;
+        *average = system->impl->phase_times(count);
+        if (evaluations != nullptr) {
+            *evaluations = count;
+        }
+    });
+}
+
+int ob_system_step_kernels(ob_system *system, int32_t integrator, double dt, uint32_t *kernels) {
+    return guarded([&] {
+        require(system != nullptr && kernels != nullptr, "NULL argument");
+        *kernels = system->impl->step_kernels(integrator, dt);
+    });
+}
+
+int ob_system_size(const ob_system *system, uint64_t *n) {
+    return guarded([&] {
+        require(system != nullptr && n != nullptr, "NULL argument");
+        *n = system->impl->size();
+    });
+}
+
+} // extern "C"

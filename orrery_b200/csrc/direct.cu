@@ -1,0 +1,581 @@
+// Direct O(N^2) force sum on sm_100a.
+//
+// Replaces the reference's direct_kernel (src/solvers/cuda_direct_kernel.cu:87-184)
+// and the CPU DirectSolver it mirrors (src/solvers/direct_solver.cpp:20-80).
+// The force law is the reference's Plummer-softened one,
+// a_i = sum_{j != i} m_j d_ij (|d_ij|^2 + eps^2)^{-3/2}
+// (include/orrery/core/softening.hpp:83-100), with G = 1.
+//
+// Layout and schedule (FP32 and split forms):
+//   * sources are packed once per evaluation into float4 (x, y, z, m), padded
+//     with zero-mass entries to a whole number of tiles;
+//   * a CTA owns THREADS*R targets held in registers (R per thread) and walks a
+//     contiguous range of source tiles, each 512-particle tile brought into
+//     shared memory by one 1-D bulk copy (cp.async.bulk) on an mbarrier,
+//     double-buffered so the next tile lands while this one is summed;
+//   * every thread reads the same source at the same time, so each float4 read
+//     is a shared-memory broadcast amortised over the R targets of the thread;
+//   * tiles that contain no target of the CTA and no padding run a branch-free
+//     loop; the few that do select zero mass for j == i and j >= n, as the
+//     reference kernel masks (cuda_direct_kernel.cu:155-160);
+//   * when the targets alone cannot fill 148 SMs, S CTAs of one thread-block
+//     cluster split the source range and their partial sums are reduced through
+//     distributed shared memory in a fixed rank order (deterministic).
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "internal.hpp"
+
+namespace cg = cooperative_groups;
+
+namespace ob {
+namespace {
+
+struct DirectArgs {
+    const float4 *hi;
+    const float4 *lo;
+    uint32_t n;
+    uint32_t padded;
+    float eps2;
+    double *ax;
+    double *ay;
+    double *az;
+    unsigned *status;
+};
+
+// Range of source tiles [tb, te) handled by split rank `rank`.
+__device__ __forceinline__ void source_tiles(uint32_t n, uint32_t split, uint32_t rank,
+                                             uint32_t &tb, uint32_t &te) {
+    const uint32_t tiles = ceil_div(n, kDirectTile);
+    const uint32_t per = ceil_div(tiles, split);
+    tb = min(rank * per, tiles);
+    te = min(tb + per, tiles);
+}
+
+// Issues the bulk copies of tile `k` into buffer `buf` (thread 0 only).
+template <bool SPLIT>
+__device__ __forceinline__ void stage_tile(const DirectArgs &a, float4 *tiles_hi,
+                                           float4 *tiles_lo, uint64_t *bars, uint32_t k,
+                                           uint32_t buf) {
+    constexpr uint32_t bytes = kDirectTile * sizeof(float4);
+    mbar_arrive_expect_tx(&bars[buf], SPLIT ? 2 * bytes : bytes);
+    bulk_copy_g2s(tiles_hi + buf * kDirectTile, a.hi + static_cast<size_t>(k) * kDirectTile,
+                  bytes, &bars[buf]);
+    if (SPLIT) {
+        bulk_copy_g2s(tiles_lo + buf * kDirectTile, a.lo + static_cast<size_t>(k) * kDirectTile,
+                      bytes, &bars[buf]);
+    }
+}
+
+// Writes the CTA's per-target sums, reducing across the cluster when split.
+// `partial` holds 3*BT values of type T laid out [component][slot].
+template <int THREADS, int R, typename T>
+__device__ __forceinline__ void finish_targets(const DirectArgs &a, uint32_t t0, T *partial,
+                                               const double (&sx)[R], const double (&sy)[R],
+                                               const double (&sz)[R]) {
+    constexpr uint32_t BT = THREADS * R;
+    const uint32_t split = gridDim.x;
+    const uint32_t tid = threadIdx.x;
+    if (split == 1) {
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const uint32_t i = t0 + r * THREADS + tid;
+            if (i < a.n) {
+                a.ax[i] = sx[r];
+                a.ay[i] = sy[r];
+                a.az[i] = sz[r];
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const uint32_t slot = r * THREADS + tid;
+        partial[slot] = static_cast<T>(sx[r]);
+        partial[BT + slot] = static_cast<T>(sy[r]);
+        partial[2 * BT + slot] = static_cast<T>(sz[r]);
+    }
+    cg::cluster_group cluster = cg::this_cluster();
+    cluster.sync();
+    const uint32_t rank = blockIdx.x;
+    const uint32_t per = BT / split;
+    for (uint32_t k = tid; k < per; k += THREADS) {
+        const uint32_t slot = rank * per + k;
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+        for (uint32_t q = 0; q < split; ++q) {
+            const T *remote = cluster.map_shared_rank(partial, q);
+            s0 += static_cast<double>(remote[slot]);
+            s1 += static_cast<double>(remote[BT + slot]);
+            s2 += static_cast<double>(remote[2 * BT + slot]);
+        }
+        const uint32_t i = t0 + slot;
+        if (i < a.n) {
+            a.ax[i] = s0;
+            a.ay[i] = s1;
+            a.az[i] = s2;
+        }
+    }
+    cluster.sync();
+}
+
+template <int THREADS, int R>
+__global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr uint32_t BT = THREADS * R;
+    float4 *tiles = reinterpret_cast<float4 *>(smem);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * kDirectTile * sizeof(float4));
+    float *partial = reinterpret_cast<float *>(bars + 2);
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t t0 = blockIdx.y * BT;
+    const float eps2 = a.eps2;
+
+    float px[R], py[R], pz[R], ax[R], ay[R], az[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const float4 p = a.hi[t0 + r * THREADS + tid];
+        px[r] = p.x;
+        py[r] = p.y;
+        pz[r] = p.z;
+        ax[r] = ay[r] = az[r] = 0.0f;
+    }
+
+    uint32_t tb, te;
+    source_tiles(a.n, gridDim.x, blockIdx.x, tb, te);
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (uint32_t k = tb; k < min(tb + 2, te); ++k) {
+            stage_tile<false>(a, tiles, nullptr, bars, k, k - tb);
+        }
+    }
+
+    bool ok = true;
+    for (uint32_t k = tb; k < te; ++k) {
+        const uint32_t it = k - tb;
+        const uint32_t buf = it & 1u;
+        if (ok) {
+            ok = mbar_wait_bounded(&bars[buf], (it >> 1) & 1u, a.status);
+        }
+        if (ok) {
+            const float4 *tile = tiles + buf * kDirectTile;
+            const uint32_t j0 = k * kDirectTile;
+            const bool masked = (j0 + kDirectTile > a.n) || (j0 < t0 + BT && t0 < j0 + kDirectTile);
+            if (!masked) {
+#pragma unroll 4
+                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                    const float4 s = tile[jj];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const float dx = s.x - px[r];
+                        const float dy = s.y - py[r];
+                        const float dz = s.z - pz[r];
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+                        const float inv = rsqrt_approx(r2);
+                        const float f = (s.w * inv) * (inv * inv);
+                        ax[r] = fmaf(f, dx, ax[r]);
+                        ay[r] = fmaf(f, dy, ay[r]);
+                        az[r] = fmaf(f, dz, az[r]);
+                    }
+                }
+            } else {
+                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                    const float4 s = tile[jj];
+                    const uint32_t j = j0 + jj;
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const uint32_t i = t0 + r * THREADS + tid;
+                        const bool skip = (j == i) || (j >= a.n);
+                        const float dx = s.x - px[r];
+                        const float dy = s.y - py[r];
+                        const float dz = s.z - pz[r];
+                        const float r2 =
+                            skip ? 1.0f : fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+                        const float w = skip ? 0.0f : s.w;
+                        const float inv = rsqrt_approx(r2);
+                        const float f = (w * inv) * (inv * inv);
+                        ax[r] = fmaf(f, dx, ax[r]);
+                        ay[r] = fmaf(f, dy, ay[r]);
+                        az[r] = fmaf(f, dz, az[r]);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && ok && k + 2 < te) {
+            fence_proxy_async_shared();
+            stage_tile<false>(a, tiles, nullptr, bars, k + 2, buf);
+        }
+    }
+
+    double sx[R], sy[R], sz[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        sx[r] = ax[r];
+        sy[r] = ay[r];
+        sz[r] = az[r];
+    }
+    finish_targets<THREADS, R, float>(a, t0, partial, sx, sy, sz);
+}
+
+// One Kahan step: (sum, c) += term, with c holding the negated lost low part.
+__device__ __forceinline__ void kahan_add(float &sum, float &c, float f, float d) {
+    const float y = fmaf(f, d, -c);
+    const float t = sum + y;
+    c = (t - sum) - y;
+    sum = t;
+}
+
+template <int THREADS, int R>
+__global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr uint32_t BT = THREADS * R;
+    float4 *tiles_hi = reinterpret_cast<float4 *>(smem);
+    float4 *tiles_lo = tiles_hi + 2 * kDirectTile;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 2 * kDirectTile);
+    double *partial = reinterpret_cast<double *>(bars + 2);
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t t0 = blockIdx.y * BT;
+    const float eps2 = a.eps2;
+
+    float hx[R], hy[R], hz[R], lx[R], ly[R], lz[R];
+    double sx[R], sy[R], sz[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        const float4 p = a.hi[t0 + r * THREADS + tid];
+        const float4 q = a.lo[t0 + r * THREADS + tid];
+        hx[r] = p.x;
+        hy[r] = p.y;
+        hz[r] = p.z;
+        lx[r] = q.x;
+        ly[r] = q.y;
+        lz[r] = q.z;
+        sx[r] = sy[r] = sz[r] = 0.0;
+    }
+
+    uint32_t tb, te;
+    source_tiles(a.n, gridDim.x, blockIdx.x, tb, te);
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (uint32_t k = tb; k < min(tb + 2, te); ++k) {
+            stage_tile<true>(a, tiles_hi, tiles_lo, bars, k, k - tb);
+        }
+    }
+
+    bool ok = true;
+    for (uint32_t k = tb; k < te; ++k) {
+        const uint32_t it = k - tb;
+        const uint32_t buf = it & 1u;
+        if (ok) {
+            ok = mbar_wait_bounded(&bars[buf], (it >> 1) & 1u, a.status);
+        }
+        if (ok) {
+            const float4 *th = tiles_hi + buf * kDirectTile;
+            const float4 *tl = tiles_lo + buf * kDirectTile;
+            const uint32_t j0 = k * kDirectTile;
+            const bool masked = (j0 + kDirectTile > a.n) || (j0 < t0 + BT && t0 < j0 + kDirectTile);
+            float kx[R], ky[R], kz[R], cx[R], cy[R], cz[R];
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                kx[r] = ky[r] = kz[r] = cx[r] = cy[r] = cz[r] = 0.0f;
+            }
+#pragma unroll 2
+            for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                const float4 s = th[jj];
+                const float4 l = tl[jj];
+                const uint32_t j = j0 + jj;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    // Coordinate differences from the split: the hi parts are
+                    // close, so their difference is exact or nearly; the lo
+                    // parts restore the bits FP32 positions would lose.
+                    const float dx = (s.x - hx[r]) + (l.x - lx[r]);
+                    const float dy = (s.y - hy[r]) + (l.y - ly[r]);
+                    const float dz = (s.z - hz[r]) + (l.z - lz[r]);
+                    float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+                    float w = s.w;
+                    if (masked) {
+                        const bool skip = (j == t0 + r * THREADS + tid) || (j >= a.n);
+                        r2 = skip ? 1.0f : r2;
+                        w = skip ? 0.0f : w;
+                    }
+                    // SFU estimate refined by one Newton-Raphson step,
+                    // y <- y + (y/2)(1 - r2 y^2), to about one ulp.
+                    float y = rsqrt_approx(r2);
+                    const float e = fmaf(-r2, y * y, 1.0f);
+                    y = fmaf(0.5f * y, e, y);
+                    const float f = (w * y) * (y * y);
+                    kahan_add(kx[r], cx[r], f, dx);
+                    kahan_add(ky[r], cy[r], f, dy);
+                    kahan_add(kz[r], cz[r], f, dz);
+                }
+            }
+            // Fold the tile's compensated FP32 partials into FP64.
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                sx[r] += static_cast<double>(kx[r]) - static_cast<double>(cx[r]);
+                sy[r] += static_cast<double>(ky[r]) - static_cast<double>(cy[r]);
+                sz[r] += static_cast<double>(kz[r]) - static_cast<double>(cz[r]);
+            }
+        }
+        __syncthreads();
+        if (tid == 0 && ok && k + 2 < te) {
+            fence_proxy_async_shared();
+            stage_tile<true>(a, tiles_hi, tiles_lo, bars, k + 2, buf);
+        }
+    }
+    finish_targets<THREADS, R, double>(a, t0, partial, sx, sy, sz);
+}
+
+// FP64 direct sum in the order of accumulate_range_scalar
+// (src/solvers/direct_kernel_scalar.cpp:31-59) with the split at i of
+// DirectSolver::evaluate (src/solvers/direct_solver.cpp:49-56): every operation
+// is an explicitly rounded FP64 intrinsic, so nothing is contracted and the
+// result is bit-identical to the reference's scalar kernel.
+constexpr int kF64Threads = 128;
+constexpr int kF64Tile = 256;
+
+__global__ void __launch_bounds__(kF64Threads)
+    direct_f64_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                      const double *__restrict__ z, const double *__restrict__ m, uint32_t n,
+                      double eps2, double *ax, double *ay, double *az) {
+    __shared__ double tx[kF64Tile], ty[kF64Tile], tz[kF64Tile], tm[kF64Tile];
+    const uint32_t i = blockIdx.x * kF64Threads + threadIdx.x;
+    const bool valid = i < n;
+    const double px = valid ? x[i] : 0.0;
+    const double py = valid ? y[i] : 0.0;
+    const double pz = valid ? z[i] : 0.0;
+    double bx = 0.0, by = 0.0, bz = 0.0; // sources before i
+    double fx = 0.0, fy = 0.0, fz = 0.0; // sources after i
+    for (uint32_t base = 0; base < n; base += kF64Tile) {
+        for (uint32_t k = threadIdx.x; k < kF64Tile; k += kF64Threads) {
+            const uint32_t j = base + k;
+            tx[k] = j < n ? x[j] : 0.0;
+            ty[k] = j < n ? y[j] : 0.0;
+            tz[k] = j < n ? z[j] : 0.0;
+            tm[k] = j < n ? m[j] : 0.0;
+        }
+        __syncthreads();
+        const uint32_t count = min(static_cast<uint32_t>(kF64Tile), n - base);
+        for (uint32_t k = 0; k < count; ++k) {
+            const uint32_t j = base + k;
+            if (j == i) {
+                continue;
+            }
+            const double dx = __dsub_rn(tx[k], px);
+            const double dy = __dsub_rn(ty[k], py);
+            const double dz = __dsub_rn(tz[k], pz);
+            const double s2 =
+                __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+            const double inv = __ddiv_rn(1.0, __dsqrt_rn(__dadd_rn(s2, eps2)));
+            const double f = __dmul_rn(tm[k], __dmul_rn(__dmul_rn(inv, inv), inv));
+            if (j < i) {
+                bx = __dadd_rn(bx, __dmul_rn(f, dx));
+                by = __dadd_rn(by, __dmul_rn(f, dy));
+                bz = __dadd_rn(bz, __dmul_rn(f, dz));
+            } else {
+                fx = __dadd_rn(fx, __dmul_rn(f, dx));
+                fy = __dadd_rn(fy, __dmul_rn(f, dy));
+                fz = __dadd_rn(fz, __dmul_rn(f, dz));
+            }
+        }
+        __syncthreads();
+    }
+    if (valid) {
+        ax[i] = __dadd_rn(bx, fx);
+        ay[i] = __dadd_rn(by, fy);
+        az[i] = __dadd_rn(bz, fz);
+    }
+}
+
+__global__ void pack_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                            const double *__restrict__ z, const double *__restrict__ m,
+                            uint32_t n, uint32_t padded, float4 *hi, float4 *lo) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < padded;
+         i += gridDim.x * blockDim.x) {
+        if (i < n) {
+            const double X = x[i], Y = y[i], Z = z[i];
+            const float hx = __double2float_rn(X);
+            const float hy = __double2float_rn(Y);
+            const float hz = __double2float_rn(Z);
+            hi[i] = make_float4(hx, hy, hz, __double2float_rn(m[i]));
+            if (lo != nullptr) {
+                // X - hx is exact in FP64; rounding it gives the low part.
+                lo[i] = make_float4(__double2float_rn(X - static_cast<double>(hx)),
+                                    __double2float_rn(Y - static_cast<double>(hy)),
+                                    __double2float_rn(Z - static_cast<double>(hz)), 0.0f);
+            }
+        } else {
+            hi[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (lo != nullptr) {
+                lo[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            }
+        }
+    }
+}
+
+template <int THREADS, int R, bool SPLIT> size_t direct_smem_bytes() {
+    const size_t tiles = (SPLIT ? 4 : 2) * kDirectTile * sizeof(float4);
+    const size_t partial = 3 * THREADS * R * (SPLIT ? sizeof(double) : sizeof(float));
+    return tiles + 2 * sizeof(uint64_t) + partial;
+}
+
+template <int THREADS, int R, bool SPLIT>
+cudaError_t launch_direct_t(const DirectArgs &args, int split, cudaStream_t stream) {
+    const uint32_t bt = THREADS * R;
+    const dim3 grid(static_cast<unsigned>(split), ceil_div(args.n, bt), 1);
+    const size_t smem = direct_smem_bytes<THREADS, R, SPLIT>();
+    auto kernel = SPLIT ? direct_split_kernel<THREADS, R> : direct_f32_kernel<THREADS, R>;
+    // Set once per process (one process drives one device), before any graph
+    // capture reaches this launch.
+    static const cudaError_t configured = cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (configured != cudaSuccess) {
+        return configured;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(THREADS, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = static_cast<unsigned>(split);
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, args);
+}
+
+template <bool SPLIT>
+cudaError_t dispatch_direct(const DirectArgs &args, const DirectConfig &c, cudaStream_t stream) {
+#define OB_DIRECT_CASE(T, RR)                                                                      \
+    if (c.threads == T && c.targets_per_thread == RR)                                              \
+        return launch_direct_t<T, RR, SPLIT>(args, c.split, stream);
+    OB_DIRECT_CASE(128, 1)
+    OB_DIRECT_CASE(128, 2)
+    OB_DIRECT_CASE(128, 4)
+    OB_DIRECT_CASE(256, 1)
+    OB_DIRECT_CASE(256, 2)
+    OB_DIRECT_CASE(256, 4)
+    if (!SPLIT) {
+        OB_DIRECT_CASE(128, 8)
+        OB_DIRECT_CASE(256, 8)
+    }
+#undef OB_DIRECT_CASE
+    return cudaErrorInvalidValue;
+}
+
+bool valid_split(int split) { return split == 1 || split == 2 || split == 4 || split == 8; }
+
+} // namespace
+
+uint32_t direct_padded_count(uint32_t n, const DirectConfig &config) {
+    const uint32_t bt = static_cast<uint32_t>(config.threads * config.targets_per_thread);
+    const uint32_t unit = bt > kDirectTile ? bt : kDirectTile;
+    const uint32_t padded = ceil_div(n, unit) * unit;
+    return padded == 0 ? unit : padded;
+}
+
+cudaError_t pack_sources(const double *x, const double *y, const double *z, const double *m,
+                         uint32_t n, uint32_t padded, float4 *hi, float4 *lo,
+                         cudaStream_t stream) {
+    if (padded == 0) {
+        return cudaSuccess;
+    }
+    const uint32_t threads = 256;
+    const uint32_t blocks = min(ceil_div(padded, threads), 148u * 16u);
+    pack_kernel<<<blocks, threads, 0, stream>>>(x, y, z, m, n, padded, hi, lo);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_direct_f32(const float4 *sources, uint32_t n, uint32_t padded, float eps2,
+                              double *ax, double *ay, double *az, const DirectConfig &config,
+                              unsigned *status, cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    if (!valid_split(config.split) || padded < direct_padded_count(n, config)) {
+        return cudaErrorInvalidValue;
+    }
+    const DirectArgs args{sources, nullptr, n, padded, eps2, ax, ay, az, status};
+    return dispatch_direct<false>(args, config, stream);
+}
+
+cudaError_t launch_direct_split(const float4 *hi, const float4 *lo, uint32_t n, uint32_t padded,
+                                float eps2, double *ax, double *ay, double *az,
+                                const DirectConfig &config, unsigned *status,
+                                cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    if (!valid_split(config.split) || padded < direct_padded_count(n, config)) {
+        return cudaErrorInvalidValue;
+    }
+    const DirectArgs args{hi, lo, n, padded, eps2, ax, ay, az, status};
+    return dispatch_direct<true>(args, config, stream);
+}
+
+cudaError_t launch_direct_f64(const double *x, const double *y, const double *z, const double *m,
+                              uint32_t n, double eps2, double *ax, double *ay, double *az,
+                              cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    direct_f64_kernel<<<ceil_div(n, kF64Threads), kF64Threads, 0, stream>>>(x, y, z, m, n, eps2,
+                                                                          ax, ay, az);
+    return cudaGetLastError();
+}
+
+int direct_candidates(bool split, DirectConfig *out, int capacity) {
+    static const int shapes[][2] = {{128, 1}, {128, 2}, {128, 4}, {256, 1},
+                                    {256, 2}, {256, 4}, {128, 8}, {256, 8}};
+    const int shape_count = split ? 6 : 8;
+    static const int splits[] = {1, 2, 4, 8};
+    int count = 0;
+    for (int s = 0; s < shape_count; ++s) {
+        for (int k = 0; k < 4; ++k) {
+            if (count < capacity) {
+                out[count] = DirectConfig{shapes[s][0], shapes[s][1], splits[k]};
+            }
+            ++count;
+        }
+    }
+    return count;
+}
+
+DirectConfig direct_default_config(uint32_t n, bool split, int sm_count) {
+    DirectConfig c;
+    c.threads = split ? 128 : 256;
+    c.targets_per_thread = split ? 2 : 4;
+    // Shrink the target tile until the targets alone give every SM work.
+    const uint32_t want = static_cast<uint32_t>(sm_count > 0 ? sm_count : 148) * 2u;
+    while (c.targets_per_thread > 1 &&
+           ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread)) < want) {
+        c.targets_per_thread /= 2;
+    }
+    if (c.threads > 128 && ceil_div(n, static_cast<uint32_t>(c.threads)) < want) {
+        c.threads = 128;
+    }
+    // Then split the sources across a cluster for what is still missing.
+    const uint32_t blocks = ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread));
+    const uint32_t tiles = ceil_div(n, kDirectTile);
+    while (c.split < 8 && blocks * static_cast<uint32_t>(c.split) < want &&
+           static_cast<uint32_t>(c.split * 2) <= tiles) {
+        c.split *= 2;
+    }
+    return c;
+}
+
+} // namespace ob

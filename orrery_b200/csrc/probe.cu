@@ -1,0 +1,112 @@
+// Throughput probes for the direct kernel's roofline: FP32 FFMA lane
+// operations per second and SFU reciprocal-square-root lane operations per
+// second, measured on the device this process runs on. The reference measures
+// its ceilings the same way rather than quoting a data sheet
+// (benchmarks/cuda_probes.cu:15-115).
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+#include "orrery_b200.h"
+#include "runtime.hpp"
+
+namespace ob {
+namespace {
+
+constexpr int kChains = 8;
+constexpr int kProbeThreads = 256;
+
+__global__ void __launch_bounds__(kProbeThreads) ffma_probe(float *out, int iterations, float a,
+                                                            float b) {
+    float v[kChains];
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        v[k] = threadIdx.x * 1e-3f + k;
+    }
+    for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+        for (int k = 0; k < kChains; ++k) {
+            v[k] = fmaf(v[k], a, b);
+        }
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        s += v[k];
+    }
+    if (s == 12345.678f) {
+        out[threadIdx.x] = s;
+    }
+}
+
+__global__ void __launch_bounds__(kProbeThreads) rsqrt_probe(float *out, int iterations) {
+    float v[kChains];
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        v[k] = 1.0f + threadIdx.x * 1e-3f + k;
+    }
+    for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+        for (int k = 0; k < kChains; ++k) {
+            v[k] = rsqrt_approx(v[k]);
+        }
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        s += v[k];
+    }
+    if (s == 12345.678f) {
+        out[threadIdx.x] = s;
+    }
+}
+
+template <typename Launch> double lane_ops_per_second(Launch launch, double ops) {
+    cudaEvent_t a, b;
+    check(cudaEventCreate(&a), "probe event");
+    check(cudaEventCreate(&b), "probe event");
+    launch();
+    check(cudaGetLastError(), "probe launch");
+    check(cudaEventRecord(a), "probe event");
+    launch();
+    check(cudaEventRecord(b), "probe event");
+    check(cudaEventSynchronize(b), "probe");
+    float ms = 0.0f;
+    check(cudaEventElapsedTime(&ms, a, b), "probe timing");
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ops / (ms * 1e-3);
+}
+
+} // namespace
+} // namespace ob
+
+extern "C" int ob_probe_fp32(double *ffma_lane_per_s, double *rsqrt_lane_per_s) {
+    try {
+        int device = 0, sms = 0;
+        ob::check(cudaGetDevice(&device), "cudaGetDevice");
+        ob::check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SMs");
+        float *sink = nullptr;
+        ob::check(cudaMalloc(&sink, ob::kProbeThreads * sizeof(float)), "probe buffer");
+        const int blocks = sms * 8;
+        const double threads = static_cast<double>(blocks) * ob::kProbeThreads;
+        const int fma_iterations = 1 << 16;
+        const int rsq_iterations = 1 << 13;
+        if (ffma_lane_per_s != nullptr) {
+            *ffma_lane_per_s = ob::lane_ops_per_second(
+                [&] {
+                    ob::ffma_probe<<<blocks, ob::kProbeThreads>>>(sink, fma_iterations, 0.999f,
+                                                                  1e-3f);
+                },
+                threads * fma_iterations * ob::kChains);
+        }
+        if (rsqrt_lane_per_s != nullptr) {
+            *rsqrt_lane_per_s = ob::lane_ops_per_second(
+                [&] { ob::rsqrt_probe<<<blocks, ob::kProbeThreads>>>(sink, rsq_iterations); },
+                threads * rsq_iterations * ob::kChains);
+        }
+        cudaFree(sink);
+        return OB_OK;
+    } catch (const ob::Error &e) {
+        return ob::set_error(e.code(), e.what());
+    }
+}

@@ -1,0 +1,82 @@
+// A particle system resident in HBM, integrated on the device.
+//
+// The device counterpart of sim::Simulation's state handling
+// (src/sim/simulation.cpp:16-70): positions, velocities, accelerations and
+// masses as ten FP64 SoA arrays that never leave the device between steps.
+// One integrator step is captured once as a CUDA graph and replayed.
+#pragma once
+
+#include <cstdint>
+#include <memory>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "runtime.hpp"
+#include "solver.hpp"
+
+namespace ob {
+
+class System {
+public:
+    enum Array { kX = 0, kY, kZ, kVx, kVy, kVz, kAx, kAy, kAz, kM };
+
+    System(const ob_solver_params &params, uint32_t n);
+    ~System();
+    System(const System &) = delete;
+    System &operator=(const System &) = delete;
+
+    void set_state(const double *x, const double *y, const double *z, const double *vx,
+                   const double *vy, const double *vz, const double *m);
+    void set_accelerations(const double *ax, const double *ay, const double *az);
+    void get_state(double *const *out); // x y z vx vy vz ax ay az, NULL entries skipped
+    void refresh();
+    void step_async(int integrator, double dt, uint64_t steps);
+    void synchronize();
+    void energy(double *kinetic, double *potential);
+
+    [[nodiscard]] Solver &solver() noexcept { return *solver_; }
+    [[nodiscard]] uint32_t size() const noexcept { return n_; }
+    [[nodiscard]] double *array(int k) const noexcept {
+        return state_.data() + static_cast<size_t>(k) * n_;
+    }
+    [[nodiscard]] cudaStream_t stream() const noexcept { return stream_; }
+
+    static int evaluations_per_step(int integrator);
+
+    // Per-phase timing of graph replays (see ob_system_profile).
+    void profile(uint32_t steps);
+    ob_timings phase_times(uint32_t &evaluations);
+    uint32_t step_kernels(int integrator, double dt);
+
+private:
+    void upload(int first, int count, const double *const *host);
+    void evaluate(bool count, const cudaEvent_t *marks = nullptr);
+    void enqueue_substep(double timestep, const cudaEvent_t *marks);
+    void enqueue_step(int integrator, double dt);
+    void drop_graph();
+    void ensure_graph(int integrator, double dt);
+    void set_marks(const std::vector<cudaEvent_t> &events, size_t offset);
+
+    std::unique_ptr<Solver> solver_;
+    uint32_t n_;
+    DeviceArray<double> state_;
+    DeviceArray<double> terms_;
+    cudaStream_t stream_ = nullptr;
+    cudaGraph_t template_ = nullptr;  // kept so its event nodes can be retargeted
+    cudaGraphExec_t graph_ = nullptr;
+    int graph_integrator_ = -1;
+    double graph_dt_ = 0.0;
+    uint32_t graph_kernels_ = 0;
+
+    // Four placeholder events per evaluation of a step, captured as event
+    // nodes; before a profiled replay they are pointed at a fresh slot of ring_.
+    std::vector<cudaEvent_t> marks_;
+    std::vector<cudaGraphNode_t> mark_nodes_;
+    std::vector<cudaEvent_t> ring_;
+    uint32_t ring_steps_ = 0;     // capacity in steps
+    uint32_t ring_used_ = 0;      // steps recorded
+    bool marks_retargeted_ = false;
+};
+
+} // namespace ob

@@ -1,0 +1,99 @@
+"""Host-side checks of the C ABI that need no GPU: the library loads, exports
+every symbol the headers declare, validates arguments, and reports "no device"
+as the try_create contract asks (src/solvers/cuda_direct_solver.cpp:140-164)."""
+from __future__ import annotations
+
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+import pytest
+
+import orrery_b200 as ob
+from orrery_b200 import initial_conditions as ic
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = set()
+    for header in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(header).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for match in re.finditer(r"\b(ob_[a-z0-9_]+)\s*\(", text):
+            names.add(match.group(1))
+    return sorted(names)
+
+
+@pytest.fixture(scope="module")
+def lib():
+    if not os.path.exists(ob.library_path()):
+        from orrery_b200 import build
+        build.build()
+    return ob.load_library()
+
+
+def test_every_declared_symbol_is_exported(lib):
+    names = declared_symbols()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_version_and_error_text(lib):
+    assert "sm_100a" in ob.version()
+    assert isinstance(lib.ob_last_error(), bytes)
+
+
+def test_invalid_parameters_are_rejected_before_the_device(lib):
+    handle = C.c_void_p()
+    bad = ob.make_params(kind=7)
+    assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
+    assert handle.value is None
+    bad = ob.make_params(softening=-1.0)
+    assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
+    bad = ob.make_params(kind=ob.SOLVER_TREE, precision="fp64")
+    assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_UNSUPPORTED
+    assert lib.ob_solver_create(None, C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
+
+
+def test_null_handles_are_errors_not_crashes(lib):
+    counts = ob.Counts()
+    assert lib.ob_solver_counts(None, C.byref(counts)) == ob.ERROR_INVALID_ARGUMENT
+    assert lib.ob_system_step(None, 0, 1e-3, 1) == ob.ERROR_INVALID_ARGUMENT
+    lib.ob_solver_destroy(None)
+    lib.ob_system_destroy(None)
+
+
+def test_try_create_without_a_device_returns_none(lib):
+    if ob.device_count() > 0:
+        pytest.skip("a device is present; the no-device contract is tested without one")
+    assert ob.B200DirectSolver.try_create(0.01) is None
+    assert ob.B200TreeSolver.try_create(0.01) is None
+    handle = C.c_void_p()
+    params = ob.make_params()
+    assert lib.ob_system_create(C.byref(params), 16, C.byref(handle)) == ob.ERROR_NO_DEVICE
+
+
+def test_plummer_generator_is_seeded_and_centred():
+    a = ic.plummer_sphere(3000, seed=7)
+    b = ic.plummer_sphere(3000, seed=7)
+    c = ic.plummer_sphere(3000, seed=8)
+    assert np.array_equal(a["x"], b["x"]) and not np.array_equal(a["x"], c["x"])
+    assert abs(a["m"].sum() - 1.0) < 1e-12
+    com = np.array([(a[k] * a["m"]).sum() for k in ("x", "y", "z")])
+    assert np.all(np.abs(com) < 1e-12)
+    # Half-mass radius of a Plummer sphere: a / sqrt(2^{2/3} - 1) ~ 1.305 a.
+    r = np.sqrt(a["x"] ** 2 + a["y"] ** 2 + a["z"] ** 2)
+    assert 1.15 < np.median(r) < 1.45
+
+
+def test_collision_generator_geometry():
+    g = ic.galaxy_collision(20000, seed=3)
+    assert len(g["x"]) == 20000
+    assert abs(g["m"].sum() - 1.0) < 1e-12
+    assert np.allclose(g["m"], g["m"][0])
+    b = ic.collision_impact_parameter(1.0, 20.0, 0.8, 3.0)
+    assert 0 < b < 20

@@ -1,0 +1,150 @@
+"""Direct solver on the GPU against the oracle and the reference's outputs.
+
+Restates the contract of the reference's CUDA direct tests
+(tests/solvers/cuda_direct_solver_test.cpp) with this backend swapped in:
+FP32 bounds against the compensated reference (worst < 2e-4, RMS < 2e-5),
+counters N(N-1), empty/single inputs, the origin-padding known answer. The
+FP64 form is held to bit equality with the reference's scalar DirectSolver and
+the split precision form to a per-particle relative error of 1e-6.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import relative_errors
+
+pytestmark = pytest.mark.gpu
+
+# Tolerances (per-particle relative error |a - a_ref| / |a_ref|).
+FP32_WORST, FP32_RMS = 2e-4, 2e-5        # cuda_direct_solver_test.cpp:122-151 (FP32 build)
+SPLIT_WORST, SPLIT_MEDIAN = 1e-6, 1e-7   # the precision form's stated target
+
+
+def _xyzm(d):
+    return d["x"], d["y"], d["z"], d["m"]
+
+
+def test_fp64_is_bit_identical_to_reference(b200, golden_plummer):
+    g = golden_plummer
+    for eps in (0.01, 0.05):
+        s = b200.B200DirectSolver(eps, "fp64")
+        a = s.evaluate((g["x"], g["y"], g["z"]), g["m"])
+        assert np.array_equal(a, g[f"direct_eps{eps}"])
+        assert s.interaction_count().particle_particle == 2048 * 2047
+
+
+def test_fp32_within_reference_bounds(b200, restatement, golden_plummer):
+    g = golden_plummer
+    x, y, z, m = _xyzm(g)
+    exact = restatement.reference_accelerations(x, y, z, m, 0.05)
+    a = b200.B200DirectSolver(0.05, "fp32").evaluate((x, y, z), m)
+    err = relative_errors(a, exact)
+    assert err.max() < FP32_WORST
+    assert np.sqrt(np.mean(err ** 2)) < FP32_RMS
+    # Against the CPU solver (cuda_direct_solver_test.cpp:154-192): 2x the bound.
+    assert relative_errors(a, g["direct_eps0.05"]).max() < 2 * FP32_WORST
+
+
+def test_split_precision_meets_its_target(b200, golden_plummer):
+    g = golden_plummer
+    x, y, z, m = _xyzm(g)
+    a = b200.B200DirectSolver(0.01, "split").evaluate((x, y, z), m)
+    err = relative_errors(a, g["direct_eps0.01"])
+    assert err.max() < SPLIT_WORST, err.max()
+    assert np.median(err) < SPLIT_MEDIAN, np.median(err)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "split", "fp64"])
+def test_pair_known_answer(b200, precision):
+    a = b200.B200DirectSolver(0.0, precision).evaluate(
+        (np.array([-1.0, 1.0]), np.zeros(2), np.zeros(2)), np.array([2.0, 3.0]))
+    tol = 0.0 if precision == "fp64" else 1e-6
+    assert np.allclose(a, [[0.75, 0, 0], [-0.5, 0, 0]], rtol=0, atol=tol)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "split", "fp64"])
+def test_origin_particle_survives_padding(b200, precision):
+    # cuda_direct_solver_test.cpp:296-337: unsoftened, a particle at the origin
+    # next to zero-mass padding must get exactly (1, 1/4, 0).
+    a = b200.B200DirectSolver(0.0, precision).evaluate(
+        (np.array([0.0, 1.0, 0.0]), np.array([0.0, 0.0, 2.0]), np.zeros(3)), np.ones(3))
+    assert np.all(np.isfinite(a))
+    tol = 1e-14 if precision == "fp64" else 1e-6
+    assert abs(a[0, 0] - 1.0) < tol and abs(a[0, 1] - 0.25) < tol and abs(a[0, 2]) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp32", "split", "fp64"])
+def test_empty_and_single(b200, precision):
+    s = b200.B200DirectSolver(0.1, precision)
+    assert s.evaluate((np.zeros(0), np.zeros(0), np.zeros(0)), np.zeros(0)).shape == (0, 3)
+    a = s.evaluate((np.ones(1), np.ones(1), np.ones(1)), np.ones(1))
+    assert a.tolist() == [[0.0, 0.0, 0.0]]
+    c = s.interaction_count()
+    assert c.evaluations == 2 and c.particle_particle == 0
+
+
+@pytest.mark.parametrize("n", [2, 3, 31, 33, 511, 513, 1023, 1025, 4097])
+def test_ragged_sizes_against_oracle(b200, restatement, n):
+    from orrery_b200 import initial_conditions as ic
+    d = ic.plummer_sphere(n, seed=100 + n)
+    x, y, z, m = _xyzm(d)
+    exact, _ = restatement.direct(x, y, z, m, 0.02)
+    for precision, bound in (("fp32", 5e-4), ("split", 2e-6)):
+        a = b200.B200DirectSolver(0.02, precision).evaluate((x, y, z), m)
+        assert relative_errors(a, exact).max() < bound, (precision, n)
+    a = b200.B200DirectSolver(0.02, "fp64").evaluate((x, y, z), m)
+    assert np.array_equal(a, exact)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "split"])
+def test_every_kernel_shape_computes_the_same_sum(b200, golden_plummer, precision):
+    g = golden_plummer
+    x, y, z, m = _xyzm(g)
+    s = b200.B200DirectSolver(0.05, precision)
+    results = []
+    for shape in b200.direct_shapes(precision):
+        s.set_shape(len(m), shape)
+        results.append(s.evaluate((x, y, z), m))
+    ref = g["direct_eps0.05"]
+    bound = 2 * FP32_WORST if precision == "fp32" else SPLIT_WORST
+    for a in results:
+        assert relative_errors(a, ref).max() < bound
+    # Splitting the sources changes only the order of a few partial sums.
+    spread = max(relative_errors(a, results[0]).max() for a in results)
+    assert spread < (1e-5 if precision == "fp32" else 1e-7)
+
+
+def test_autotune_picks_a_working_shape(b200, golden_plummer):
+    g = golden_plummer
+    s = b200.B200DirectSolver(0.05, "fp32")
+    shape, ms = s.autotune(len(g["m"]))
+    assert shape in b200.direct_shapes("fp32") and ms > 0
+    a = s.evaluate((g["x"], g["y"], g["z"]), g["m"])
+    assert relative_errors(a, g["direct_eps0.05"]).max() < 2 * FP32_WORST
+
+
+def test_momentum_is_conserved_at_scale(b200):
+    # A size-independent property at the precision form's full size (262,144):
+    # sum_i m_i a_i = 0 up to rounding (conservation_test.cpp:135-180).
+    from orrery_b200 import initial_conditions as ic
+    d = ic.plummer_sphere(262144, seed=20260811)
+    x, y, z, m = _xyzm(d)
+    for precision, bound in (("fp32", 1e-4), ("split", 1e-7)):
+        a = b200.B200DirectSolver(0.01, precision).evaluate((x, y, z), m)
+        net = np.abs((a * m[:, None]).sum(axis=0)).max()
+        scale = (np.linalg.norm(a, axis=1) * m).sum()
+        assert net / scale < bound, (precision, net / scale)
+
+
+def test_device_pointer_entry_point(b200, golden_plummer):
+    torch = pytest.importorskip("torch")
+    g = golden_plummer
+    dev = torch.device("cuda:0")
+    ins = [torch.tensor(g[k], dtype=torch.float64, device=dev) for k in ("x", "y", "z", "m")]
+    outs = [torch.empty(len(g["m"]), dtype=torch.float64, device=dev) for _ in range(3)]
+    s = b200.B200DirectSolver(0.01, "fp64")
+    s.evaluate_device(len(g["m"]), *ins, *outs, stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    a = torch.stack(outs, dim=1).cpu().numpy()
+    assert np.array_equal(a, g["direct_eps0.01"])

@@ -1,0 +1,121 @@
+"""Device-resident integration against the reference's integrators.
+
+With the FP64 direct field the device kick/drift and force are bit-identical
+to the reference's host VelocityVerlet / Yoshida4 over DirectSolver, so whole
+trajectories are compared for equality (tests/golden/trajectory_512.npz holds
+the reference's own output). The FP32 and split fields are compared through
+energy behaviour, as the reference's integrator tests do
+(tests/integrators/energy_behaviour_test.cpp, conservation_test.cpp).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+
+
+def _system(b200, g, precision, eps=0.01):
+    n = len(g["m"])
+    s = b200.DeviceSystem(n, eps, precision=precision)
+    s.set_state(g["start_x"], g["start_y"], g["start_z"], g["start_vx"], g["start_vy"],
+                g["start_vz"], g["m"])
+    return s
+
+
+@pytest.mark.parametrize("integrator,steps,tag", [("vv", 20, "vv20"), ("yoshida4", 10, "y4_10")])
+def test_fp64_trajectory_is_bit_identical(b200, golden_trajectory, integrator, steps, tag):
+    g = golden_trajectory
+    s = _system(b200, g, "fp64")
+    # The reference carried its own starting accelerations; they equal ours.
+    st = s.state()
+    for k in ("ax", "ay", "az"):
+        assert np.array_equal(st[k], g[f"start_{k}"])
+    s.step(1e-3, steps, integrator)
+    st = s.state()
+    for k in KEYS:
+        assert np.array_equal(st[k], g[f"{tag}_{k}"]), k
+    c = s.interaction_count()
+    per = 3 if integrator == "yoshida4" else 1
+    assert c.evaluations == 1 + steps * per
+    assert c.particle_particle == c.evaluations * 512 * 511
+
+
+def test_steps_split_across_calls_equal_one_call(b200, golden_trajectory):
+    g = golden_trajectory
+    a = _system(b200, g, "fp64")
+    a.step(1e-3, 20, "vv")
+    b = _system(b200, g, "fp64")
+    for _ in range(4):
+        b.step_async(1e-3, 5, "vv")
+    b.synchronize()
+    sa, sb = a.state(), b.state()
+    assert all(np.array_equal(sa[k], sb[k]) for k in KEYS)
+
+
+def test_energies_are_bit_identical(b200, golden_plummer):
+    g = golden_plummer
+    s = b200.DeviceSystem(len(g["m"]), 0.01, precision="fp64")
+    s.set_state(g["x"], g["y"], g["z"], g["vx"], g["vy"], g["vz"], g["m"])
+    ke, pe = s.energy()
+    assert pe == float(g["pe_eps0.01"])
+    assert ke == float(g["ke"])
+
+
+def test_c1_energy_and_forces_against_reference(b200, restatement):
+    # Plummer N=4096, eps 0.01, velocity Verlet dt 1e-3, 100 steps: FP32 device
+    # forces against the oracle's FP64 run of the same steps.
+    from orrery_b200 import initial_conditions as ic
+    d = ic.plummer_sphere(4096, seed=20260811)
+    x, y, z, m = d["x"], d["y"], d["z"], d["m"]
+    a0, _ = restatement.direct(x, y, z, m, 0.01)
+    start = dict(x=x, y=y, z=z, vx=d["vx"], vy=d["vy"], vz=d["vz"], ax=a0[:, 0].copy(),
+                 ay=a0[:, 1].copy(), az=a0[:, 2].copy())
+    e0 = restatement.kinetic_energy(d["vx"], d["vy"], d["vz"], m) + \
+        restatement.potential_energy(x, y, z, m, 0.01)
+    ref, _ = restatement.integrate_direct(start, m, 0.01, 1e-3, 100, "vv")
+    e_ref = restatement.kinetic_energy(ref["vx"], ref["vy"], ref["vz"], m) + \
+        restatement.potential_energy(ref["x"], ref["y"], ref["z"], m, 0.01)
+    for precision in ("fp32", "split"):
+        s = b200.DeviceSystem(4096, 0.01, precision=precision)
+        s.set_state(x, y, z, d["vx"], d["vy"], d["vz"], m)
+        s.step(1e-3, 100, "vv")
+        ke, pe = s.energy()
+        drift_dev = (ke + pe - e0) / abs(e0)
+        drift_ref = (e_ref - e0) / abs(e0)
+        assert abs(drift_dev - drift_ref) < (1e-6 if precision == "fp32" else 1e-9), precision
+        st = s.state()
+        pos_err = np.max(np.abs(st["x"] - ref["x"]))
+        assert pos_err < (1e-5 if precision == "fp32" else 1e-9), (precision, pos_err)
+
+
+def test_momentum_conserved_over_steps(b200):
+    # tests/integrators/conservation_test.cpp:94-123: 64 bodies, 200 steps,
+    # dt 1e-3, eps 0.03; momentum to 64 * steps * machine epsilon * scale.
+    from orrery_b200 import initial_conditions as ic
+    d = ic.plummer_sphere(64, seed=9)
+    s = b200.DeviceSystem(64, 0.03, precision="fp64")
+    s.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+    s.step(1e-3, 200, "vv")
+    st = s.state()
+    p = np.array([(st[k] * d["m"]).sum() for k in ("vx", "vy", "vz")])
+    scale = (np.sqrt(st["vx"] ** 2 + st["vy"] ** 2 + st["vz"] ** 2) * d["m"]).sum()
+    assert np.abs(p).max() <= 64 * 200 * np.finfo(float).eps * scale
+
+
+def test_yoshida_energy_error_below_velocity_verlet(b200):
+    # energy_behaviour_test.cpp:137-176: Yoshida-4's energy error is below VV's
+    # at the same timestep.
+    from orrery_b200 import initial_conditions as ic
+    d = ic.plummer_sphere(1024, seed=11)
+    errs = {}
+    for integ in ("vv", "yoshida4"):
+        s = b200.DeviceSystem(1024, 0.05, precision="fp64")
+        s.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+        ke0, pe0 = s.energy()
+        s.step(1e-2, 50, integ)
+        ke, pe = s.energy()
+        errs[integ] = abs((ke + pe) - (ke0 + pe0)) / abs(ke0 + pe0)
+    assert errs["yoshida4"] < errs["vv"]
