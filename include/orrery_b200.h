@@ -123,6 +123,21 @@ int ob_solver_counts(ob_solver *solver, ob_counts *counts);
 int ob_solver_reset_counts(ob_solver *solver);
 int ob_solver_timings(const ob_solver *solver, ob_timings *timings);
 
+/* Inspection of the last tree evaluation: the Morton order and the octree as
+ * the reference lays them out (MortonOrdering::keys, Octree::nodes /
+ * quadrupoles / leaf_count / depth; include/orrery/solvers/morton.hpp:182-210,
+ * octree.hpp:208-248). Synchronous; for tests and tools. */
+int ob_tree_stats(ob_solver *solver, uint64_t *nodes, uint64_t *leaves, uint32_t *depth);
+
+/* reals: 5 doubles per node (mass, centre of mass x y z, acceptance radius^2);
+ * idx: 3 per node (next, first particle, particle count); quads: 6 per node
+ * (xx xy xz yy yz zz) or NULL. Arrays must hold ob_tree_stats' node count. */
+int ob_tree_copy(ob_solver *solver, double *reals, uint64_t *idx, double *quads);
+
+/* codes and indices of the sorted keys (n each), the cube origin (3) and size. */
+int ob_tree_copy_order(ob_solver *solver, uint64_t *codes, uint32_t *indices, double *origin,
+                       double *size);
+
 /* Tile shape of the direct kernels: threads per CTA, targets per thread and
  * the number of CTAs (one thread-block cluster) that split the sources of a
  * target tile. No reference counterpart: the reference picks one block size

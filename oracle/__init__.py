@@ -104,6 +104,9 @@ class Restatement:
         lib.oc_tree_free.argtypes = [C.POINTER(_Tree)]
         lib.oc_barnes_hut.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, C.c_double,
                                       C.c_uint64, C.c_int, _dp, _dp, _dp, C.POINTER(Counts)]
+        lib.oc_barnes_hut_targets.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double,
+                                              C.c_double, C.c_uint64, C.c_int, C.c_size_t,
+                                              _u64p, _dp, _u64p, _u64p]
         for name in ("oc_vv_step_direct", "oc_yoshida_step_direct"):
             getattr(lib, name).argtypes = [C.c_size_t] + [_dp] * 10 + [C.c_double, C.c_double,
                                                                        C.POINTER(Counts)]
@@ -203,6 +206,22 @@ class Restatement:
         if rc != 0:
             raise MemoryError("oracle Barnes-Hut failed")
         return np.stack(a, axis=1), counts
+
+    def barnes_hut_targets(self, x, y, z, m, softening, opening_angle, leaf_capacity,
+                           quadrupole, targets):
+        """Accelerations (k, 3), pair and cell counts of the listed targets only."""
+        t = np.ascontiguousarray(targets, dtype=np.uint64)
+        k = len(t)
+        acc = np.zeros((k, 3))
+        pairs = np.zeros(k, np.uint64)
+        cells = np.zeros(k, np.uint64)
+        rc = self.lib.oc_barnes_hut_targets(len(m), _d(x), _d(y), _d(z), _d(m), softening,
+                                            opening_angle, leaf_capacity,
+                                            1 if quadrupole else 0, k, _u(t), _d(acc),
+                                            _u(pairs), _u(cells))
+        if rc != 0:
+            raise MemoryError("oracle Barnes-Hut failed")
+        return acc, pairs, cells
 
     # -- integrators and energies -------------------------------------------
     def integrate_direct(self, state, m, softening, dt, steps, integrator="vv"):

@@ -593,6 +593,57 @@ done:
     return rc;
 }
 
+int oc_barnes_hut_targets(size_t n, const double *x, const double *y, const double *z,
+                          const double *m, double softening, double opening_angle,
+                          uint64_t leaf_capacity, int quadrupole, size_t count,
+                          const uint64_t *targets, double *acc, uint64_t *pairs,
+                          uint64_t *cells) {
+    const size_t alloc = n ? n : 1;
+    uint64_t *codes = (uint64_t *)malloc(alloc * sizeof(uint64_t));
+    uint64_t *index = (uint64_t *)malloc(alloc * sizeof(uint64_t));
+    uint64_t *where = (uint64_t *)malloc(alloc * sizeof(uint64_t));
+    double *sx = (double *)malloc(alloc * sizeof(double));
+    double *sy = (double *)malloc(alloc * sizeof(double));
+    double *sz = (double *)malloc(alloc * sizeof(double));
+    double *sm = (double *)malloc(alloc * sizeof(double));
+    int rc = 0;
+    if (!codes || !index || !where || !sx || !sy || !sz || !sm) {
+        rc = -1;
+        goto done;
+    }
+    double origin[3], size;
+    oc_morton_order(n, x, y, z, codes, index, origin, &size);
+    for (size_t i = 0; i < n; ++i) {
+        sx[i] = x[index[i]];
+        sy[i] = y[index[i]];
+        sz[i] = z[index[i]];
+        sm[i] = m[index[i]];
+        where[index[i]] = i;
+    }
+    oc_tree tree;
+    if (oc_tree_build(n, sx, sy, sz, sm, codes, origin, size, opening_angle, leaf_capacity,
+                      quadrupole, &tree) != 0) {
+        rc = -1;
+        goto done;
+    }
+    for (size_t k = 0; k < count; ++k) {
+        uint64_t p = 0, c = 0;
+        oc_walk(&tree, n, sx, sy, sz, sm, where[targets[k]], softening, acc + 3 * k, &p, &c);
+        pairs[k] = p;
+        cells[k] = c;
+    }
+    oc_tree_free(&tree);
+done:
+    free(codes);
+    free(index);
+    free(where);
+    free(sx);
+    free(sy);
+    free(sz);
+    free(sm);
+    return rc;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Integrators (velocity_verlet.cpp:20-72, yoshida4.cpp:24-59)                 */
 /* ------------------------------------------------------------------------- */

@@ -106,6 +106,15 @@ int oc_barnes_hut(size_t n, const double *x, const double *y, const double *z, c
                   double softening, double opening_angle, uint64_t leaf_capacity, int quadrupole,
                   double *ax, double *ay, double *az, oc_counts *counts);
 
+/* BarnesHutSolver::evaluate restricted to some targets (original indices):
+ * the full ordering and tree, then walk_tree for each listed target only.
+ * Writes 3 accelerations and the pair and cell counts per target. */
+int oc_barnes_hut_targets(size_t n, const double *x, const double *y, const double *z,
+                          const double *m, double softening, double opening_angle,
+                          uint64_t leaf_capacity, int quadrupole, size_t count,
+                          const uint64_t *targets, double *acc, uint64_t *pairs,
+                          uint64_t *cells);
+
 /* velocity_verlet_step (velocity_verlet.cpp:59-72) with the direct field. */
 void oc_vv_step_direct(size_t n, double *x, double *y, double *z, double *vx, double *vy,
                        double *vz, double *ax, double *ay, double *az, const double *m,

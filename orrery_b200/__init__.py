@@ -134,6 +134,10 @@ def load_library():
     lib.ob_system_counts.argtypes = [vp, C.POINTER(Counts)]
     lib.ob_system_size.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.ob_probe_fp32.argtypes = [_dp, _dp]
+    _u64p = C.POINTER(C.c_uint64)
+    lib.ob_tree_stats.argtypes = [vp, _u64p, _u64p, C.POINTER(C.c_uint32)]
+    lib.ob_tree_copy.argtypes = [vp, _dp, _u64p, _dp]
+    lib.ob_tree_copy_order.argtypes = [vp, _u64p, C.POINTER(C.c_uint32), _dp, _dp]
     lib.ob_system_stream.argtypes = [vp, C.POINTER(vp)]
     lib.ob_system_profile.argtypes = [vp, C.c_uint32]
     lib.ob_system_phase_times.argtypes = [vp, C.POINTER(Timings), C.POINTER(C.c_uint32)]
@@ -292,6 +296,37 @@ class B200TreeSolver(_Solver):
                  leaf_capacity: int = 32, quadrupole: bool = False):
         super().__init__(make_params(SOLVER_TREE, "fp32", softening, opening_angle,
                                      leaf_capacity, quadrupole))
+
+    def tree_stats(self):
+        """(node count, leaf count, depth) of the last tree."""
+        nodes, leaves, depth = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        _check(self._lib.ob_tree_stats(self._handle, C.byref(nodes), C.byref(leaves),
+                                       C.byref(depth)))
+        return nodes.value, leaves.value, depth.value
+
+    def tree(self):
+        """The last octree: reals (n, 5) mass, com xyz, r2; idx (n, 3) next,
+        first, count; quads (n, 6) or None; leaf count; depth."""
+        nodes, leaves, depth = self.tree_stats()
+        reals = np.zeros((nodes, 5))
+        idx = np.zeros((nodes, 3), np.uint64)
+        quad = bool(self.params().quadrupole)
+        quads = np.zeros((nodes, 6)) if quad else None
+        u64 = C.POINTER(C.c_uint64)
+        _check(self._lib.ob_tree_copy(self._handle, _ptr(reals), idx.ctypes.data_as(u64),
+                                      _ptr(quads) if quad else None))
+        return reals, idx, quads, leaves, depth
+
+    def order(self, n: int):
+        """(codes uint64, indices, cube origin, cube size) of the last ordering."""
+        codes = np.zeros(n, np.uint64)
+        idx = np.zeros(n, np.uint32)
+        origin = np.zeros(3)
+        size = C.c_double()
+        _check(self._lib.ob_tree_copy_order(
+            self._handle, codes.ctypes.data_as(C.POINTER(C.c_uint64)),
+            idx.ctypes.data_as(C.POINTER(C.c_uint32)), _ptr(origin), C.byref(size)))
+        return codes, idx, origin, size.value
 
     @classmethod
     def try_create(cls, softening: float = 0.0, opening_angle: float = 0.5,

@@ -11,6 +11,7 @@
 #include "orrery_b200.h"
 #include "solver.hpp"
 #include "system.hpp"
+#include "tree.hpp"
 
 namespace ob {
 
@@ -126,9 +127,14 @@ void System::set_accelerations(const double *ax, const double *ay, const double 
 }
 
 void System::refresh() {
-    evaluate(true);
-    check(cudaStreamSynchronize(stream_), "evaluating accelerations");
-    solver_->check_status(stream_);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        evaluate(attempt == 0);
+        check(cudaStreamSynchronize(stream_), "evaluating accelerations");
+        if (!solver_->grew_after_overflow(stream_)) {
+            return;
+        }
+    }
+    throw Error(OB_ERROR_CAPACITY, "the octree outgrew its node capacity twice");
 }
 
 void System::evaluate(bool count, const cudaEvent_t *marks) {
@@ -184,7 +190,8 @@ void System::enqueue_step(int integrator, double dt) {
 }
 
 void System::ensure_graph(int integrator, double dt) {
-    if (graph_ != nullptr && graph_integrator_ == integrator && graph_dt_ == dt) {
+    if (graph_ != nullptr && graph_integrator_ == integrator && graph_dt_ == dt &&
+        graph_generation_ == solver_->generation()) {
         return;
     }
     drop_graph();
@@ -211,6 +218,7 @@ void System::ensure_graph(int integrator, double dt) {
     check(cudaGraphInstantiate(&graph_, graph, 0), "instantiating the step graph");
     graph_integrator_ = integrator;
     graph_dt_ = dt;
+    graph_generation_ = solver_->generation();
     // Find the event-record node of each placeholder, and count kernels.
     size_t count = 0;
     check(cudaGraphGetNodes(graph, nullptr, &count), "listing graph nodes");
@@ -462,6 +470,31 @@ int ob_solver_timings(const ob_solver *solver, ob_timings *timings) {
     return guarded([&] {
         require(solver != nullptr && timings != nullptr, "NULL argument");
         *timings = solver->impl->timings();
+    });
+}
+
+int ob_tree_stats(ob_solver *solver, uint64_t *nodes, uint64_t *leaves, uint32_t *depth) {
+    return guarded([&] {
+        require(solver != nullptr, "solver is NULL");
+        const ob::TreeMeta m = solver->impl->tree().meta();
+        if (nodes != nullptr) *nodes = m.node_count;
+        if (leaves != nullptr) *leaves = m.leaf_count;
+        if (depth != nullptr) *depth = m.depth;
+    });
+}
+
+int ob_tree_copy(ob_solver *solver, double *reals, uint64_t *idx, double *quads) {
+    return guarded([&] {
+        require(solver != nullptr && reals != nullptr && idx != nullptr, "NULL argument");
+        solver->impl->tree().copy_tree(reals, idx, quads, nullptr, nullptr);
+    });
+}
+
+int ob_tree_copy_order(ob_solver *solver, uint64_t *codes, uint32_t *indices, double *origin,
+                       double *size) {
+    return guarded([&] {
+        require(solver != nullptr, "solver is NULL");
+        solver->impl->tree().copy_order(codes, indices, origin, size);
     });
 }
 

@@ -47,15 +47,18 @@ public:
                                            count_(std::exchange(o.count_, 0)) {}
     ~DeviceArray() { release(); }
 
-    void reserve(size_t count) {
+    // Returns true when the storage moved (callers holding the old pointer,
+    // such as captured graphs, must refresh).
+    bool reserve(size_t count) {
         if (count <= count_) {
-            return;
+            return false;
         }
         release();
         void *p = nullptr;
         check(cudaMalloc(&p, count * sizeof(T)), "device allocation");
         ptr_ = static_cast<T *>(p);
         count_ = count;
+        return true;
     }
     void release() noexcept {
         if (ptr_ != nullptr) {

@@ -108,9 +108,11 @@ void Solver::evaluate_direct(uint32_t n, const double *x, const double *y, const
     const bool split = params_.precision == OB_PRECISION_SPLIT;
     const DirectConfig config = direct_config(n);
     const uint32_t padded = direct_padded_count(n, config);
-    hi_.reserve(padded);
-    if (split) {
-        lo_.reserve(padded);
+    if (hi_.reserve(padded)) {
+        ++generation_;
+    }
+    if (split && lo_.reserve(padded)) {
+        ++generation_;
     }
     check(pack_sources(x, y, z, m, n, padded, hi_.data(), split ? lo_.data() : nullptr, stream),
           "packing sources");
@@ -167,6 +169,7 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
         if (split) {
             lo_.reserve(padded);
         }
+        ++generation_;
         check(pack_sources(d, d + n, d + 2ull * n, d + 3ull * n, n, padded, hi_.data(),
                            split ? lo_.data() : nullptr, stream_),
               "packing autotune sources");
@@ -201,6 +204,7 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
         throw Error(OB_ERROR_CUDA, "no direct kernel shape could be launched");
     }
     configs_[n] = chosen;
+    ++generation_;
     return best;
 }
 
@@ -242,25 +246,57 @@ void Solver::evaluate_host(uint64_t n64, const double *x, const double *y, const
     staging_.reserve(7ull * n);
     double *d = staging_.data();
     const size_t bytes = sizeof(double) * n;
-    check(cudaEventRecord(events_[0], stream_), "recording an event");
-    const double *in[4] = {x, y, z, m};
-    for (int k = 0; k < 4; ++k) {
-        check(cudaMemcpyAsync(d + static_cast<size_t>(k) * n, in[k], bytes,
-                              cudaMemcpyHostToDevice, stream_),
-              "copying particles to the device");
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        check(cudaEventRecord(events_[0], stream_), "recording an event");
+        const double *in[4] = {x, y, z, m};
+        for (int k = 0; k < 4; ++k) {
+            check(cudaMemcpyAsync(d + static_cast<size_t>(k) * n, in[k], bytes,
+                                  cudaMemcpyHostToDevice, stream_),
+                  "copying particles to the device");
+        }
+        evaluate_device(n, d, d + n, d + 2ull * n, d + 3ull * n, d + 4ull * n, d + 5ull * n,
+                        d + 6ull * n, stream_, attempt == 0);
+        double *out[3] = {ax, ay, az};
+        for (int k = 0; k < 3; ++k) {
+            check(cudaMemcpyAsync(out[k], d + static_cast<size_t>(4 + k) * n, bytes,
+                                  cudaMemcpyDeviceToHost, stream_),
+                  "copying accelerations to the host");
+        }
+        check(cudaEventRecord(events_[5], stream_), "recording an event");
+        check(cudaStreamSynchronize(stream_), "evaluating forces");
+        timed_host_ = true;
+        if (!grew_after_overflow(stream_)) {
+            return;
+        }
     }
-    evaluate_device(n, d, d + n, d + 2ull * n, d + 3ull * n, d + 4ull * n, d + 5ull * n,
-                    d + 6ull * n, stream_);
-    double *out[3] = {ax, ay, az};
-    for (int k = 0; k < 3; ++k) {
-        check(cudaMemcpyAsync(out[k], d + static_cast<size_t>(4 + k) * n, bytes,
-                              cudaMemcpyDeviceToHost, stream_),
-              "copying accelerations to the host");
+    throw Error(OB_ERROR_CAPACITY, "the octree outgrew its node capacity twice");
+}
+
+TreePipeline &Solver::tree() {
+    if (!tree_) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "not a tree solver");
     }
-    check(cudaEventRecord(events_[5], stream_), "recording an event");
-    check(cudaStreamSynchronize(stream_), "evaluating forces");
-    timed_host_ = true;
-    check_status(stream_);
+    return *tree_;
+}
+
+uint64_t Solver::generation() const noexcept {
+    return generation_ + (tree_ ? tree_->generation() : 0);
+}
+
+bool Solver::grew_after_overflow(cudaStream_t stream) {
+    const unsigned status = read_and_clear_status(status_.data(), stream);
+    if (status & kStatusTimeout) {
+        throw Error(OB_ERROR_TIMEOUT, "a device-side wait ran out of its bound");
+    }
+    if ((status & kStatusOverflow) && tree_) {
+        const uint32_t required = tree_->meta().required;
+        tree_->grow_nodes(required + required / 4 + 1024);
+        return true;
+    }
+    if (status & kStatusOverflow) {
+        throw Error(OB_ERROR_CAPACITY, "a device-side buffer bound was exceeded");
+    }
+    return false;
 }
 
 void Solver::check_status(cudaStream_t stream) {

@@ -60,9 +60,23 @@ public:
 
     // Chooses (and caches) the direct kernel shape for n particles.
     DirectConfig direct_config(uint32_t n);
-    void set_direct_config(uint32_t n, const DirectConfig &config) { configs_[n] = config; }
+    void set_direct_config(uint32_t n, const DirectConfig &config) {
+        configs_[n] = config;
+        ++generation_;
+    }
 
     int sm_count() const noexcept { return sm_count_; }
+
+    // The tree pipeline (tree solvers only; throws otherwise).
+    TreePipeline &tree();
+
+    // Changes whenever a device buffer the evaluation uses is reallocated.
+    uint64_t generation() const noexcept;
+
+    // After a synchronised evaluation: true if the tree ran out of node
+    // capacity, in which case the capacity has been raised and the
+    // evaluation must be repeated.
+    bool grew_after_overflow(cudaStream_t stream);
 
     // Times every implemented shape on synthetic sources of n particles and
     // keeps the fastest for n. Returns the time per evaluation in ms.
@@ -85,6 +99,7 @@ private:
     bool timed_host_ = false;
     cudaStream_t stream_ = nullptr;
     std::map<uint32_t, DirectConfig> configs_;
+    uint64_t generation_ = 0;
     std::unique_ptr<TreePipeline> tree_;
 };
 

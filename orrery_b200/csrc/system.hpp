@@ -68,6 +68,7 @@ private:
     int graph_integrator_ = -1;
     double graph_dt_ = 0.0;
     uint32_t graph_kernels_ = 0;
+    uint64_t graph_generation_ = 0;
 
     // Four placeholder events per evaluation of a step, captured as event
     // nodes; before a profiled replay they are pointed at a fresh slot of ring_.

@@ -1,18 +1,665 @@
-// Barnes-Hut pipeline (under construction).
+// Octree construction on the device, node for node the reference's tree.
+//
+// The reference builds top-down by recursion (src/solvers/octree.cpp:273-372):
+// a cell is split while it holds more than leaf_capacity particles and is
+// above level 21, empty octants are skipped, and nodes are emitted in
+// depth-first pre-order with octants in order 0..7. This file computes the
+// same node set and layout without recursion, one thread per sorted particle:
+//
+//   * the cells whose first particle is b are the level-L cells starting at b
+//     for L above c(b), the number of leading octal digits b's code shares with
+//     b-1's; those that are nodes form one contiguous run of levels, from
+//     c(b)+1 (when the enclosing level-c(b) cell is split) down to the first
+//     leaf;
+//   * ordering all nodes by (first particle, level) is the pre-order, so a
+//     node's index is the exclusive prefix sum of per-particle node counts plus
+//     its rank in its run, and its escape index (TreeNode::next) is the prefix
+//     sum at the end of its particle range.
+//
+// Moments are then formed bottom-up in one kernel: each leaf's thread sums its
+// particles, and the last child to finish computes its parent (an atomic
+// arrival count; no thread ever waits). All arithmetic is FP64 with explicitly
+// rounded operations in the reference's order (set_leaf_moments,
+// gather_moments, add_displaced_moment, acceptance_radius_squared;
+// octree.cpp:75-185, 374-387), so masses, centres of mass, quadrupoles and
+// acceptance radii are bit-identical to the reference's.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
 #include "tree.hpp"
+#include "tree_kernels.hpp"
 
 namespace ob {
+namespace {
 
-TreePipeline::TreePipeline(const ob_solver_params &params) : params_(params) {}
-TreePipeline::~TreePipeline() = default;
+constexpr uint32_t kLevels = 21;
+constexpr uint32_t kThreads = 256;
 
-void TreePipeline::evaluate(uint32_t, const double *, const double *, const double *,
-                            const double *, double *, double *, double *, unsigned *,
-                            cudaEvent_t, cudaEvent_t, bool, cudaStream_t) {
-    throw Error(OB_ERROR_UNSUPPORTED, "the tree solver is not built yet");
+__device__ __forceinline__ int common_levels(const unsigned long long *codes, uint32_t b) {
+    if (b == 0) {
+        return -1;
+    }
+    const unsigned long long x = codes[b] ^ codes[b - 1];
+    if (x == 0ull) {
+        return static_cast<int>(kLevels);
+    }
+    const int high = 63 - __clzll(static_cast<long long>(x));
+    return 20 - high / 3;
 }
 
-ob_counts TreePipeline::device_counts() { return ob_counts{}; }
-void TreePipeline::reset_counts() {}
+__device__ __forceinline__ unsigned long long prefix(unsigned long long code, uint32_t level) {
+    return level == 0 ? 0ull : code >> (3u * (kLevels - level));
+}
+
+// First index after i whose level-`level` prefix differs from codes[i]'s.
+__device__ uint32_t cell_end(const unsigned long long *codes, uint32_t n, uint32_t i,
+                             uint32_t level) {
+    if (level == 0) {
+        return n;
+    }
+    const unsigned long long p = prefix(codes[i], level);
+    uint32_t lo = i; // known inside
+    uint32_t step = 1;
+    while (lo + step < n && prefix(codes[lo + step], level) == p) {
+        lo += step;
+        step <<= 1;
+    }
+    uint32_t hi = min(lo + step, n); // first candidate outside (or n)
+    while (hi - lo > 1) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (prefix(codes[mid], level) == p) {
+            lo = mid;
+        } else {
+            hi = mid;
+        }
+    }
+    return hi;
+}
+
+// First index of the level-`level` cell containing i.
+__device__ uint32_t cell_start(const unsigned long long *codes, uint32_t i, uint32_t level) {
+    if (level == 0) {
+        return 0;
+    }
+    const unsigned long long p = prefix(codes[i], level);
+    uint32_t hi = i; // known inside
+    uint32_t step = 1;
+    while (step <= hi && prefix(codes[hi - step], level) == p) {
+        hi -= step;
+        step <<= 1;
+    }
+    // Outside candidate below hi: hi - step (or none if step > hi).
+    int64_t lo = static_cast<int64_t>(hi) - static_cast<int64_t>(step);
+    if (lo < 0) {
+        lo = -1;
+    }
+    while (static_cast<int64_t>(hi) - lo > 1) {
+        const uint32_t mid = static_cast<uint32_t>(lo + (static_cast<int64_t>(hi) - lo) / 2);
+        if (prefix(codes[mid], level) == p) {
+            hi = mid;
+        } else {
+            lo = mid;
+        }
+    }
+    return hi;
+}
+
+// The run of node levels starting at particle b: [lo, hi], or lo > hi for none.
+__device__ void node_run(const unsigned long long *codes, uint32_t n, uint32_t cap, uint32_t b,
+                         int &c, uint32_t &lo, uint32_t &hi) {
+    c = common_levels(codes, b);
+    if (b > 0) {
+        if (c >= static_cast<int>(kLevels)) {
+            lo = 1;
+            hi = 0;
+            return;
+        }
+        const uint32_t level = static_cast<uint32_t>(c);
+        const uint32_t start = cell_start(codes, b - 1, level);
+        const uint32_t end = cell_end(codes, n, b, level);
+        if (end - start <= cap) {
+            lo = 1;
+            hi = 0;
+            return;
+        }
+        lo = level + 1;
+    } else {
+        lo = 0;
+    }
+    uint32_t level = lo;
+    while (true) {
+        const uint32_t end = cell_end(codes, n, b, level);
+        if (end - b <= cap || level >= kLevels) {
+            break;
+        }
+        ++level;
+    }
+    hi = level;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    layout_count_kernel(const unsigned long long *__restrict__ codes, uint32_t n, uint32_t cap,
+                        uint32_t *counts) {
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+        int c;
+        uint32_t lo, hi;
+        node_run(codes, n, cap, b, c, lo, hi);
+        counts[b] = lo <= hi ? hi - lo + 1 : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    layout_write_kernel(const unsigned long long *__restrict__ codes, uint32_t n, uint32_t cap,
+                        const uint32_t *__restrict__ offsets, uint32_t capacity,
+                        DeviceNode *nodes, uint32_t *children, TreeMeta *meta,
+                        unsigned *status) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint32_t total = offsets[n];
+        meta->node_count = total <= capacity ? total : 0u;
+        meta->required = total;
+        if (total > capacity) {
+            atomicOr(status, kStatusOverflow);
+        }
+    }
+    if (offsets[n] > capacity) {
+        return;
+    }
+    uint32_t leaves = 0, depth = 0;
+    for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+        int c;
+        uint32_t lo, hi;
+        node_run(codes, n, cap, b, c, lo, hi);
+        if (lo > hi) {
+            continue;
+        }
+        uint32_t index = offsets[b];
+        uint32_t parent;
+        if (b == 0) {
+            parent = index; // the root is its own parent
+        } else {
+            // The enclosing level-c cell starts at `start`; its node is in the
+            // run of `start` at rank c - (c(start) + 1).
+            const uint32_t level = static_cast<uint32_t>(c);
+            const uint32_t start = cell_start(codes, b - 1, level);
+            const int cs = common_levels(codes, start);
+            const uint32_t first_level = start == 0 ? 0u : static_cast<uint32_t>(cs + 1);
+            parent = offsets[start] + (level - first_level);
+        }
+        for (uint32_t level = lo; level <= hi; ++level, ++index) {
+            const uint32_t end = cell_end(codes, n, b, level);
+            const bool leaf = level == hi;
+            DeviceNode node;
+            node.com_x = node.com_y = node.com_z = 0.0;
+            node.r2 = 0.0;
+            node.mass = 0.0;
+            node.next = offsets[end];
+            node.count = leaf ? end - b : 0u;
+            node.first = b;
+            node.level = level;
+            node.parent = parent;
+            node.pad = 0;
+            nodes[index] = node;
+            if (parent != index) {
+                atomicAdd(&children[parent], 1u);
+            }
+            parent = index;
+            if (leaf) {
+                ++leaves;
+                depth = max(depth, level);
+            }
+        }
+    }
+    // Block-reduce the leaf count and depth before touching the globals.
+    for (int off = 16; off > 0; off >>= 1) {
+        leaves += __shfl_down_sync(0xffffffffu, leaves, off);
+        depth = max(depth, __shfl_down_sync(0xffffffffu, depth, off));
+    }
+    if ((threadIdx.x & 31u) == 0 && leaves > 0) {
+        atomicAdd(&meta->leaf_count, leaves);
+        atomicMax(&meta->depth, depth);
+    }
+}
+
+// Geometric centre and edge of the cell at `level` holding `code`, by the
+// reference's recursion: child centre = centre +- size/4 per axis, child size
+// = size/2 (octree.cpp:41-47, 305-310).
+__device__ void cell_geometry(const TreeMeta *meta, unsigned long long code, uint32_t level,
+                              double c[3], double &size) {
+    c[0] = meta->root_centre[0];
+    c[1] = meta->root_centre[1];
+    c[2] = meta->root_centre[2];
+    size = meta->size;
+    for (uint32_t l = 1; l <= level; ++l) {
+        const uint32_t octant = static_cast<uint32_t>((code >> (3u * (kLevels - l))) & 7u);
+        const double quarter = __ddiv_rn(size, 4.0);
+        c[0] = __dadd_rn(c[0], (octant & 4u) ? quarter : -quarter);
+        c[1] = __dadd_rn(c[1], (octant & 2u) ? quarter : -quarter);
+        c[2] = __dadd_rn(c[2], (octant & 1u) ? quarter : -quarter);
+        size = __ddiv_rn(size, 2.0);
+    }
+}
+
+// add_displaced_moment (octree.cpp:75-84).
+__device__ __forceinline__ void add_displaced(DeviceQuadrupole &q, double mass, double dx,
+                                              double dy, double dz) {
+    const double trace =
+        __dmul_rn(mass, __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)),
+                                  __dmul_rn(dz, dz)));
+    const double m3 = __dmul_rn(3.0, mass);
+    q.xx = __dadd_rn(q.xx, __dsub_rn(__dmul_rn(__dmul_rn(m3, dx), dx), trace));
+    q.xy = __dadd_rn(q.xy, __dmul_rn(__dmul_rn(m3, dx), dy));
+    q.xz = __dadd_rn(q.xz, __dmul_rn(__dmul_rn(m3, dx), dz));
+    q.yy = __dadd_rn(q.yy, __dsub_rn(__dmul_rn(__dmul_rn(m3, dy), dy), trace));
+    q.yz = __dadd_rn(q.yz, __dmul_rn(__dmul_rn(m3, dy), dz));
+    q.zz = __dadd_rn(q.zz, __dsub_rn(__dmul_rn(__dmul_rn(m3, dz), dz), trace));
+}
+
+// acceptance_radius_squared (octree.cpp:374-387) of a cell with its moments.
+__device__ double acceptance(const TreeMeta *meta, unsigned long long code, uint32_t level,
+                             double cx, double cy, double cz, double theta) {
+    double centre[3], size;
+    cell_geometry(meta, code, level, centre, size);
+    const double ox = __dsub_rn(cx, centre[0]);
+    const double oy = __dsub_rn(cy, centre[1]);
+    const double oz = __dsub_rn(cz, centre[2]);
+    const double offset =
+        __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(ox, ox), __dmul_rn(oy, oy)), __dmul_rn(oz, oz)));
+    if (!(theta > 0.0)) {
+        return INFINITY;
+    }
+    const double radius = __dadd_rn(__ddiv_rn(size, theta), offset);
+    return __dmul_rn(radius, radius);
+}
+
+// Escape index of a child; an index that does not move forward (never
+// produced by the layout) ends the loop instead of repeating forever.
+__device__ __forceinline__ uint32_t next_child(const DeviceNode *nodes, uint32_t child,
+                                               uint32_t stop) {
+    const uint32_t next = __ldcg(&nodes[child].next);
+    return next > child ? next : stop;
+}
+
+__device__ void store_quads(DeviceQuadrupole *quads, float *quads32, uint32_t k,
+                            const DeviceQuadrupole &q) {
+    quads[k] = q;
+    float4 *w = reinterpret_cast<float4 *>(quads32 + 8ull * k);
+    w[0] = make_float4(__double2float_rn(q.xx), __double2float_rn(q.xy), __double2float_rn(q.xz),
+                       __double2float_rn(q.yy));
+    w[1] = make_float4(__double2float_rn(q.yz), __double2float_rn(q.zz), 0.0f, 0.0f);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    moments_kernel(const double *__restrict__ sorted, const unsigned long long *__restrict__ codes,
+                   uint32_t n, DeviceNode *nodes, DeviceQuadrupole *quads, float *quads32,
+                   const uint32_t *__restrict__ children, uint32_t *arrived, float4 *leaf_rel,
+                   TreeMeta *meta, double theta) {
+    const double *X = sorted;
+    const double *Y = sorted + n;
+    const double *Z = sorted + 2ull * n;
+    const double *M = sorted + 3ull * n;
+    const uint32_t count_nodes = meta->node_count;
+    const bool with_quads = quads != nullptr;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count_nodes;
+         k += gridDim.x * blockDim.x) {
+        if (nodes[k].count == 0) {
+            continue; // internal nodes are formed by their last child
+        }
+        // set_leaf_moments (octree.cpp:91-135).
+        const uint32_t begin = nodes[k].first;
+        const uint32_t end = begin + nodes[k].count;
+        double mass = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+        for (uint32_t i = begin; i < end; ++i) {
+            const double pm = M[i];
+            mass = __dadd_rn(mass, pm);
+            wx = __dadd_rn(wx, __dmul_rn(X[i], pm));
+            wy = __dadd_rn(wy, __dmul_rn(Y[i], pm));
+            wz = __dadd_rn(wz, __dmul_rn(Z[i], pm));
+        }
+        double cx, cy, cz;
+        if (mass > 0.0) {
+            cx = __ddiv_rn(wx, mass);
+            cy = __ddiv_rn(wy, mass);
+            cz = __ddiv_rn(wz, mass);
+        } else {
+            cx = X[begin];
+            cy = Y[begin];
+            cz = Z[begin];
+        }
+        DeviceQuadrupole q{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (uint32_t i = begin; i < end; ++i) {
+            if (with_quads) {
+                add_displaced(q, M[i], __dsub_rn(X[i], cx), __dsub_rn(Y[i], cy),
+                              __dsub_rn(Z[i], cz));
+            }
+            // Sources relative to the leaf's centre of mass, for the FP32 walk.
+            leaf_rel[i] = make_float4(__double2float_rn(__dsub_rn(X[i], cx)),
+                                      __double2float_rn(__dsub_rn(Y[i], cy)),
+                                      __double2float_rn(__dsub_rn(Z[i], cz)),
+                                      __double2float_rn(M[i]));
+        }
+        const uint32_t level = nodes[k].level;
+        nodes[k].mass = mass;
+        nodes[k].com_x = cx;
+        nodes[k].com_y = cy;
+        nodes[k].com_z = cz;
+        nodes[k].r2 = acceptance(meta, codes[begin], level, cx, cy, cz, theta);
+        if (with_quads) {
+            store_quads(quads, quads32, k, q);
+        }
+
+        // Climb while this thread completes its parent (gather_moments,
+        // octree.cpp:142-185). A cell has at most 22 ancestors.
+        uint32_t current = k;
+        for (int climb = 0; climb < 64; ++climb) {
+            __threadfence();
+            const uint32_t parent = nodes[current].parent;
+            if (parent == current) {
+                break;
+            }
+            const uint32_t before = atomicAdd(&arrived[parent], 1u);
+            if (before + 1 != children[parent]) {
+                break;
+            }
+            __threadfence();
+            const uint32_t stop = __ldcg(&nodes[parent].next);
+            double pm = 0.0, px = 0.0, py = 0.0, pz = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
+            uint32_t kids = 0;
+            for (uint32_t child = parent + 1; child < stop;
+                 child = next_child(nodes, child, stop)) {
+                const double cm = __ldcg(&nodes[child].mass);
+                const double ccx = __ldcg(&nodes[child].com_x);
+                const double ccy = __ldcg(&nodes[child].com_y);
+                const double ccz = __ldcg(&nodes[child].com_z);
+                pm = __dadd_rn(pm, cm);
+                px = __dadd_rn(px, __dmul_rn(ccx, cm));
+                py = __dadd_rn(py, __dmul_rn(ccy, cm));
+                pz = __dadd_rn(pz, __dmul_rn(ccz, cm));
+                mx = __dadd_rn(mx, ccx);
+                my = __dadd_rn(my, ccy);
+                mz = __dadd_rn(mz, ccz);
+                ++kids;
+            }
+            double gx, gy, gz;
+            if (pm > 0.0) {
+                gx = __ddiv_rn(px, pm);
+                gy = __ddiv_rn(py, pm);
+                gz = __ddiv_rn(pz, pm);
+            } else {
+                const double cnt = static_cast<double>(kids == 0 ? 1u : kids);
+                gx = __ddiv_rn(mx, cnt);
+                gy = __ddiv_rn(my, cnt);
+                gz = __ddiv_rn(mz, cnt);
+            }
+            if (with_quads) {
+                DeviceQuadrupole moment{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+                for (uint32_t child = parent + 1; child < stop;
+                     child = next_child(nodes, child, stop)) {
+                    moment.xx = __dadd_rn(moment.xx, __ldcg(&quads[child].xx));
+                    moment.xy = __dadd_rn(moment.xy, __ldcg(&quads[child].xy));
+                    moment.xz = __dadd_rn(moment.xz, __ldcg(&quads[child].xz));
+                    moment.yy = __dadd_rn(moment.yy, __ldcg(&quads[child].yy));
+                    moment.yz = __dadd_rn(moment.yz, __ldcg(&quads[child].yz));
+                    moment.zz = __dadd_rn(moment.zz, __ldcg(&quads[child].zz));
+                    add_displaced(moment, __ldcg(&nodes[child].mass),
+                                  __dsub_rn(__ldcg(&nodes[child].com_x), gx),
+                                  __dsub_rn(__ldcg(&nodes[child].com_y), gy),
+                                  __dsub_rn(__ldcg(&nodes[child].com_z), gz));
+                }
+                store_quads(quads, quads32, parent, moment);
+            }
+            const uint32_t plevel = __ldcg(&nodes[parent].level);
+            const uint32_t pfirst = __ldcg(&nodes[parent].first);
+            nodes[parent].mass = pm;
+            nodes[parent].com_x = gx;
+            nodes[parent].com_y = gy;
+            nodes[parent].com_z = gz;
+            nodes[parent].r2 = acceptance(meta, codes[pfirst], plevel, gx, gy, gz, theta);
+            current = parent;
+        }
+    }
+}
+
+uint32_t grid_for(uint32_t n) { return std::max(1u, std::min(ceil_div(n, kThreads), 148u * 8u)); }
+
+} // namespace
+
+cudaError_t launch_layout_count(const unsigned long long *codes, uint32_t n, uint32_t leaf_cap,
+                                uint32_t *counts, cudaStream_t stream) {
+    layout_count_kernel<<<grid_for(n), kThreads, 0, stream>>>(codes, n, leaf_cap, counts);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_layout_write(const unsigned long long *codes, uint32_t n, uint32_t leaf_cap,
+                                const uint32_t *offsets, uint32_t node_capacity,
+                                DeviceNode *nodes, uint32_t *children, TreeMeta *meta,
+                                unsigned *status, cudaStream_t stream) {
+    layout_write_kernel<<<grid_for(n), kThreads, 0, stream>>>(codes, n, leaf_cap, offsets,
+                                                             node_capacity, nodes, children,
+                                                             meta, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_moments(const double *sorted, const unsigned long long *codes, uint32_t n,
+                           DeviceNode *nodes, DeviceQuadrupole *quads, float *quads32,
+                           const uint32_t *children, uint32_t *arrived, float4 *leaf_rel,
+                           TreeMeta *meta, double opening_angle, uint32_t node_capacity,
+                           cudaStream_t stream) {
+    moments_kernel<<<grid_for(node_capacity), kThreads, 0, stream>>>(
+        sorted, codes, n, nodes, quads, quads32, children, arrived, leaf_rel, meta,
+        opening_angle);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// TreePipeline
+// ---------------------------------------------------------------------------
+
+TreePipeline::TreePipeline(const ob_solver_params &params) : params_(params) {
+    int device = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "SMs");
+    meta_.reserve(1);
+    check(cudaMemset(meta_.data(), 0, sizeof(TreeMeta)), "clearing tree scalars");
+    counters_.reserve(2);
+    check(cudaMemset(counters_.data(), 0, 2 * sizeof(unsigned long long)), "clearing counters");
+}
+
+TreePipeline::~TreePipeline() = default;
+
+uint32_t TreePipeline::nodes_for(uint32_t n) const {
+    const uint64_t cap = params_.leaf_capacity < 1 ? 1 : params_.leaf_capacity;
+    const uint64_t estimate = 8ull * n / cap + n / 2 + 1024;
+    const uint64_t bound = 22ull * n + 1;
+    return static_cast<uint32_t>(std::min<uint64_t>(std::min(estimate, bound), 0xffffffffull));
+}
+
+void TreePipeline::reserve(uint32_t n) {
+    if (n > kMaxTreeParticles) {
+        throw Error(OB_ERROR_CAPACITY, "the tree solver handles at most 2^30 - 1 particles");
+    }
+    if (n > capacity_) {
+        ++generation_;
+        for (int k = 0; k < 2; ++k) {
+            keys_[k].reserve(n);
+            perm_[k].reserve(n);
+        }
+        sorted_.reserve(4ull * n);
+        leaf_rel_.reserve(n);
+        node_start_.reserve(2ull * n + 1);
+        scan_partials_.reserve(scan_partials_needed(n));
+        reduce_.reserve(cube_partials_needed(n));
+        hist_.reserve(kRadixPasses * kRadix);
+        lookback_.reserve(static_cast<size_t>(kRadixPasses) * sort_tiles(n) * kRadix);
+        tile_counter_.reserve(kRadixPasses);
+        capacity_ = n;
+    }
+    const uint32_t want = std::max(nodes_for(n), grow_to_);
+    if (want > node_capacity_) {
+        ++generation_;
+        nodes_.reserve(want);
+        if (params_.quadrupole) {
+            quads_.reserve(want);
+            quads32_.reserve(8ull * want);
+        }
+        level_lists_.reserve(2ull * want); // children counts, then arrivals
+        node_capacity_ = want;
+    }
+}
+
+void TreePipeline::evaluate(uint32_t n, const double *x, const double *y, const double *z,
+                            const double *m, double *ax, double *ay, double *az,
+                            unsigned *status, cudaEvent_t ordered, cudaEvent_t built,
+                            bool external, cudaStream_t stream) {
+    if (n == 0) {
+        record(ordered, stream, external);
+        record(built, stream, external);
+        return;
+    }
+    reserve(n);
+    last_n_ = n;
+    const uint32_t tiles = sort_tiles(n);
+    // Per-evaluation scalars and scratch.
+    check(cudaMemsetAsync(meta_.data(), 0, sizeof(TreeMeta), stream), "clearing tree scalars");
+    check(cudaMemsetAsync(hist_.data(), 0, hist_.bytes(), stream), "clearing histograms");
+    check(cudaMemsetAsync(lookback_.data(), 0,
+                          sizeof(uint32_t) * kRadixPasses * static_cast<size_t>(tiles) * kRadix,
+                          stream),
+          "clearing look-back words");
+    check(cudaMemsetAsync(tile_counter_.data(), 0, sizeof(uint32_t) * kRadixPasses, stream),
+          "clearing tile tickets");
+    check(cudaMemsetAsync(level_lists_.data(), 0, sizeof(uint32_t) * 2ull * node_capacity_,
+                          stream),
+          "clearing child counts");
+
+    // Ordering: cube, codes + histograms, eight onesweep passes, gather.
+    check(launch_bounding_cube(x, y, z, n, reduce_.data(), meta_.data(), stream), "cube");
+    check(launch_encode(x, y, z, n, meta_.data(), keys_[0].data(), perm_[0].data(), hist_.data(),
+                        stream),
+          "Morton codes");
+    check(launch_scan_histograms(hist_.data(), stream), "digit offsets");
+    for (int pass = 0; pass < kRadixPasses; ++pass) {
+        const int src = pass & 1;
+        check(launch_onesweep(keys_[src].data(), perm_[src].data(), keys_[1 - src].data(),
+                              perm_[1 - src].data(), n, pass, hist_.data(),
+                              lookback_.data() + static_cast<size_t>(pass) * tiles * kRadix,
+                              tile_counter_.data() + pass, status, stream),
+              "radix sort pass");
+    }
+    // Eight passes end in buffer 0.
+    const unsigned long long *codes = keys_[0].data();
+    const uint32_t *perm = perm_[0].data();
+    check(launch_gather(x, y, z, m, perm, n, sorted_.data(), stream), "gather");
+    record(ordered, stream, external);
+
+    // Construction: layout, node offsets, records, moments.
+    const uint32_t cap = static_cast<uint32_t>(std::min<uint64_t>(params_.leaf_capacity,
+                                                                 0xffffffffull));
+    uint32_t *counts = node_start_.data();
+    uint32_t *offsets = node_start_.data() + n;
+    check(launch_layout_count(codes, n, cap, counts, stream), "node counts");
+    check(launch_exclusive_scan(counts, offsets, n, scan_partials_.data(), stream), "node scan");
+    uint32_t *children = level_lists_.data();
+    uint32_t *arrived = level_lists_.data() + node_capacity_;
+    check(launch_layout_write(codes, n, cap, offsets, node_capacity_, nodes_.data(), children,
+                              meta_.data(), status, stream),
+          "node layout");
+    check(launch_moments(sorted_.data(), codes, n, nodes_.data(),
+                         params_.quadrupole ? quads_.data() : nullptr,
+                         params_.quadrupole ? quads32_.data() : nullptr, children, arrived,
+                         leaf_rel_.data(), meta_.data(), params_.opening_angle, node_capacity_,
+                         stream),
+          "moments");
+    record(built, stream, external);
+
+    // Traversal.
+    check(launch_walk(nodes_.data(), params_.quadrupole ? quads32_.data() : nullptr,
+                      leaf_rel_.data(), sorted_.data(), perm, n,
+                      params_.softening * params_.softening, ax, ay, az, meta_.data(),
+                      counters_.data(), stream),
+          "tree walk");
+}
+
+ob_counts TreePipeline::device_counts() {
+    unsigned long long host[2] = {0, 0};
+    check(cudaMemcpy(host, counters_.data(), sizeof(host), cudaMemcpyDeviceToHost),
+          "reading tree counters");
+    ob_counts c{};
+    c.particle_particle = host[0];
+    c.particle_cell = host[1];
+    return c;
+}
+
+void TreePipeline::reset_counts() {
+    check(cudaMemset(counters_.data(), 0, 2 * sizeof(unsigned long long)), "clearing counters");
+}
+
+TreeMeta TreePipeline::meta() {
+    TreeMeta h{};
+    check(cudaMemcpy(&h, meta_.data(), sizeof(TreeMeta), cudaMemcpyDeviceToHost),
+          "reading tree scalars");
+    return h;
+}
+
+uint32_t TreePipeline::node_count() { return meta().node_count; }
+
+void TreePipeline::copy_tree(double *reals, uint64_t *idx, double *quads, uint32_t *leaf_count,
+                             uint32_t *depth) {
+    const TreeMeta h = meta();
+    std::vector<DeviceNode> nodes(h.node_count);
+    if (h.node_count > 0) {
+        check(cudaMemcpy(nodes.data(), nodes_.data(), sizeof(DeviceNode) * h.node_count,
+                         cudaMemcpyDeviceToHost),
+              "copying the tree");
+    }
+    for (uint32_t k = 0; k < h.node_count; ++k) {
+        reals[5ull * k + 0] = nodes[k].mass;
+        reals[5ull * k + 1] = nodes[k].com_x;
+        reals[5ull * k + 2] = nodes[k].com_y;
+        reals[5ull * k + 3] = nodes[k].com_z;
+        reals[5ull * k + 4] = nodes[k].r2;
+        idx[3ull * k + 0] = nodes[k].next;
+        idx[3ull * k + 1] = nodes[k].first;
+        idx[3ull * k + 2] = nodes[k].count;
+    }
+    if (quads != nullptr && params_.quadrupole && h.node_count > 0) {
+        check(cudaMemcpy(quads, quads_.data(), sizeof(DeviceQuadrupole) * h.node_count,
+                         cudaMemcpyDeviceToHost),
+              "copying quadrupoles");
+    }
+    if (leaf_count != nullptr) {
+        *leaf_count = h.leaf_count;
+    }
+    if (depth != nullptr) {
+        *depth = h.depth;
+    }
+}
+
+void TreePipeline::copy_order(uint64_t *codes, uint32_t *indices, double *origin, double *size) {
+    const TreeMeta h = meta();
+    if (last_n_ > 0) {
+        if (codes != nullptr) {
+            check(cudaMemcpy(codes, keys_[0].data(), sizeof(uint64_t) * last_n_,
+                             cudaMemcpyDeviceToHost),
+                  "copying codes");
+        }
+        if (indices != nullptr) {
+            check(cudaMemcpy(indices, perm_[0].data(), sizeof(uint32_t) * last_n_,
+                             cudaMemcpyDeviceToHost),
+                  "copying the permutation");
+        }
+    }
+    if (origin != nullptr) {
+        origin[0] = h.origin[0];
+        origin[1] = h.origin[1];
+        origin[2] = h.origin[2];
+    }
+    if (size != nullptr) {
+        *size = h.size;
+    }
+}
+
+void TreePipeline::grow_nodes(uint32_t at_least) { grow_to_ = std::max(grow_to_, at_least); }
 
 } // namespace ob

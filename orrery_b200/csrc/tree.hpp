@@ -11,23 +11,24 @@
 
 namespace ob {
 
-// One octree node as the walk reads it: FP64 centre of mass, mass and squared
-// acceptance radius (the FP64 accept test of src/solvers/tree_walk.cpp:46 is
-// reproduced exactly), FP32 geometric centre of the cell, and the escape /
-// particle-range fields of TreeNode (include/orrery/solvers/octree.hpp:104-139)
-// narrowed to 32 bits as the reference's CudaTreeNode does
-// (include/orrery/solvers/cuda_kernels.hpp:137-145).
+// One octree node, 64 bytes, read by the walk as four 16-byte loads: FP64
+// centre of mass and squared acceptance radius (so the accept test of
+// src/solvers/tree_walk.cpp:46 is reproduced exactly), FP64 mass, and the
+// escape / particle-range fields of TreeNode (include/orrery/solvers/
+// octree.hpp:104-139) narrowed to 32 bits as the reference's CudaTreeNode
+// does (include/orrery/solvers/cuda_kernels.hpp:137-145).
 struct alignas(16) DeviceNode {
-    double com_x, com_y, com_z;
+    double com_x, com_y;
+    double com_z, r2;    // r2: acceptance radius squared (+inf when theta = 0)
     double mass;
-    double r2;          // acceptance radius squared (+inf when theta = 0)
-    uint32_t next;      // escape index: first node after this subtree
-    uint32_t first;     // first particle (sorted order)
-    uint32_t count;     // particle count if a leaf, 0 for internal nodes
-    uint32_t level;     // depth of the cell (root 0)
-    double centre_x, centre_y, centre_z; // geometric centre of the cell
-    double size;        // edge length of the cell
+    uint32_t next;       // escape index: first node after this subtree
+    uint32_t count;      // particle count if a leaf, 0 for internal nodes
+    uint32_t first;      // first particle of the cell (sorted order)
+    uint32_t level;      // depth of the cell (root 0)
+    uint32_t parent;     // parent node (the root points at itself)
+    uint32_t pad;
 };
+static_assert(sizeof(DeviceNode) == 64, "DeviceNode is four 16-byte words");
 
 // Traceless quadrupole (include/orrery/solvers/octree.hpp:89-96).
 struct DeviceQuadrupole {
@@ -42,7 +43,7 @@ struct TreeMeta {
     uint32_t node_count;
     uint32_t leaf_count;
     uint32_t depth;
-    uint32_t pad;
+    uint32_t required;  // nodes the layout needed (reported on overflow)
     unsigned long long pairs;
     unsigned long long cells;
 };
@@ -73,30 +74,43 @@ public:
     void copy_order(uint64_t *codes, uint32_t *indices, double *origin, double *size);
     uint32_t capacity_nodes() const noexcept { return node_capacity_; }
 
+    // Raises the node capacity used from the next evaluation on.
+    void grow_nodes(uint32_t at_least);
+
+    // The device scalars of the last evaluation (synchronous).
+    TreeMeta meta();
+
+    // Bumped whenever a device buffer is reallocated (captured graphs that
+    // hold the old pointers must be captured again).
+    uint64_t generation() const noexcept { return generation_; }
+
 private:
     void reserve(uint32_t n);
+    uint32_t nodes_for(uint32_t n) const;
 
     ob_solver_params params_;
     uint32_t capacity_ = 0;
     uint32_t node_capacity_ = 0;
+    uint32_t grow_to_ = 0;
+    uint64_t generation_ = 0;
+    uint32_t last_n_ = 0;
     int sm_count_ = 148;
     DeviceArray<unsigned long long> keys_[2];    // Morton codes (double-buffered)
     DeviceArray<uint32_t> perm_[2];              // particle index payload
-    DeviceArray<uint32_t> hist_;                 // radix histograms
+    DeviceArray<uint32_t> hist_;                 // digit histograms, then offsets
     DeviceArray<uint32_t> lookback_;             // onesweep tile status words
-    DeviceArray<uint32_t> tile_counter_;         // onesweep tile ticket counters
+    DeviceArray<uint32_t> tile_counter_;         // onesweep tile tickets
     DeviceArray<double> sorted_;                 // x, y, z, m in Morton order (FP64)
-    DeviceArray<float4> leaf_rel_;               // FP32 position - leaf centre, mass
-    DeviceArray<uint32_t> node_start_;           // nodes starting at each particle (+ scan)
-    DeviceArray<uint32_t> scan_partials_;        // decoupled scan tile status
-    DeviceArray<uint32_t> node_of_particle_;     // leaf index of each sorted particle
+    DeviceArray<float4> leaf_rel_;               // FP32 position - leaf centre of mass, mass
+    DeviceArray<uint32_t> node_start_;           // nodes starting at each particle + scan
+    DeviceArray<uint32_t> scan_partials_;        // block sums of the scan
     DeviceArray<DeviceNode> nodes_;
-    DeviceArray<DeviceQuadrupole> quads_;
-    DeviceArray<uint32_t> level_offsets_;        // nodes per level (upward pass)
-    DeviceArray<uint32_t> level_lists_;          // node indices grouped by level
-    DeviceArray<double> acc_sorted_;             // accelerations in Morton order
+    DeviceArray<DeviceQuadrupole> quads_;        // FP64 moments (parity, upward pass)
+    DeviceArray<float> quads32_;                 // FP32 copies the walk reads (8 per node)
+    DeviceArray<uint32_t> level_lists_;          // child counts, then arrival counts
     DeviceArray<TreeMeta> meta_;
     DeviceArray<double> reduce_;                 // cube min/max partials
+    DeviceArray<unsigned long long> counters_;   // pair and cell counts (accumulating)
 };
 
 } // namespace ob

@@ -1,0 +1,91 @@
+// Launch interface of the Barnes-Hut pipeline's kernels (sort.cu, tree.cu,
+// walk.cu). Raw device pointers; every launcher enqueues on `stream` only.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "tree.hpp"
+
+namespace ob {
+
+// ---------------------------------------------------------------- ordering
+
+// Radix sort geometry: 8-bit digits, 8 passes over the 63-bit codes.
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kRadixPasses = 8;
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr uint32_t kSortTile = kSortThreads * kSortItems;
+
+// Largest particle count the onesweep status words can carry (30-bit counts).
+constexpr uint32_t kMaxTreeParticles = (1u << 30) - 1;
+
+uint32_t sort_tiles(uint32_t n);
+size_t cube_partials_needed(uint32_t n);
+
+// Bounding cube (src/solvers/morton.cpp:60-104) into meta->origin/size and
+// meta->root_centre; `partials` holds 6 doubles per reduction block.
+cudaError_t launch_bounding_cube(const double *x, const double *y, const double *z, uint32_t n,
+                                 double *partials, TreeMeta *meta, cudaStream_t stream);
+
+// Morton codes (morton.cpp:128-164) with index payload, and the eight digit
+// histograms of the codes (hist: kRadixPasses x kRadix, zeroed beforehand).
+cudaError_t launch_encode(const double *x, const double *y, const double *z, uint32_t n,
+                          const TreeMeta *meta, unsigned long long *codes, uint32_t *indices,
+                          uint32_t *hist, cudaStream_t stream);
+
+// Exclusive scan of each pass's histogram, in place.
+cudaError_t launch_scan_histograms(uint32_t *hist, cudaStream_t stream);
+
+// One onesweep pass (stable) over digit `pass`. `lookback` holds
+// sort_tiles(n) * kRadix status words for this pass and `ticket` one counter,
+// both zeroed beforehand.
+cudaError_t launch_onesweep(const unsigned long long *keys_in, const uint32_t *vals_in,
+                            unsigned long long *keys_out, uint32_t *vals_out, uint32_t n,
+                            int pass, const uint32_t *offsets, uint32_t *lookback,
+                            uint32_t *ticket, unsigned *status, cudaStream_t stream);
+
+// sorted[k * n + i] = source_k[perm[i]] for x, y, z, m.
+cudaError_t launch_gather(const double *x, const double *y, const double *z, const double *m,
+                          const uint32_t *perm, uint32_t n, double *sorted, cudaStream_t stream);
+
+// Exclusive scan of n uint32 values into out[0..n] (out[n] = total). `scratch`
+// holds scan_partials_needed(n) words.
+size_t scan_partials_needed(uint32_t n);
+cudaError_t launch_exclusive_scan(const uint32_t *in, uint32_t *out, uint32_t n,
+                                  uint32_t *scratch, cudaStream_t stream);
+
+// ------------------------------------------------------------------ octree
+
+// Per sorted particle b: the number of octree nodes whose first particle is b.
+cudaError_t launch_layout_count(const unsigned long long *codes, uint32_t n, uint32_t leaf_cap,
+                                uint32_t *counts, cudaStream_t stream);
+
+// Writes the node records (escape, first, count, level, parent) and counts
+// each internal node's children. `offsets` is the exclusive scan of counts.
+cudaError_t launch_layout_write(const unsigned long long *codes, uint32_t n, uint32_t leaf_cap,
+                                const uint32_t *offsets, uint32_t node_capacity,
+                                DeviceNode *nodes, uint32_t *children, TreeMeta *meta,
+                                unsigned *status, cudaStream_t stream);
+
+// Moments bottom-up (mass, centre of mass, quadrupole, acceptance radius) and
+// the leaf-relative FP32 source positions the walk reads.
+cudaError_t launch_moments(const double *sorted, const unsigned long long *codes, uint32_t n,
+                           DeviceNode *nodes, DeviceQuadrupole *quads, float *quads32,
+                           const uint32_t *children, uint32_t *arrived, float4 *leaf_rel,
+                           TreeMeta *meta, double opening_angle, uint32_t node_capacity,
+                           cudaStream_t stream);
+
+// ------------------------------------------------------------------- walk
+
+// Accelerations written in the caller's (unsorted) order through perm;
+// pair and cell counts added to counters[0] and counters[1].
+cudaError_t launch_walk(const DeviceNode *nodes, const float *quads32, const float4 *leaf_rel,
+                        const double *sorted, const uint32_t *perm, uint32_t n, double eps2,
+                        double *ax, double *ay, double *az, TreeMeta *meta,
+                        unsigned long long *counters, cudaStream_t stream);
+
+} // namespace ob
