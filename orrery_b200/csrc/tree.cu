@@ -620,7 +620,9 @@ void TreePipeline::copy_tree(double *reals, uint64_t *idx, double *quads, uint32
         reals[5ull * k + 3] = nodes[k].com_z;
         reals[5ull * k + 4] = nodes[k].r2;
         idx[3ull * k + 0] = nodes[k].next;
-        idx[3ull * k + 1] = nodes[k].first;
+        // The reference sets first_particle on leaves only (octree.cpp:335-337);
+        // internal nodes keep their default of 0.
+        idx[3ull * k + 1] = nodes[k].count > 0 ? nodes[k].first : 0u;
         idx[3ull * k + 2] = nodes[k].count;
     }
     if (quads != nullptr && params_.quadrupole && h.node_count > 0) {
