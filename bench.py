@@ -9,6 +9,7 @@ Workloads (seeded synthetic inputs with the shapes of the measured configs):
                            force / FP64 state, velocity Verlet dt 5e-4; a step
                            is one VV step (Morton order, tree, walk, kicks).
                            Metric: BH ms/step at 2M (lower is better).
+  bh-collision-500k        the same scenario at 500,000 particles (profiling size).
   direct-plummer-4096      Plummer sphere N=4096, eps 0.01, FP32 direct, VV
                            dt 1e-3. Metric: direct Gint/s, N(N-1) per step.
   direct-plummer-262144    the same at N=262,144 with the split-precision
@@ -52,6 +53,11 @@ WORKLOADS = {
                             theta=0.5, leaf=32, quadrupole=True, precision="fp32",
                             metric="BH ms/step at 2M", unit="ms/step", higher=False,
                             generator="collision"),
+    # The same scenario at a quarter of the size, for profiler captures.
+    "bh-collision-500k": dict(kind="tree", n=500_000, eps=0.02, dt=5e-4, integrator="vv",
+                              theta=0.5, leaf=32, quadrupole=True, precision="fp32",
+                              metric="BH ms/step at 500k", unit="ms/step", higher=False,
+                              generator="collision"),
     "direct-plummer-4096": dict(kind="direct", n=4096, eps=0.01, dt=1e-3, integrator="vv",
                                 precision="fp32", metric="direct Gint/s", unit="Gint/s",
                                 higher=True, generator="plummer"),
@@ -60,7 +66,7 @@ WORKLOADS = {
                                   metric="direct Gint/s", unit="Gint/s", higher=True,
                                   generator="plummer"),
 }
-DEFAULT_WORKLOAD = "direct-plummer-4096"
+DEFAULT_WORKLOAD = "bh-collision-2m"
 
 
 def make_inputs(w, seed=20260811):
@@ -310,7 +316,7 @@ def e2e_drop_in(ob, w, data, steps, torch):
         step()
     sec = (time.perf_counter() - t0) / steps
     evals = len(weights)
-    return sec, evals * 4 * 8 * n, evals * 3 * 8 * n
+    return sec, evals * 4 * 8 * n, evals * 3 * 8 * n, solver
 
 
 def run_b200(args, w):
@@ -340,6 +346,7 @@ def run_b200(args, w):
         flush = torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=device)
 
     K = args.steps
+    counts_start = system.interaction_count()
     system.profile(K)
     sampler = ClockSampler(local)
     barrier(dist)
@@ -374,6 +381,9 @@ def run_b200(args, w):
     clocks = sampler.stop()
     total_ms = reduce_max(dist, total_ms, device)
     phases, evals = system.phase_times()
+    counts_end = system.interaction_count()
+    interactions = (counts_end.particle_particle + counts_end.particle_cell -
+                    counts_start.particle_particle - counts_start.particle_cell)
 
     ms_per_step = total_ms / K
     if w["unit"] == "ms/step":
@@ -395,17 +405,29 @@ def run_b200(args, w):
                     "kernel_ms": kernel_ms}
     else:
         hbm, src = load_peaks()
-        bytes_per_target = 16 + 24 + 12
-        achieved = bytes_per_target * n / (kernel_ms * 1e-3) / 1e9
-        roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                    "frac": achieved / hbm, "traffic": None,
-                    "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)",
-                    "kernel_ms": kernel_ms}
-
+        roofline = {"bound": "hbm", "peak": hbm, "unit": "GB/s",
+                    "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs, a copy kernel)",
+                    "kernel_ms": kernel_ms, "traffic": None}
+    line = None
     line = None
     if rank == 0:
         e2e_steps = max(2, min(K, 10 if w["kind"] == "tree" else 50))
-        sec, h2d, d2h = e2e_drop_in(ob, w, data, e2e_steps, torch)
+        sec, h2d, d2h, solver = e2e_drop_in(ob, w, data, e2e_steps, torch)
+        if w["kind"] == "tree":
+            nodes, leaves, depth = solver.tree_stats()
+            # Algorithmic bytes of one walk launch: each target's FP64 position
+            # (24 B) and permutation entry (4 B) read and FP64 acceleration
+            # (24 B) written, every leaf-relative source (16 B) and every node
+            # (64 B) and FP32 quadrupole (32 B) read once.
+            quad_bytes = 32 if w["quadrupole"] else 0
+            algorithmic = n * (24 + 4 + 24 + 16) + nodes * (64 + quad_bytes)
+            achieved = algorithmic / (kernel_ms * 1e-3) / 1e9
+            per_eval = interactions / max(1, K * evaluations_per_step(w))
+            roofline.update({"achieved": achieved, "frac": achieved / roofline["peak"],
+                             "algorithmic_bytes": algorithmic, "nodes": nodes,
+                             "leaves": leaves, "depth": depth,
+                             "interactions_per_walk": per_eval,
+                             "interaction_rate_gint_s": per_eval / (kernel_ms * 1e-3) / 1e9})
         if w["unit"] == "ms/step":
             e2e_value = sec * 1e3
         else:
