@@ -281,20 +281,36 @@ __device__ __forceinline__ uint32_t next_child(const DeviceNode *nodes, uint32_t
     return next > child ? next : stop;
 }
 
-__device__ void store_quads(DeviceQuadrupole *quads, float *quads32, uint32_t k,
-                            const DeviceQuadrupole &q) {
-    quads[k] = q;
-    float4 *w = reinterpret_cast<float4 *>(quads32 + 8ull * k);
-    w[0] = make_float4(__double2float_rn(q.xx), __double2float_rn(q.xy), __double2float_rn(q.xz),
-                       __double2float_rn(q.yy));
-    w[1] = make_float4(__double2float_rn(q.yz), __double2float_rn(q.zz), 0.0f, 0.0f);
+// Writes the walk's compact record of node k (see WalkNode).
+__device__ void store_walk_node(WalkNode *walk, uint32_t *first_of, uint32_t k,
+                                const DeviceNode &node, const DeviceQuadrupole *q) {
+    const float hx = __double2float_rn(node.com_x);
+    const float hy = __double2float_rn(node.com_y);
+    const float hz = __double2float_rn(node.com_z);
+    WalkNode w;
+    w.a = make_float4(hx, hy, hz, __double2float_rn(node.mass));
+    w.b = make_float4(__double2float_rn(__dsub_rn(node.com_x, static_cast<double>(hx))),
+                      __double2float_rn(__dsub_rn(node.com_y, static_cast<double>(hy))),
+                      __double2float_rn(__dsub_rn(node.com_z, static_cast<double>(hz))),
+                      __double2float_rn(node.r2));
+    if (q != nullptr) {
+        w.c = make_float4(__double2float_rn(q->xx), __double2float_rn(q->xy),
+                          __double2float_rn(q->xz), __double2float_rn(q->yy));
+        w.d = make_float4(__double2float_rn(q->yz), __double2float_rn(q->zz),
+                          __uint_as_float(node.next), __uint_as_float(node.count));
+    } else {
+        w.c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        w.d = make_float4(0.0f, 0.0f, __uint_as_float(node.next), __uint_as_float(node.count));
+    }
+    walk[k] = w;
+    first_of[k] = node.first;
 }
 
 __global__ void __launch_bounds__(kThreads)
     moments_kernel(const double *__restrict__ sorted, const unsigned long long *__restrict__ codes,
-                   uint32_t n, DeviceNode *nodes, DeviceQuadrupole *quads, float *quads32,
-                   const uint32_t *__restrict__ children, uint32_t *arrived, float4 *leaf_rel,
-                   TreeMeta *meta, double theta) {
+                   uint32_t n, DeviceNode *nodes, DeviceQuadrupole *quads, WalkNode *walk,
+                   uint32_t *first_of, const uint32_t *__restrict__ children, uint32_t *arrived,
+                   float4 *leaf_rel, TreeMeta *meta, double theta) {
     const double *X = sorted;
     const double *Y = sorted + n;
     const double *Z = sorted + 2ull * n;
@@ -346,8 +362,9 @@ __global__ void __launch_bounds__(kThreads)
         nodes[k].com_z = cz;
         nodes[k].r2 = acceptance(meta, codes[begin], level, cx, cy, cz, theta);
         if (with_quads) {
-            store_quads(quads, quads32, k, q);
+            quads[k] = q;
         }
+        store_walk_node(walk, first_of, k, nodes[k], with_quads ? &q : nullptr);
 
         // Climb while this thread completes its parent (gather_moments,
         // octree.cpp:142-185). A cell has at most 22 ancestors.
@@ -407,7 +424,7 @@ __global__ void __launch_bounds__(kThreads)
                                   __dsub_rn(__ldcg(&nodes[child].com_y), gy),
                                   __dsub_rn(__ldcg(&nodes[child].com_z), gz));
                 }
-                store_quads(quads, quads32, parent, moment);
+                quads[parent] = moment;
             }
             const uint32_t plevel = __ldcg(&nodes[parent].level);
             const uint32_t pfirst = __ldcg(&nodes[parent].first);
@@ -416,6 +433,19 @@ __global__ void __launch_bounds__(kThreads)
             nodes[parent].com_y = gy;
             nodes[parent].com_z = gz;
             nodes[parent].r2 = acceptance(meta, codes[pfirst], plevel, gx, gy, gz, theta);
+            {
+                DeviceNode copy;
+                copy.com_x = gx;
+                copy.com_y = gy;
+                copy.com_z = gz;
+                copy.mass = pm;
+                copy.r2 = nodes[parent].r2;
+                copy.next = stop;
+                copy.count = 0;
+                copy.first = pfirst;
+                const DeviceQuadrupole *pq = with_quads ? &quads[parent] : nullptr;
+                store_walk_node(walk, first_of, parent, copy, pq);
+            }
             current = parent;
         }
     }
@@ -442,12 +472,12 @@ cudaError_t launch_layout_write(const unsigned long long *codes, uint32_t n, uin
 }
 
 cudaError_t launch_moments(const double *sorted, const unsigned long long *codes, uint32_t n,
-                           DeviceNode *nodes, DeviceQuadrupole *quads, float *quads32,
-                           const uint32_t *children, uint32_t *arrived, float4 *leaf_rel,
-                           TreeMeta *meta, double opening_angle, uint32_t node_capacity,
-                           cudaStream_t stream) {
+                           DeviceNode *nodes, DeviceQuadrupole *quads, WalkNode *walk_nodes,
+                           uint32_t *first_of, const uint32_t *children, uint32_t *arrived,
+                           float4 *leaf_rel, TreeMeta *meta, double opening_angle,
+                           uint32_t node_capacity, cudaStream_t stream) {
     moments_kernel<<<grid_for(node_capacity), kThreads, 0, stream>>>(
-        sorted, codes, n, nodes, quads, quads32, children, arrived, leaf_rel, meta,
+        sorted, codes, n, nodes, quads, walk_nodes, first_of, children, arrived, leaf_rel, meta,
         opening_angle);
     return cudaGetLastError();
 }
@@ -501,8 +531,9 @@ void TreePipeline::reserve(uint32_t n) {
         nodes_.reserve(want);
         if (params_.quadrupole) {
             quads_.reserve(want);
-            quads32_.reserve(8ull * want);
         }
+        walk_nodes_.reserve(want);
+        first_of_.reserve(want);
         level_lists_.reserve(2ull * want); // children counts, then arrivals
         node_capacity_ = want;
     }
@@ -566,18 +597,17 @@ void TreePipeline::evaluate(uint32_t n, const double *x, const double *y, const 
                               meta_.data(), status, stream),
           "node layout");
     check(launch_moments(sorted_.data(), codes, n, nodes_.data(),
-                         params_.quadrupole ? quads_.data() : nullptr,
-                         params_.quadrupole ? quads32_.data() : nullptr, children, arrived,
-                         leaf_rel_.data(), meta_.data(), params_.opening_angle, node_capacity_,
-                         stream),
+                         params_.quadrupole ? quads_.data() : nullptr, walk_nodes_.data(),
+                         first_of_.data(), children, arrived, leaf_rel_.data(), meta_.data(),
+                         params_.opening_angle, node_capacity_, stream),
           "moments");
     record(built, stream, external);
 
     // Traversal.
-    check(launch_walk(nodes_.data(), params_.quadrupole ? quads32_.data() : nullptr,
-                      leaf_rel_.data(), sorted_.data(), perm, n,
-                      params_.softening * params_.softening, ax, ay, az, meta_.data(),
-                      counters_.data(), stream),
+    check(launch_walk(nodes_.data(), walk_nodes_.data(), first_of_.data(), leaf_rel_.data(),
+                      sorted_.data(), perm, n, params_.softening * params_.softening,
+                      params_.quadrupole != 0, ax, ay, az, meta_.data(), counters_.data(),
+                      stream),
           "tree walk");
 }
 

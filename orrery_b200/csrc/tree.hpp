@@ -30,6 +30,18 @@ struct alignas(16) DeviceNode {
 };
 static_assert(sizeof(DeviceNode) == 64, "DeviceNode is four 16-byte words");
 
+// The walk's compact copy of a node, four 16-byte words:
+//   a = (com_x hi, com_y hi, com_z hi, mass)       FP32
+//   b = (com_x lo, com_y lo, com_z lo, r2)         FP32 (r2 rounded to nearest)
+//   c = (Qxx, Qxy, Qxz, Qyy)                       FP32 quadrupole
+//   d = (Qyz, Qzz, next, count)                    next/count as uint32 bits
+// hi + lo carries each FP64 coordinate to ~2^-48 relative, so offsets to the
+// target (also split) come out in FP32 to ~1e-7 relative without conversions.
+struct alignas(16) WalkNode {
+    float4 a, b, c, d;
+};
+static_assert(sizeof(WalkNode) == 64, "WalkNode is four 16-byte words");
+
 // Traceless quadrupole (include/orrery/solvers/octree.hpp:89-96).
 struct DeviceQuadrupole {
     double xx, xy, xz, yy, yz, zz;
@@ -106,7 +118,8 @@ private:
     DeviceArray<uint32_t> scan_partials_;        // block sums of the scan
     DeviceArray<DeviceNode> nodes_;
     DeviceArray<DeviceQuadrupole> quads_;        // FP64 moments (parity, upward pass)
-    DeviceArray<float> quads32_;                 // FP32 copies the walk reads (8 per node)
+    DeviceArray<WalkNode> walk_nodes_;           // compact FP32 node records the walk reads
+    DeviceArray<uint32_t> first_of_;             // first particle of each node (leaves)
     DeviceArray<uint32_t> level_lists_;          // child counts, then arrival counts
     DeviceArray<TreeMeta> meta_;
     DeviceArray<double> reduce_;                 // cube min/max partials

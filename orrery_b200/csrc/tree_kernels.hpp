@@ -74,17 +74,18 @@ cudaError_t launch_layout_write(const unsigned long long *codes, uint32_t n, uin
 // Moments bottom-up (mass, centre of mass, quadrupole, acceptance radius) and
 // the leaf-relative FP32 source positions the walk reads.
 cudaError_t launch_moments(const double *sorted, const unsigned long long *codes, uint32_t n,
-                           DeviceNode *nodes, DeviceQuadrupole *quads, float *quads32,
-                           const uint32_t *children, uint32_t *arrived, float4 *leaf_rel,
-                           TreeMeta *meta, double opening_angle, uint32_t node_capacity,
-                           cudaStream_t stream);
+                           DeviceNode *nodes, DeviceQuadrupole *quads, WalkNode *walk_nodes,
+                           uint32_t *first_of, const uint32_t *children, uint32_t *arrived,
+                           float4 *leaf_rel, TreeMeta *meta, double opening_angle,
+                           uint32_t node_capacity, cudaStream_t stream);
 
 // ------------------------------------------------------------------- walk
 
 // Accelerations written in the caller's (unsorted) order through perm;
 // pair and cell counts added to counters[0] and counters[1].
-cudaError_t launch_walk(const DeviceNode *nodes, const float *quads32, const float4 *leaf_rel,
-                        const double *sorted, const uint32_t *perm, uint32_t n, double eps2,
+cudaError_t launch_walk(const DeviceNode *nodes, const WalkNode *walk_nodes,
+                        const uint32_t *first_of, const float4 *leaf_rel, const double *sorted,
+                        const uint32_t *perm, uint32_t n, double eps2, bool quadrupole,
                         double *ax, double *ay, double *az, TreeMeta *meta,
                         unsigned long long *counters, cudaStream_t stream);
 
