@@ -223,6 +223,10 @@ int ob_system_size(const ob_system *system, uint64_t *n);
  * benchmarks/cuda_probes.cu:15-115). */
 int ob_probe_fp32(double *ffma_lane_per_s, double *rsqrt_lane_per_s);
 
+/* Measured FMAs per second through packed FP32x2 FMA instructions (each
+ * counts as two), for comparison with the scalar FFMA rate. */
+int ob_probe_fp32x2(double *ffma2_flop_lanes_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -134,6 +134,7 @@ def load_library():
     lib.ob_system_counts.argtypes = [vp, C.POINTER(Counts)]
     lib.ob_system_size.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.ob_probe_fp32.argtypes = [_dp, _dp]
+    lib.ob_probe_fp32x2.argtypes = [_dp]
     _u64p = C.POINTER(C.c_uint64)
     lib.ob_tree_stats.argtypes = [vp, _u64p, _u64p, C.POINTER(C.c_uint32)]
     lib.ob_tree_copy.argtypes = [vp, _dp, _u64p, _dp]
@@ -457,6 +458,13 @@ def probe_fp32():
     a, b = C.c_double(), C.c_double()
     _check(load_library().ob_probe_fp32(C.byref(a), C.byref(b)))
     return a.value, b.value
+
+
+def probe_fp32x2() -> float:
+    """Measured FMAs per second issued as packed FP32x2 instructions."""
+    a = C.c_double()
+    _check(load_library().ob_probe_fp32x2(C.byref(a)))
+    return a.value
 
 
 def compute_accelerations(positions, masses, softening: float = 0.0, solver: str = "direct",

@@ -38,6 +38,32 @@ __global__ void __launch_bounds__(kProbeThreads) ffma_probe(float *out, int iter
     }
 }
 
+// Packed FP32x2 FMA (sm_100 FFMA2): each instruction does two FMAs.
+__global__ void __launch_bounds__(kProbeThreads) ffma2_probe(float *out, int iterations, float a,
+                                                             float b) {
+    float2 v[kChains];
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        v[k] = make_float2(threadIdx.x * 1e-3f + k, threadIdx.x * 2e-3f + k);
+    }
+    const float2 a2 = make_float2(a, a);
+    const float2 b2 = make_float2(b, b);
+    for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+        for (int k = 0; k < kChains; ++k) {
+            v[k] = __ffma2_rn(v[k], a2, b2);
+        }
+    }
+    float s = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        s += v[k].x + v[k].y;
+    }
+    if (s == 12345.678f) {
+        out[threadIdx.x] = s;
+    }
+}
+
 __global__ void __launch_bounds__(kProbeThreads) rsqrt_probe(float *out, int iterations) {
     float v[kChains];
 #pragma unroll
@@ -79,6 +105,28 @@ template <typename Launch> double lane_ops_per_second(Launch launch, double ops)
 
 } // namespace
 } // namespace ob
+
+extern "C" int ob_probe_fp32x2(double *ffma2_flop_lanes_per_s) {
+    try {
+        int device = 0, sms = 0;
+        ob::check(cudaGetDevice(&device), "cudaGetDevice");
+        ob::check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SMs");
+        float *sink = nullptr;
+        ob::check(cudaMalloc(&sink, ob::kProbeThreads * sizeof(float)), "probe buffer");
+        const int blocks = sms * 8;
+        const double threads = static_cast<double>(blocks) * ob::kProbeThreads;
+        const int iterations = 1 << 15;
+        *ffma2_flop_lanes_per_s = ob::lane_ops_per_second(
+            [&] {
+                ob::ffma2_probe<<<blocks, ob::kProbeThreads>>>(sink, iterations, 0.999f, 1e-3f);
+            },
+            threads * iterations * ob::kChains * 2.0);
+        cudaFree(sink);
+        return OB_OK;
+    } catch (const ob::Error &e) {
+        return ob::set_error(e.code(), e.what());
+    }
+}
 
 extern "C" int ob_probe_fp32(double *ffma_lane_per_s, double *rsqrt_lane_per_s) {
     try {
