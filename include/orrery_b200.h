@@ -55,14 +55,16 @@ extern "C" {
 #define OB_INTEGRATOR_VV 0
 #define OB_INTEGRATOR_YOSHIDA4 1
 
-/* Solver parameters. Mirrors core::Softening (softening.hpp:50-60, the
- * length; the square is used) and solvers::TreeParameters (octree.hpp:147-191;
+/* Solver parameters. Mirrors core::Softening (softening.hpp:50-60), which
+ * stores the square of the softening length -- pass Softening::squared() so
+ * FP64 results stay bit-identical -- and solvers::TreeParameters
+ * (octree.hpp:147-191;
  * defaults theta 0.5, leaf 32, no quadrupole; corrected like
  * corrected_parameters, octree.cpp:189-194). */
 typedef struct ob_solver_params {
     int32_t kind;           /* OB_SOLVER_* */
     int32_t precision;      /* OB_PRECISION_* */
-    double softening;       /* softening length epsilon (>= 0) */
+    double softening_squared; /* epsilon^2 (>= 0) */
     double opening_angle;   /* theta, clamped to [0, 1] (tree only) */
     uint64_t leaf_capacity; /* at least 1 (tree only) */
     int32_t quadrupole;     /* nonzero: carry traceless quadrupoles (tree only) */

@@ -56,7 +56,7 @@ class OrreryError(RuntimeError):
 
 
 class SolverParams(C.Structure):
-    _fields_ = [("kind", C.c_int32), ("precision", C.c_int32), ("softening", C.c_double),
+    _fields_ = [("kind", C.c_int32), ("precision", C.c_int32), ("softening_squared", C.c_double),
                 ("opening_angle", C.c_double), ("leaf_capacity", C.c_uint64),
                 ("quadrupole", C.c_int32), ("reserved", C.c_int32)]
 
@@ -173,7 +173,9 @@ def _ptr(a):
 def make_params(kind=SOLVER_DIRECT, precision="fp32", softening=0.0, opening_angle=0.5,
                 leaf_capacity=32, quadrupole=False) -> SolverParams:
     prec = _PRECISIONS[precision] if isinstance(precision, str) else int(precision)
-    return SolverParams(kind, prec, float(softening), float(opening_angle), int(leaf_capacity),
+    eps = float(softening)
+    # core::Softening keeps the square, formed as length * length.
+    return SolverParams(kind, prec, eps * eps, float(opening_angle), int(leaf_capacity),
                         1 if quadrupole else 0, 0)
 
 
@@ -213,7 +215,8 @@ class _Solver:
         return p
 
     def softening(self) -> float:
-        return self.params().softening
+        """The softening length (the square root of the stored square)."""
+        return float(np.sqrt(self.params().softening_squared))
 
     def evaluate(self, positions, masses, accelerations=None) -> np.ndarray:
         """ForceSolver::evaluate: positions (3, N) or (N, 3) FP64, masses (N,).

@@ -364,8 +364,8 @@ void System::energy(double *kinetic, double *potential) {
         *kinetic = compensated_sum(host) / 2.0;
     }
     if (potential != nullptr) {
-        const double eps = solver_->params().softening;
-        check(launch_potential_rows(array(kX), array(kY), array(kZ), array(kM), n_, eps * eps,
+        const double eps2 = solver_->params().softening_squared;
+        check(launch_potential_rows(array(kX), array(kY), array(kZ), array(kM), n_, eps2,
                                     terms_.data(), stream_),
               "potential energy rows");
         check(cudaMemcpyAsync(host.data(), terms_.data(), sizeof(double) * n_,

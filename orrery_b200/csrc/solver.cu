@@ -29,8 +29,8 @@ ob_solver_params corrected(const ob_solver_params &in) {
         throw Error(OB_ERROR_UNSUPPORTED,
                     "the tree solver computes FP32 forces on FP64 state (precision FP32)");
     }
-    if (!(p.softening >= 0.0) || !std::isfinite(p.softening)) {
-        throw Error(OB_ERROR_INVALID_ARGUMENT, "softening must be finite and >= 0");
+    if (!(p.softening_squared >= 0.0) || !std::isfinite(p.softening_squared)) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "softening squared must be finite and >= 0");
     }
     // corrected_parameters: theta clamped to [0, 1], leaf capacity >= 1.
     if (!(p.opening_angle >= 0.0)) {
@@ -98,7 +98,7 @@ void Solver::evaluate_direct(uint32_t n, const double *x, const double *y, const
                              const double *m, double *ax, double *ay, double *az,
                              cudaStream_t stream, cudaEvent_t ordered, cudaEvent_t built,
                              bool external) {
-    const double eps2d = params_.softening * params_.softening;
+    const double eps2d = params_.softening_squared;
     if (params_.precision == OB_PRECISION_FP64) {
         record(ordered, stream, external);
         record(built, stream, external);
@@ -155,7 +155,7 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
           "uploading autotune sources");
     DirectConfig candidates[64];
     const int count = direct_candidates(split, candidates, 64);
-    const auto eps2 = static_cast<float>(params_.softening * params_.softening + 1e-6);
+    const auto eps2 = static_cast<float>(params_.softening_squared + 1e-6);
     double best = 1e300;
     const double *d = dev.data();
     double *out = dev.data() + 4ull * n;

@@ -52,7 +52,10 @@ def test_invalid_parameters_are_rejected_before_the_device(lib):
     bad = ob.make_params(kind=7)
     assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
     assert handle.value is None
-    bad = ob.make_params(softening=-1.0)
+    bad = ob.make_params()
+    bad.softening_squared = -1.0
+    assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
+    bad.softening_squared = float("nan")
     assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
     bad = ob.make_params(kind=ob.SOLVER_TREE, precision="fp64")
     assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_UNSUPPORTED
