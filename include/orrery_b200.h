@@ -140,6 +140,23 @@ int ob_tree_copy(ob_solver *solver, double *reals, uint64_t *idx, double *quads)
 int ob_tree_copy_order(ob_solver *solver, uint64_t *codes, uint32_t *indices, double *origin,
                        double *size);
 
+/* Morton ordering (codes sorted ascending with their particle indices) of n
+ * particles whose FP64 positions are in device memory, written to the
+ * caller's device arrays codes[n] and indices[n], enqueued on `stream`
+ * without synchronising. It allocates nothing: for callers that cannot
+ * allocate device memory when they need an ordering -- code running in a
+ * stream or host callback, where calls that may synchronise are forbidden,
+ * and services that take device memory only from their own fixed pool.
+ * Every intermediate buffer lives in one fixed device array of about 14 MB
+ * that each device holds from the library's loading until the process exits;
+ * n above 1,048,576 is refused with OB_ERROR_CAPACITY. The first call on a
+ * device looks up that array's device address, so make it before any stream
+ * capture. All calls share the one array: calls whose work overlaps on the
+ * GPU race and must be ordered by the caller. No counterpart in the
+ * reference (its MortonOrdering allocates on the host). */
+int ob_morton_order_noalloc(uint64_t n, const double *x, const double *y, const double *z,
+                            uint64_t *codes, uint32_t *indices, void *stream);
+
 /* Tile shape of the direct kernels: threads per CTA, targets per thread and
  * the number of CTAs (one thread-block cluster) that split the sources of a
  * target tile. No reference counterpart: the reference picks one block size
