@@ -118,26 +118,35 @@ __device__ __forceinline__ void finish_targets(const DirectArgs &a, uint32_t t0,
     cluster.sync();
 }
 
+// Sources of the FP32 kernel are stored pre-duplicated, two float4 per
+// particle: (x, x, y, y) and (z, z, m, m), so that each half is already a
+// packed FP32x2 operand for a pair of targets and no register moves are needed.
 template <int THREADS, int R>
 __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a) {
+    static_assert(R % 2 == 0, "targets are processed in packed pairs");
+    constexpr int P = R / 2;
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr uint32_t BT = THREADS * R;
-    float4 *tiles = reinterpret_cast<float4 *>(smem);
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 2 * kDirectTile * sizeof(float4));
+    float4 *tiles = reinterpret_cast<float4 *>(smem); // 2 buffers x 2*kDirectTile
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 4 * kDirectTile * sizeof(float4));
     float *partial = reinterpret_cast<float *>(bars + 2);
 
     const uint32_t tid = threadIdx.x;
     const uint32_t t0 = blockIdx.y * BT;
-    const float eps2 = a.eps2;
+    const float2 eps2 = make_float2(a.eps2, a.eps2);
 
-    float px[R], py[R], pz[R], ax[R], ay[R], az[R];
+    // Target r = 2p + h is slot (2p + h) * THREADS + tid; pair p packs h = 0, 1.
+    float2 nx[P], ny[P], nz[P], ax[P], ay[P], az[P];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const float4 p = a.hi[t0 + r * THREADS + tid];
-        px[r] = p.x;
-        py[r] = p.y;
-        pz[r] = p.z;
-        ax[r] = ay[r] = az[r] = 0.0f;
+    for (int p = 0; p < P; ++p) {
+        const float4 u0 = a.hi[2ull * (t0 + (2 * p) * THREADS + tid)];
+        const float4 u1 = a.hi[2ull * (t0 + (2 * p) * THREADS + tid) + 1];
+        const float4 v0 = a.hi[2ull * (t0 + (2 * p + 1) * THREADS + tid)];
+        const float4 v1 = a.hi[2ull * (t0 + (2 * p + 1) * THREADS + tid) + 1];
+        nx[p] = make_float2(-u0.x, -v0.x);
+        ny[p] = make_float2(-u0.z, -v0.z);
+        nz[p] = make_float2(-u1.x, -v1.x);
+        ax[p] = ay[p] = az[p] = make_float2(0.0f, 0.0f);
     }
 
     uint32_t tb, te;
@@ -148,9 +157,15 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
         fence_barrier_init();
     }
     __syncthreads();
+    constexpr uint32_t tile_bytes = 2 * kDirectTile * sizeof(float4);
+    auto stage = [&](uint32_t k, uint32_t buf) {
+        mbar_arrive_expect_tx(&bars[buf], tile_bytes);
+        bulk_copy_g2s(tiles + buf * 2 * kDirectTile,
+                      a.hi + 2ull * static_cast<size_t>(k) * kDirectTile, tile_bytes, &bars[buf]);
+    };
     if (tid == 0) {
         for (uint32_t k = tb; k < min(tb + 2, te); ++k) {
-            stage_tile<false>(a, tiles, nullptr, bars, k, k - tb);
+            stage(k, k - tb);
         }
     }
 
@@ -162,45 +177,58 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
             ok = mbar_wait_bounded(&bars[buf], (it >> 1) & 1u, a.status);
         }
         if (ok) {
-            const float4 *tile = tiles + buf * kDirectTile;
+            const float4 *tile = tiles + buf * 2 * kDirectTile;
             const uint32_t j0 = k * kDirectTile;
             const bool masked = (j0 + kDirectTile > a.n) || (j0 < t0 + BT && t0 < j0 + kDirectTile);
             if (!masked) {
-#pragma unroll 4
+#pragma unroll 2
                 for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
-                    const float4 s = tile[jj];
+                    const float4 s0 = tile[2 * jj];     // (x, x, y, y)
+                    const float4 s1 = tile[2 * jj + 1]; // (z, z, m, m)
+                    const float2 sx = make_float2(s0.x, s0.y);
+                    const float2 sy = make_float2(s0.z, s0.w);
+                    const float2 sz = make_float2(s1.x, s1.y);
+                    const float2 sm = make_float2(s1.z, s1.w);
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const float dx = s.x - px[r];
-                        const float dy = s.y - py[r];
-                        const float dz = s.z - pz[r];
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-                        const float inv = rsqrt_approx(r2);
-                        const float f = (s.w * inv) * (inv * inv);
-                        ax[r] = fmaf(f, dx, ax[r]);
-                        ay[r] = fmaf(f, dy, ay[r]);
-                        az[r] = fmaf(f, dz, az[r]);
+                    for (int p = 0; p < P; ++p) {
+                        const float2 dx = __fadd2_rn(sx, nx[p]);
+                        const float2 dy = __fadd2_rn(sy, ny[p]);
+                        const float2 dz = __fadd2_rn(sz, nz[p]);
+                        float2 r2 = __ffma2_rn(dx, dx, eps2);
+                        r2 = __ffma2_rn(dy, dy, r2);
+                        r2 = __ffma2_rn(dz, dz, r2);
+                        const float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                        const float2 f = __fmul2_rn(__fmul2_rn(sm, inv), __fmul2_rn(inv, inv));
+                        ax[p] = __ffma2_rn(f, dx, ax[p]);
+                        ay[p] = __ffma2_rn(f, dy, ay[p]);
+                        az[p] = __ffma2_rn(f, dz, az[p]);
                     }
                 }
             } else {
                 for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
-                    const float4 s = tile[jj];
+                    const float4 s0 = tile[2 * jj];
+                    const float4 s1 = tile[2 * jj + 1];
                     const uint32_t j = j0 + jj;
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const uint32_t i = t0 + r * THREADS + tid;
-                        const bool skip = (j == i) || (j >= a.n);
-                        const float dx = s.x - px[r];
-                        const float dy = s.y - py[r];
-                        const float dz = s.z - pz[r];
-                        const float r2 =
-                            skip ? 1.0f : fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-                        const float w = skip ? 0.0f : s.w;
-                        const float inv = rsqrt_approx(r2);
-                        const float f = (w * inv) * (inv * inv);
-                        ax[r] = fmaf(f, dx, ax[r]);
-                        ay[r] = fmaf(f, dy, ay[r]);
-                        az[r] = fmaf(f, dz, az[r]);
+                    for (int p = 0; p < P; ++p) {
+                        const uint32_t i0 = t0 + (2 * p) * THREADS + tid;
+                        const uint32_t i1 = i0 + THREADS;
+                        const bool skip0 = (j == i0) || (j >= a.n);
+                        const bool skip1 = (j == i1) || (j >= a.n);
+                        const float2 dx = __fadd2_rn(make_float2(s0.x, s0.y), nx[p]);
+                        const float2 dy = __fadd2_rn(make_float2(s0.z, s0.w), ny[p]);
+                        const float2 dz = __fadd2_rn(make_float2(s1.x, s1.y), nz[p]);
+                        float2 r2 = __ffma2_rn(dx, dx, eps2);
+                        r2 = __ffma2_rn(dy, dy, r2);
+                        r2 = __ffma2_rn(dz, dz, r2);
+                        r2.x = skip0 ? 1.0f : r2.x;
+                        r2.y = skip1 ? 1.0f : r2.y;
+                        const float2 w = make_float2(skip0 ? 0.0f : s1.z, skip1 ? 0.0f : s1.w);
+                        const float2 inv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                        const float2 f = __fmul2_rn(__fmul2_rn(w, inv), __fmul2_rn(inv, inv));
+                        ax[p] = __ffma2_rn(f, dx, ax[p]);
+                        ay[p] = __ffma2_rn(f, dy, ay[p]);
+                        az[p] = __ffma2_rn(f, dz, az[p]);
                     }
                 }
             }
@@ -208,16 +236,19 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
         __syncthreads();
         if (tid == 0 && ok && k + 2 < te) {
             fence_proxy_async_shared();
-            stage_tile<false>(a, tiles, nullptr, bars, k + 2, buf);
+            stage(k + 2, buf);
         }
     }
 
     double sx[R], sy[R], sz[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        sx[r] = ax[r];
-        sy[r] = ay[r];
-        sz[r] = az[r];
+    for (int p = 0; p < P; ++p) {
+        sx[2 * p] = ax[p].x;
+        sx[2 * p + 1] = ax[p].y;
+        sy[2 * p] = ay[p].x;
+        sy[2 * p + 1] = ay[p].y;
+        sz[2 * p] = az[p].x;
+        sz[2 * p + 1] = az[p].y;
     }
     finish_targets<THREADS, R, float>(a, t0, partial, sx, sy, sz);
 }
@@ -398,36 +429,45 @@ __global__ void __launch_bounds__(kF64Threads)
     }
 }
 
+// Packs FP64 SoA into the kernels' source layout. FP32 form (lo == nullptr):
+// two float4 per particle, (x, x, y, y) and (z, z, m, m). Split form: hi =
+// (x, y, z, m) rounded, lo = (x - hi, y - hi, z - hi, 0).
 __global__ void pack_kernel(const double *__restrict__ x, const double *__restrict__ y,
                             const double *__restrict__ z, const double *__restrict__ m,
                             uint32_t n, uint32_t padded, float4 *hi, float4 *lo) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < padded;
          i += gridDim.x * blockDim.x) {
-        if (i < n) {
-            const double X = x[i], Y = y[i], Z = z[i];
-            const float hx = __double2float_rn(X);
-            const float hy = __double2float_rn(Y);
-            const float hz = __double2float_rn(Z);
-            hi[i] = make_float4(hx, hy, hz, __double2float_rn(m[i]));
-            if (lo != nullptr) {
-                // X - hx is exact in FP64; rounding it gives the low part.
-                lo[i] = make_float4(__double2float_rn(X - static_cast<double>(hx)),
-                                    __double2float_rn(Y - static_cast<double>(hy)),
-                                    __double2float_rn(Z - static_cast<double>(hz)), 0.0f);
-            }
+        const bool real = i < n;
+        const double X = real ? x[i] : 0.0, Y = real ? y[i] : 0.0, Z = real ? z[i] : 0.0;
+        const float hx = __double2float_rn(X);
+        const float hy = __double2float_rn(Y);
+        const float hz = __double2float_rn(Z);
+        const float hm = real ? __double2float_rn(m[i]) : 0.0f;
+        if (lo == nullptr) {
+            hi[2ull * i] = make_float4(hx, hx, hy, hy);
+            hi[2ull * i + 1] = make_float4(hz, hz, hm, hm);
         } else {
-            hi[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (lo != nullptr) {
-                lo[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            }
+            hi[i] = make_float4(hx, hy, hz, hm);
+            // X - hx is exact in FP64; rounding it gives the low part.
+            lo[i] = make_float4(__double2float_rn(X - static_cast<double>(hx)),
+                                __double2float_rn(Y - static_cast<double>(hy)),
+                                __double2float_rn(Z - static_cast<double>(hz)), 0.0f);
         }
     }
 }
 
 template <int THREADS, int R, bool SPLIT> size_t direct_smem_bytes() {
-    const size_t tiles = (SPLIT ? 4 : 2) * kDirectTile * sizeof(float4);
+    const size_t tiles = 4 * kDirectTile * sizeof(float4);
     const size_t partial = 3 * THREADS * R * (SPLIT ? sizeof(double) : sizeof(float));
     return tiles + 2 * sizeof(uint64_t) + partial;
+}
+
+template <int THREADS, int R, bool SPLIT> auto direct_kernel_for() {
+    if constexpr (SPLIT) {
+        return direct_split_kernel<THREADS, R>;
+    } else {
+        return direct_f32_kernel<THREADS, R>;
+    }
 }
 
 template <int THREADS, int R, bool SPLIT>
@@ -435,7 +475,7 @@ cudaError_t launch_direct_t(const DirectArgs &args, int split, cudaStream_t stre
     const uint32_t bt = THREADS * R;
     const dim3 grid(static_cast<unsigned>(split), ceil_div(args.n, bt), 1);
     const size_t smem = direct_smem_bytes<THREADS, R, SPLIT>();
-    auto kernel = SPLIT ? direct_split_kernel<THREADS, R> : direct_f32_kernel<THREADS, R>;
+    auto kernel = direct_kernel_for<THREADS, R, SPLIT>();
     // Set once per process (one process drives one device), before any graph
     // capture reaches this launch.
     static const cudaError_t configured = cudaFuncSetAttribute(
@@ -463,13 +503,14 @@ cudaError_t dispatch_direct(const DirectArgs &args, const DirectConfig &c, cudaS
 #define OB_DIRECT_CASE(T, RR)                                                                      \
     if (c.threads == T && c.targets_per_thread == RR)                                              \
         return launch_direct_t<T, RR, SPLIT>(args, c.split, stream);
-    OB_DIRECT_CASE(128, 1)
     OB_DIRECT_CASE(128, 2)
     OB_DIRECT_CASE(128, 4)
-    OB_DIRECT_CASE(256, 1)
     OB_DIRECT_CASE(256, 2)
     OB_DIRECT_CASE(256, 4)
-    if (!SPLIT) {
+    if constexpr (SPLIT) {
+        OB_DIRECT_CASE(128, 1)
+        OB_DIRECT_CASE(256, 1)
+    } else {
         OB_DIRECT_CASE(128, 8)
         OB_DIRECT_CASE(256, 8)
     }
@@ -539,9 +580,12 @@ cudaError_t launch_direct_f64(const double *x, const double *y, const double *z,
 }
 
 int direct_candidates(bool split, DirectConfig *out, int capacity) {
-    static const int shapes[][2] = {{128, 1}, {128, 2}, {128, 4}, {256, 1},
-                                    {256, 2}, {256, 4}, {128, 8}, {256, 8}};
-    const int shape_count = split ? 6 : 8;
+    static const int split_shapes[][2] = {{128, 1}, {128, 2}, {128, 4},
+                                          {256, 1}, {256, 2}, {256, 4}};
+    static const int fp32_shapes[][2] = {{128, 2}, {128, 4}, {128, 8},
+                                         {256, 2}, {256, 4}, {256, 8}};
+    const int(*shapes)[2] = split ? split_shapes : fp32_shapes;
+    const int shape_count = 6;
     static const int splits[] = {1, 2, 4, 8};
     int count = 0;
     for (int s = 0; s < shape_count; ++s) {
@@ -559,9 +603,10 @@ DirectConfig direct_default_config(uint32_t n, bool split, int sm_count) {
     DirectConfig c;
     c.threads = split ? 128 : 256;
     c.targets_per_thread = split ? 2 : 4;
+    const int smallest = split ? 1 : 2;
     // Shrink the target tile until the targets alone give every SM work.
     const uint32_t want = static_cast<uint32_t>(sm_count > 0 ? sm_count : 148) * 2u;
-    while (c.targets_per_thread > 1 &&
+    while (c.targets_per_thread > smallest &&
            ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread)) < want) {
         c.targets_per_thread /= 2;
     }

@@ -23,8 +23,10 @@ constexpr uint32_t kDirectTile = 512;
 // Length the packed source arrays must be padded to for a configuration.
 uint32_t direct_padded_count(uint32_t n, const DirectConfig &config);
 
-// Packs FP64 SoA (x, y, z, m) into float4 (x, y, z, m), zero-padded to
-// `padded`. For the split form also writes the low parts (x - hi, ...).
+// Packs FP64 SoA into the direct kernels' source layout, zero-padded to
+// `padded` particles. FP32 form (lo == nullptr): 2 * padded float4 in `hi`,
+// (x, x, y, y) and (z, z, m, m) per particle. Split form: `hi` = (x, y, z, m)
+// rounded and `lo` = (x - hi, y - hi, z - hi, 0), padded float4 each.
 cudaError_t pack_sources(const double *x, const double *y, const double *z, const double *m,
                          uint32_t n, uint32_t padded, float4 *hi, float4 *lo,
                          cudaStream_t stream);

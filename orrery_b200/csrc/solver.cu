@@ -108,7 +108,7 @@ void Solver::evaluate_direct(uint32_t n, const double *x, const double *y, const
     const bool split = params_.precision == OB_PRECISION_SPLIT;
     const DirectConfig config = direct_config(n);
     const uint32_t padded = direct_padded_count(n, config);
-    if (hi_.reserve(padded)) {
+    if (hi_.reserve(split ? padded : 2ull * padded)) {
         ++generation_;
     }
     if (split && lo_.reserve(padded)) {
@@ -165,7 +165,7 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
             continue;
         }
         const uint32_t padded = direct_padded_count(n, c);
-        hi_.reserve(padded);
+        hi_.reserve(split ? padded : 2ull * padded);
         if (split) {
             lo_.reserve(padded);
         }
