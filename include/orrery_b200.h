@@ -233,6 +233,10 @@ int ob_system_phase_times(ob_system *system, ob_timings *average, uint32_t *eval
  * captured step graph). */
 int ob_system_step_kernels(ob_system *system, int32_t integrator, double dt, uint32_t *kernels);
 
+/* Runs ob_solver_autotune for the system's direct solver at its size and uses
+ * the chosen shape from the next step on (the step graph is captured again). */
+int ob_system_autotune(ob_system *system, ob_direct_shape *chosen, double *best_ms);
+
 int ob_system_counts(ob_system *system, ob_counts *counts);
 int ob_system_size(const ob_system *system, uint64_t *n);
 

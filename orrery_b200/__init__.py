@@ -140,6 +140,7 @@ def load_library():
     lib.ob_tree_copy.argtypes = [vp, _dp, _u64p, _dp]
     lib.ob_tree_copy_order.argtypes = [vp, _u64p, C.POINTER(C.c_uint32), _dp, _dp]
     lib.ob_system_stream.argtypes = [vp, C.POINTER(vp)]
+    lib.ob_system_autotune.argtypes = [vp, C.POINTER(DirectShape), C.POINTER(C.c_double)]
     lib.ob_system_profile.argtypes = [vp, C.c_uint32]
     lib.ob_system_phase_times.argtypes = [vp, C.POINTER(Timings), C.POINTER(C.c_uint32)]
     lib.ob_system_step_kernels.argtypes = [vp, C.c_int32, C.c_double, C.POINTER(C.c_uint32)]
@@ -430,6 +431,13 @@ class DeviceSystem:
         c = Counts()
         _check(self._lib.ob_system_counts(self._handle, C.byref(c)))
         return InteractionCount(c.evaluations, c.particle_particle, c.particle_cell)
+
+    def autotune(self):
+        """Times every direct kernel shape at this system's size and keeps the best."""
+        s = DirectShape()
+        ms = C.c_double()
+        _check(self._lib.ob_system_autotune(self._handle, C.byref(s), C.byref(ms)))
+        return (s.threads, s.targets_per_thread, s.split), ms.value
 
     def stream(self) -> int:
         """The cudaStream_t (as an integer) the system enqueues its work on."""

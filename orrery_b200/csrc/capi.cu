@@ -625,6 +625,20 @@ int ob_system_counts(ob_system *system, ob_counts *counts) {
     });
 }
 
+int ob_system_autotune(ob_system *system, ob_direct_shape *chosen, double *best_ms) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        ob::DirectConfig c;
+        const double ms = system->impl->solver().autotune(system->impl->size(), c);
+        if (chosen != nullptr) {
+            *chosen = ob_direct_shape{c.threads, c.targets_per_thread, c.split, 0};
+        }
+        if (best_ms != nullptr) {
+            *best_ms = ms;
+        }
+    });
+}
+
 int ob_system_stream(ob_system *system, void **stream) {
     return guarded([&] {
         require(system != nullptr && stream != nullptr, "NULL argument");

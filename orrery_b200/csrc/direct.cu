@@ -600,23 +600,26 @@ int direct_candidates(bool split, DirectConfig *out, int capacity) {
 }
 
 DirectConfig direct_default_config(uint32_t n, bool split, int sm_count) {
+    // Start from the widest register tile (most interactions per shared-memory
+    // read), then trade it for CTAs while the grid cannot fill the SMs, and
+    // split the sources across a cluster for what is still missing (the
+    // shapes the autotuner picks on B200 follow this pattern).
+    const uint32_t sms = static_cast<uint32_t>(sm_count > 0 ? sm_count : 148);
     DirectConfig c;
-    c.threads = split ? 128 : 256;
-    c.targets_per_thread = split ? 2 : 4;
+    c.threads = split ? 256 : 256;
+    c.targets_per_thread = split ? 4 : 8;
     const int smallest = split ? 1 : 2;
-    // Shrink the target tile until the targets alone give every SM work.
-    const uint32_t want = static_cast<uint32_t>(sm_count > 0 ? sm_count : 148) * 2u;
-    while (c.targets_per_thread > smallest &&
-           ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread)) < want) {
+    const uint32_t tiles = ceil_div(n, kDirectTile);
+    auto blocks = [&]() {
+        return ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread));
+    };
+    while (blocks() * 8u < sms && c.targets_per_thread > smallest) {
         c.targets_per_thread /= 2;
     }
-    if (c.threads > 128 && ceil_div(n, static_cast<uint32_t>(c.threads)) < want) {
+    if (blocks() * 8u < sms) {
         c.threads = 128;
     }
-    // Then split the sources across a cluster for what is still missing.
-    const uint32_t blocks = ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread));
-    const uint32_t tiles = ceil_div(n, kDirectTile);
-    while (c.split < 8 && blocks * static_cast<uint32_t>(c.split) < want &&
+    while (c.split < 8 && blocks() * static_cast<uint32_t>(c.split) < 8u * sms &&
            static_cast<uint32_t>(c.split * 2) <= tiles) {
         c.split *= 2;
     }

@@ -8,6 +8,9 @@
 // and only the accelerations come back.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <utility>
 #include <vector>
 
 #include "common.cuh"
@@ -83,10 +86,37 @@ Solver::~Solver() {
     }
 }
 
+namespace {
+// Shapes the autotuner chose, shared by every solver in the process, keyed by
+// (precision, n).
+std::mutex g_tuned_mutex;
+std::map<std::pair<int, uint32_t>, DirectConfig> g_tuned;
+} // namespace
+
+bool tuned_shape(int precision, uint32_t n, DirectConfig &out) {
+    std::lock_guard<std::mutex> lock(g_tuned_mutex);
+    const auto it = g_tuned.find({precision, n});
+    if (it == g_tuned.end()) {
+        return false;
+    }
+    out = it->second;
+    return true;
+}
+
+void remember_shape(int precision, uint32_t n, const DirectConfig &c) {
+    std::lock_guard<std::mutex> lock(g_tuned_mutex);
+    g_tuned[{precision, n}] = c;
+}
+
 DirectConfig Solver::direct_config(uint32_t n) {
     const auto it = configs_.find(n);
     if (it != configs_.end()) {
         return it->second;
+    }
+    DirectConfig tuned;
+    if (tuned_shape(params_.precision, n, tuned)) {
+        configs_[n] = tuned;
+        return tuned;
     }
     const DirectConfig c =
         direct_default_config(n, params_.precision == OB_PRECISION_SPLIT, sm_count_);
@@ -183,7 +213,7 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
             cudaGetLastError();
             continue;
         }
-        const int reps = 5;
+        const int reps = 2;
         check(cudaEventRecord(events_[0], stream_), "recording an event");
         for (int r = 0; r < reps; ++r) {
             check(launch(), "autotune launch");
@@ -204,6 +234,7 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
         throw Error(OB_ERROR_CUDA, "no direct kernel shape could be launched");
     }
     configs_[n] = chosen;
+    remember_shape(params_.precision, n, chosen);
     ++generation_;
     return best;
 }
