@@ -240,6 +240,48 @@ int ob_system_autotune(ob_system *system, ob_direct_shape *chosen, double *best_
 int ob_system_counts(ob_system *system, ob_counts *counts);
 int ob_system_size(const ob_system *system, uint64_t *n);
 
+/* ------------------------------------------------------------------------ */
+/* Batch: many independent systems integrated together                       */
+/* ------------------------------------------------------------------------ */
+/* No reference counterpart: the reference integrates one system per
+ * Simulation with one Softening per solver. A batch holds `systems` systems
+ * of uneven size, each with its own squared softening (> 0), in HBM; one
+ * persistent launch evaluates all their direct sums (precision form: split
+ * FP32 pair arithmetic, FP64 accumulation) from a largest-first work queue of
+ * (system, target tile, source chunk) items, and a step of all systems is one
+ * replayed CUDA graph. */
+typedef struct ob_batch ob_batch;
+
+typedef struct ob_batch_shape {
+    int32_t threads;
+    int32_t targets_per_thread;
+    uint32_t chunk_tiles; /* 512-source tiles per work item; 0 = a whole system */
+    int32_t reserved;
+} ob_batch_shape;
+
+int ob_batch_create(uint32_t systems, const uint64_t *counts, const double *softening_squared,
+                    ob_batch **out);
+void ob_batch_destroy(ob_batch *batch);
+int ob_batch_set_state(ob_batch *batch, uint32_t system, const double *x, const double *y,
+                       const double *z, const double *vx, const double *vy, const double *vz,
+                       const double *m);
+int ob_batch_get_state(ob_batch *batch, uint32_t system, double *x, double *y, double *z,
+                       double *vx, double *vy, double *vz, double *ax, double *ay, double *az);
+/* Evaluates every system's accelerations from its positions (after set_state). */
+int ob_batch_refresh(ob_batch *batch);
+int ob_batch_step(ob_batch *batch, int32_t integrator, double dt, uint64_t steps);
+int ob_batch_step_async(ob_batch *batch, int32_t integrator, double dt, uint64_t steps);
+int ob_batch_synchronize(ob_batch *batch);
+int ob_batch_energy(ob_batch *batch, uint32_t system, double *kinetic, double *potential);
+/* Times the implemented shapes on this batch and keeps the fastest. */
+int ob_batch_autotune(ob_batch *batch, ob_batch_shape *chosen, double *best_ms);
+int ob_batch_set_shape(ob_batch *batch, const ob_batch_shape *shape);
+/* Pair interactions of one evaluation of all systems (sum of N(N-1)),
+ * evaluations so far, and work items per evaluation. */
+int ob_batch_stats(ob_batch *batch, uint64_t *pairs_per_evaluation, uint64_t *evaluations,
+                   uint32_t *items);
+int ob_batch_stream(ob_batch *batch, void **stream);
+
 /* Measured FP32 FFMA and SFU rsqrt lane operations per second on the current
  * device: the denominators of the direct kernel's roofline. No reference
  * counterpart in the library (the reference's probes are benchmark code,

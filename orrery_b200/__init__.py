@@ -71,6 +71,11 @@ class DirectShape(C.Structure):
                 ("split", C.c_int32), ("reserved", C.c_int32)]
 
 
+class BatchShape(C.Structure):
+    _fields_ = [("threads", C.c_int32), ("targets_per_thread", C.c_int32),
+                ("chunk_tiles", C.c_uint32), ("reserved", C.c_int32)]
+
+
 class Timings(C.Structure):
     _fields_ = [("transfer_in_ms", C.c_double), ("ordering_ms", C.c_double),
                 ("construction_ms", C.c_double), ("traversal_ms", C.c_double),
@@ -144,6 +149,21 @@ def load_library():
     lib.ob_system_profile.argtypes = [vp, C.c_uint32]
     lib.ob_system_phase_times.argtypes = [vp, C.POINTER(Timings), C.POINTER(C.c_uint32)]
     lib.ob_system_step_kernels.argtypes = [vp, C.c_int32, C.c_double, C.POINTER(C.c_uint32)]
+    lib.ob_batch_create.argtypes = [C.c_uint32, C.POINTER(C.c_uint64), _dp, C.POINTER(vp)]
+    lib.ob_batch_destroy.argtypes = [vp]
+    lib.ob_batch_destroy.restype = None
+    lib.ob_batch_set_state.argtypes = [vp, C.c_uint32] + [_dp] * 7
+    lib.ob_batch_get_state.argtypes = [vp, C.c_uint32] + [_dp] * 9
+    lib.ob_batch_refresh.argtypes = [vp]
+    lib.ob_batch_step.argtypes = [vp, C.c_int32, C.c_double, C.c_uint64]
+    lib.ob_batch_step_async.argtypes = [vp, C.c_int32, C.c_double, C.c_uint64]
+    lib.ob_batch_synchronize.argtypes = [vp]
+    lib.ob_batch_energy.argtypes = [vp, C.c_uint32, _dp, _dp]
+    lib.ob_batch_autotune.argtypes = [vp, C.POINTER(BatchShape), C.POINTER(C.c_double)]
+    lib.ob_batch_set_shape.argtypes = [vp, C.POINTER(BatchShape)]
+    lib.ob_batch_stats.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_uint32)]
+    lib.ob_batch_stream.argtypes = [vp, C.POINTER(vp)]
     _lib = lib
     return lib
 
@@ -476,6 +496,84 @@ def probe_fp32x2() -> float:
     a = C.c_double()
     _check(load_library().ob_probe_fp32x2(C.byref(a)))
     return a.value
+
+
+class DeviceBatch:
+    """Many independent systems of uneven size, each with its own softening,
+    evaluated in one persistent launch and stepped together (precision form:
+    split FP32 pair arithmetic with FP64 accumulation)."""
+
+    KEYS = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+
+    def __init__(self, counts, softenings):
+        lib = load_library()
+        counts = np.ascontiguousarray(counts, dtype=np.uint64)
+        eps = np.asarray(softenings, dtype=np.float64)
+        eps2 = np.ascontiguousarray(eps * eps)
+        handle = C.c_void_p()
+        _check(lib.ob_batch_create(len(counts), counts.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                   _ptr(eps2), C.byref(handle)))
+        self._lib = lib
+        self._handle = handle
+        self.counts = [int(c) for c in counts]
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            self._lib.ob_batch_destroy(h)
+            self._handle = None
+
+    def set_state(self, system, x, y, z, vx=None, vy=None, vz=None, m=None) -> None:
+        arrs = [_f64(a) if a is not None else None for a in (x, y, z, vx, vy, vz, m)]
+        _check(self._lib.ob_batch_set_state(self._handle, int(system),
+                                            *(_ptr(a) for a in arrs)))
+
+    def refresh(self) -> None:
+        _check(self._lib.ob_batch_refresh(self._handle))
+
+    def state(self, system) -> dict:
+        n = self.counts[system]
+        out = {k: np.empty(n) for k in self.KEYS}
+        _check(self._lib.ob_batch_get_state(self._handle, int(system),
+                                            *(_ptr(out[k]) for k in self.KEYS)))
+        return out
+
+    def step(self, dt: float, steps: int = 1, integrator: str = "yoshida4") -> None:
+        _check(self._lib.ob_batch_step(self._handle, _INTEGRATORS[integrator], float(dt),
+                                       int(steps)))
+
+    def step_async(self, dt: float, steps: int = 1, integrator: str = "yoshida4") -> None:
+        _check(self._lib.ob_batch_step_async(self._handle, _INTEGRATORS[integrator], float(dt),
+                                             int(steps)))
+
+    def synchronize(self) -> None:
+        _check(self._lib.ob_batch_synchronize(self._handle))
+
+    def energy(self, system):
+        ke, pe = C.c_double(), C.c_double()
+        _check(self._lib.ob_batch_energy(self._handle, int(system), C.byref(ke), C.byref(pe)))
+        return ke.value, pe.value
+
+    def autotune(self):
+        s = BatchShape()
+        ms = C.c_double()
+        _check(self._lib.ob_batch_autotune(self._handle, C.byref(s), C.byref(ms)))
+        return (s.threads, s.targets_per_thread, s.chunk_tiles), ms.value
+
+    def set_shape(self, threads, targets_per_thread, chunk_tiles) -> None:
+        s = BatchShape(threads, targets_per_thread, chunk_tiles, 0)
+        _check(self._lib.ob_batch_set_shape(self._handle, C.byref(s)))
+
+    def stats(self):
+        pairs, evals, items = C.c_uint64(), C.c_uint64(), C.c_uint32()
+        _check(self._lib.ob_batch_stats(self._handle, C.byref(pairs), C.byref(evals),
+                                        C.byref(items)))
+        return pairs.value, evals.value, items.value
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(self._lib.ob_batch_stream(self._handle, C.byref(s)))
+        return s.value or 0
 
 
 def compute_accelerations(positions, masses, softening: float = 0.0, solver: str = "direct",

@@ -1,0 +1,577 @@
+// Batched direct sums: many systems of uneven size in one persistent launch.
+//
+// Work is a queue of (system, target tile, source chunk) items, ordered
+// largest first and pulled by CTAs with an atomic ticket, so big and small
+// systems share the SMs without a per-system launch. Each item runs the
+// precision form's arithmetic (hi/lo split positions, Newton-refined SFU
+// rsqrt, Kahan-compensated FP32 partials per 512-source tile folded into
+// FP64) with its own system's softening. Items that cover a whole system's
+// sources write accelerations directly; otherwise each writes a partial slot
+// and a second kernel sums a target tile's slots in chunk order, so results
+// do not depend on which CTA took which item.
+//
+// Each system's particles are padded to a multiple of the 512-source tile
+// with zero-mass entries; with every softening positive, a zero-mass source
+// and the target itself contribute exactly zero, so the kernel needs no masks.
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "batch.hpp"
+#include "common.cuh"
+
+namespace ob {
+namespace {
+
+struct BatchArgs {
+    const float4 *hi;
+    const float4 *lo;
+    const float *eps2;
+    const BatchItem *items;
+    uint32_t item_count;
+    double *ax;
+    double *ay;
+    double *az;
+    double *partial;
+    uint32_t *queue;
+    unsigned *status;
+};
+
+__device__ __forceinline__ void kahan(float &sum, float &c, float f, float d) {
+    const float y = fmaf(f, d, -c);
+    const float t = sum + y;
+    c = (t - sum) - y;
+    sum = t;
+}
+
+template <int THREADS, int R>
+__global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    constexpr uint32_t BT = THREADS * R;
+    float4 *tiles_hi = reinterpret_cast<float4 *>(smem);
+    float4 *tiles_lo = tiles_hi + 2 * kDirectTile;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 2 * kDirectTile);
+    __shared__ uint32_t s_item;
+    const uint32_t tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    constexpr uint32_t bytes = kDirectTile * sizeof(float4);
+    auto stage = [&](uint32_t tile, uint32_t buf) {
+        mbar_arrive_expect_tx(&bars[buf], 2 * bytes);
+        bulk_copy_g2s(tiles_hi + buf * kDirectTile, a.hi + static_cast<size_t>(tile) * kDirectTile,
+                      bytes, &bars[buf]);
+        bulk_copy_g2s(tiles_lo + buf * kDirectTile, a.lo + static_cast<size_t>(tile) * kDirectTile,
+                      bytes, &bars[buf]);
+    };
+
+    uint32_t sequence = 0; // tiles this CTA has consumed (pipeline phase)
+    bool ok = true;
+    while (true) {
+        if (tid == 0) {
+            s_item = atomicAdd(a.queue, 1u);
+        }
+        __syncthreads();
+        const uint32_t w = s_item;
+        __syncthreads();
+        if (w >= a.item_count) {
+            break;
+        }
+        const BatchItem item = a.items[w];
+        const float eps2 = a.eps2[item.system];
+        float hx[R], hy[R], hz[R], lx[R], ly[R], lz[R];
+        double sx[R], sy[R], sz[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const uint32_t i = item.target_begin + r * THREADS + tid;
+            const float4 p = a.hi[i];
+            const float4 q = a.lo[i];
+            hx[r] = p.x;
+            hy[r] = p.y;
+            hz[r] = p.z;
+            lx[r] = q.x;
+            ly[r] = q.y;
+            lz[r] = q.z;
+            sx[r] = sy[r] = sz[r] = 0.0;
+        }
+        const uint32_t first_tile = item.source_begin / kDirectTile;
+        const uint32_t tiles = item.source_tiles;
+        if (tid == 0) {
+            for (uint32_t k = 0; k < min(2u, tiles); ++k) {
+                stage(first_tile + k, (sequence + k) & 1u);
+            }
+        }
+        for (uint32_t k = 0; k < tiles; ++k) {
+            const uint32_t g = sequence + k;
+            const uint32_t buf = g & 1u;
+            if (ok) {
+                ok = mbar_wait_bounded(&bars[buf], (g >> 1) & 1u, a.status);
+            }
+            if (ok) {
+                const float4 *th = tiles_hi + buf * kDirectTile;
+                const float4 *tl = tiles_lo + buf * kDirectTile;
+                float kx[R], ky[R], kz[R], cx[R], cy[R], cz[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    kx[r] = ky[r] = kz[r] = cx[r] = cy[r] = cz[r] = 0.0f;
+                }
+#pragma unroll 2
+                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                    const float4 s = th[jj];
+                    const float4 l = tl[jj];
+#pragma unroll
+                    for (int r = 0; r < R; ++r) {
+                        const float dx = (s.x - hx[r]) + (l.x - lx[r]);
+                        const float dy = (s.y - hy[r]) + (l.y - ly[r]);
+                        const float dz = (s.z - hz[r]) + (l.z - lz[r]);
+                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
+                        float y = rsqrt_approx(r2);
+                        const float e = fmaf(-r2, y * y, 1.0f);
+                        y = fmaf(0.5f * y, e, y);
+                        const float f = (s.w * y) * (y * y);
+                        kahan(kx[r], cx[r], f, dx);
+                        kahan(ky[r], cy[r], f, dy);
+                        kahan(kz[r], cz[r], f, dz);
+                    }
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    sx[r] += static_cast<double>(kx[r]) - static_cast<double>(cx[r]);
+                    sy[r] += static_cast<double>(ky[r]) - static_cast<double>(cy[r]);
+                    sz[r] += static_cast<double>(kz[r]) - static_cast<double>(cz[r]);
+                }
+            }
+            __syncthreads();
+            if (tid == 0 && ok && k + 2 < tiles) {
+                fence_proxy_async_shared();
+                stage(first_tile + k + 2, buf);
+            }
+        }
+        sequence += tiles;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const uint32_t slot = r * THREADS + tid;
+            if (slot < item.target_count) {
+                if (item.slot == kDirectWrite) {
+                    const uint32_t i = item.target_begin + slot;
+                    a.ax[i] = sx[r];
+                    a.ay[i] = sy[r];
+                    a.az[i] = sz[r];
+                } else {
+                    double *p = a.partial + static_cast<size_t>(item.slot) * 3 * BT;
+                    p[slot] = sx[r];
+                    p[BT + slot] = sy[r];
+                    p[2 * BT + slot] = sz[r];
+                }
+            }
+        }
+        if (!__syncthreads_and(ok ? 1 : 0)) {
+            break;
+        }
+    }
+}
+
+__global__ void batch_reduce_kernel(const BatchGroup *__restrict__ groups, uint32_t count,
+                                    const double *__restrict__ partial, uint32_t bt, double *ax,
+                                    double *ay, double *az) {
+    for (uint32_t g = blockIdx.x; g < count; g += gridDim.x) {
+        const BatchGroup grp = groups[g];
+        for (uint32_t k = threadIdx.x; k < grp.target_count; k += blockDim.x) {
+            double x = 0.0, y = 0.0, z = 0.0;
+            for (uint32_t s = 0; s < grp.slots; ++s) {
+                const double *p = partial + static_cast<size_t>(grp.first_slot + s) * 3 * bt;
+                x += p[k];
+                y += p[bt + k];
+                z += p[2 * bt + k];
+            }
+            ax[grp.target_begin + k] = x;
+            ay[grp.target_begin + k] = y;
+            az[grp.target_begin + k] = z;
+        }
+    }
+}
+
+template <int THREADS, int R>
+cudaError_t launch_batch_t(const BatchArgs &args, int sm_count, cudaStream_t stream) {
+    const size_t smem = 4 * kDirectTile * sizeof(float4) + 2 * sizeof(uint64_t);
+    auto kernel = batch_split_kernel<THREADS, R>;
+    static const cudaError_t configured = cudaFuncSetAttribute(
+        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+    if (configured != cudaSuccess) {
+        return configured;
+    }
+    static int resident = 0;
+    if (resident == 0) {
+        const cudaError_t err =
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kernel, THREADS, smem);
+        if (err != cudaSuccess || resident < 1) {
+            resident = 1;
+        }
+    }
+    const uint32_t blocks = static_cast<uint32_t>(std::max(1, sm_count) * resident);
+    kernel<<<blocks, THREADS, smem, stream>>>(args);
+    return cudaGetLastError();
+}
+
+} // namespace
+
+cudaError_t launch_batch_forces(const float4 *hi, const float4 *lo, const float *eps2,
+                                const BatchItem *items, uint32_t item_count,
+                                const BatchConfig &config, double *ax, double *ay, double *az,
+                                double *partial, uint32_t *queue, unsigned *status,
+                                int sm_count, cudaStream_t stream) {
+    if (item_count == 0) {
+        return cudaSuccess;
+    }
+    const BatchArgs args{hi, lo, eps2, items, item_count, ax, ay, az, partial, queue, status};
+#define OB_BATCH_CASE(T, RR)                                                                       \
+    if (config.threads == T && config.targets_per_thread == RR)                                    \
+        return launch_batch_t<T, RR>(args, sm_count, stream);
+    OB_BATCH_CASE(128, 1)
+    OB_BATCH_CASE(128, 2)
+    OB_BATCH_CASE(128, 4)
+    OB_BATCH_CASE(256, 1)
+    OB_BATCH_CASE(256, 2)
+#undef OB_BATCH_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_batch_reduce(const BatchGroup *groups, uint32_t group_count,
+                                const double *partial, uint32_t bt, double *ax, double *ay,
+                                double *az, cudaStream_t stream) {
+    if (group_count == 0) {
+        return cudaSuccess;
+    }
+    const uint32_t blocks = std::min(group_count, 148u * 8u);
+    batch_reduce_kernel<<<blocks, 128, 0, stream>>>(groups, group_count, partial, bt, ax, ay, az);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Batch
+// ---------------------------------------------------------------------------
+
+Batch::Batch(uint32_t systems, const uint64_t *counts, const double *softening_squared) {
+    if (systems == 0) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "a batch needs at least one system");
+    }
+    uint64_t total = 0;
+    count_.resize(systems);
+    offset_.resize(systems);
+    eps2_host_.resize(systems);
+    for (uint32_t s = 0; s < systems; ++s) {
+        if (counts[s] == 0 || counts[s] > 0xffffffffull) {
+            throw Error(OB_ERROR_INVALID_ARGUMENT, "every system needs 1 .. 2^32-1 particles");
+        }
+        if (!(softening_squared[s] > 0.0) || !std::isfinite(softening_squared[s])) {
+            throw Error(OB_ERROR_INVALID_ARGUMENT,
+                        "batched systems need a positive, finite softening");
+        }
+        count_[s] = static_cast<uint32_t>(counts[s]);
+        offset_[s] = static_cast<uint32_t>(total);
+        eps2_host_[s] = softening_squared[s];
+        total += static_cast<uint64_t>(ceil_div(counts[s], kDirectTile)) * kDirectTile;
+        pairs_ += counts[s] * (counts[s] - 1);
+    }
+    // Slack past the last system for target tiles that run over (<= 1024).
+    total += 1024;
+    if (total > 0x7fffffffull) {
+        throw Error(OB_ERROR_CAPACITY, "a batch holds at most 2^31 padded particles");
+    }
+    total_ = static_cast<uint32_t>(total);
+    int device = 0;
+    check(cudaGetDevice(&device), "cudaGetDevice");
+    check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "SMs");
+    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a stream");
+    state_.reserve(10ull * total_);
+    check(cudaMemset(state_.data(), 0, state_.bytes()), "clearing state");
+    hi_.reserve(total_);
+    lo_.reserve(total_);
+    std::vector<float> eps2f(systems);
+    for (uint32_t s = 0; s < systems; ++s) {
+        eps2f[s] = static_cast<float>(eps2_host_[s]);
+    }
+    eps2_.reserve(systems);
+    check(cudaMemcpy(eps2_.data(), eps2f.data(), sizeof(float) * systems, cudaMemcpyHostToDevice),
+          "uploading softenings");
+    queue_.reserve(1);
+    status_.reserve(1);
+    check(cudaMemset(status_.data(), 0, sizeof(unsigned)), "clearing status");
+    build_items(config_);
+}
+
+Batch::~Batch() {
+    drop_graph();
+    if (stream_ != nullptr) {
+        cudaStreamDestroy(stream_);
+    }
+}
+
+void Batch::drop_graph() {
+    if (graph_ != nullptr) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+    }
+}
+
+void Batch::build_items(const BatchConfig &config) {
+    const uint32_t bt = static_cast<uint32_t>(config.threads * config.targets_per_thread);
+    std::vector<BatchItem> items;
+    std::vector<BatchGroup> groups;
+    uint32_t slots = 0;
+    for (uint32_t s = 0; s < count_.size(); ++s) {
+        const uint32_t tiles = ceil_div(count_[s], kDirectTile);
+        const uint32_t chunk = config.chunk_tiles == 0 ? tiles : std::min(config.chunk_tiles, tiles);
+        const uint32_t chunks = ceil_div(tiles, chunk);
+        for (uint32_t t = 0; t < count_[s]; t += bt) {
+            const uint32_t n_targets = std::min(bt, count_[s] - t);
+            if (chunks > 1) {
+                groups.push_back(BatchGroup{offset_[s] + t, n_targets, slots, chunks});
+            }
+            for (uint32_t c = 0; c < chunks; ++c) {
+                const uint32_t first = c * chunk;
+                items.push_back(BatchItem{s, offset_[s] + t, n_targets,
+                                          offset_[s] + first * kDirectTile,
+                                          std::min(chunk, tiles - first),
+                                          chunks > 1 ? slots + c : kDirectWrite});
+            }
+            if (chunks > 1) {
+                slots += chunks;
+            }
+        }
+    }
+    // Largest first, ties in creation order: the queue then balances itself.
+    std::stable_sort(items.begin(), items.end(), [](const BatchItem &l, const BatchItem &r) {
+        return static_cast<uint64_t>(l.target_count) * l.source_tiles >
+               static_cast<uint64_t>(r.target_count) * r.source_tiles;
+    });
+    items_.reserve(std::max<size_t>(1, items.size()));
+    check(cudaMemcpy(items_.data(), items.data(), sizeof(BatchItem) * items.size(),
+                     cudaMemcpyHostToDevice),
+          "uploading work items");
+    groups_.reserve(std::max<size_t>(1, groups.size()));
+    if (!groups.empty()) {
+        check(cudaMemcpy(groups_.data(), groups.data(), sizeof(BatchGroup) * groups.size(),
+                         cudaMemcpyHostToDevice),
+              "uploading reduction groups");
+    }
+    partial_.reserve(std::max<size_t>(1, static_cast<size_t>(slots) * 3 * bt));
+    item_count_ = static_cast<uint32_t>(items.size());
+    group_count_ = static_cast<uint32_t>(groups.size());
+    slots_ = slots;
+    config_ = config;
+    drop_graph();
+}
+
+void Batch::set_config(const BatchConfig &config) { build_items(config); }
+
+void Batch::set_state(uint32_t system, const double *x, const double *y, const double *z,
+                      const double *vx, const double *vy, const double *vz, const double *m) {
+    if (system >= count_.size()) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "no such system in the batch");
+    }
+    if (!x || !y || !z || !m) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "positions and masses are required");
+    }
+    const double *in[7] = {x, y, z, vx, vy, vz, m};
+    const int arrays[7] = {kX, kY, kZ, kVx, kVy, kVz, kM};
+    const size_t bytes = sizeof(double) * count_[system];
+    for (int k = 0; k < 7; ++k) {
+        double *dst = array(arrays[k]) + offset_[system];
+        if (in[k] == nullptr) {
+            check(cudaMemsetAsync(dst, 0, bytes, stream_), "clearing");
+        } else {
+            check(cudaMemcpyAsync(dst, in[k], bytes, cudaMemcpyHostToDevice, stream_), "upload");
+        }
+    }
+    check(cudaStreamSynchronize(stream_), "uploading a system");
+}
+
+void Batch::get_state(uint32_t system, double *const *out) {
+    if (system >= count_.size()) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "no such system in the batch");
+    }
+    for (int k = 0; k < 9; ++k) {
+        if (out[k] != nullptr) {
+            check(cudaMemcpyAsync(out[k], array(k) + offset_[system],
+                                  sizeof(double) * count_[system], cudaMemcpyDeviceToHost,
+                                  stream_),
+                  "download");
+        }
+    }
+    check(cudaStreamSynchronize(stream_), "downloading a system");
+}
+
+void Batch::evaluate() {
+    check(pack_sources(array(kX), array(kY), array(kZ), array(kM), total_, total_, hi_.data(),
+                       lo_.data(), stream_),
+          "packing sources");
+    check(cudaMemsetAsync(queue_.data(), 0, sizeof(uint32_t), stream_), "resetting the queue");
+    check(launch_batch_forces(hi_.data(), lo_.data(), eps2_.data(), items_.data(), item_count_,
+                              config_, array(kAx), array(kAy), array(kAz), partial_.data(),
+                              queue_.data(), status_.data(), sm_count_, stream_),
+          "batched forces");
+    check(launch_batch_reduce(groups_.data(), group_count_, partial_.data(),
+                              static_cast<uint32_t>(config_.threads * config_.targets_per_thread),
+                              array(kAx), array(kAy), array(kAz), stream_),
+          "reducing partial sums");
+}
+
+void Batch::refresh() {
+    evaluate();
+    ++evaluations_;
+    synchronize();
+}
+
+static void yoshida(double &outer, double &inner) {
+    constexpr double cube_root_of_two = 1.2599210498948731647672106;
+    outer = 1.0 / (2.0 - cube_root_of_two);
+    inner = -cube_root_of_two / (2.0 - cube_root_of_two);
+}
+
+void Batch::enqueue_step(int integrator, double dt) {
+    auto substep = [&](double h) {
+        const double half = h / 2.0;
+        check(launch_kick_drift(array(kX), array(kY), array(kZ), array(kVx), array(kVy),
+                                array(kVz), array(kAx), array(kAy), array(kAz), total_, half, h,
+                                stream_),
+              "kick and drift");
+        evaluate();
+        check(launch_kick(array(kVx), array(kVy), array(kVz), array(kAx), array(kAy), array(kAz),
+                          total_, half, stream_),
+              "kick");
+    };
+    if (integrator == OB_INTEGRATOR_YOSHIDA4) {
+        double outer = 0.0, inner = 0.0;
+        yoshida(outer, inner);
+        substep(outer * dt);
+        substep(inner * dt);
+        substep(outer * dt);
+    } else {
+        substep(dt);
+    }
+}
+
+void Batch::step_async(int integrator, double dt, uint64_t steps) {
+    if (integrator != OB_INTEGRATOR_VV && integrator != OB_INTEGRATOR_YOSHIDA4) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "unknown integrator");
+    }
+    if (graph_ == nullptr || graph_integrator_ != integrator || graph_dt_ != dt) {
+        drop_graph();
+        cudaGraph_t graph = nullptr;
+        check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed), "begin capture");
+        try {
+            enqueue_step(integrator, dt);
+        } catch (...) {
+            cudaStreamEndCapture(stream_, &graph);
+            if (graph != nullptr) {
+                cudaGraphDestroy(graph);
+            }
+            throw;
+        }
+        check(cudaStreamEndCapture(stream_, &graph), "end capture");
+        const cudaError_t err = cudaGraphInstantiate(&graph_, graph, 0);
+        cudaGraphDestroy(graph);
+        check(err, "instantiating the batch step graph");
+        graph_integrator_ = integrator;
+        graph_dt_ = dt;
+    }
+    for (uint64_t s = 0; s < steps; ++s) {
+        check(cudaGraphLaunch(graph_, stream_), "launching the batch step");
+    }
+    evaluations_ += steps * (integrator == OB_INTEGRATOR_YOSHIDA4 ? 3 : 1);
+}
+
+void Batch::synchronize() {
+    check(cudaStreamSynchronize(stream_), "batched integration");
+    const unsigned status = read_and_clear_status(status_.data(), stream_);
+    if (status & kStatusTimeout) {
+        throw Error(OB_ERROR_TIMEOUT, "a device-side wait ran out of its bound");
+    }
+}
+
+static double neumaier(const std::vector<double> &terms) {
+    double total = 0.0, correction = 0.0;
+    for (const double term : terms) {
+        const double updated = total + term;
+        if (std::fabs(total) >= std::fabs(term)) {
+            correction += (total - updated) + term;
+        } else {
+            correction += (term - updated) + total;
+        }
+        total = updated;
+    }
+    return total + correction;
+}
+
+void Batch::energy(uint32_t system, double *kinetic, double *potential) {
+    if (system >= count_.size()) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "no such system in the batch");
+    }
+    const uint32_t n = count_[system];
+    const uint32_t o = offset_[system];
+    terms_.reserve(n);
+    std::vector<double> host(n);
+    if (kinetic != nullptr) {
+        check(launch_kinetic_partials(array(kVx) + o, array(kVy) + o, array(kVz) + o,
+                                      array(kM) + o, n, terms_.data(), stream_),
+              "kinetic terms");
+        check(cudaMemcpyAsync(host.data(), terms_.data(), sizeof(double) * n,
+                              cudaMemcpyDeviceToHost, stream_),
+              "download");
+        check(cudaStreamSynchronize(stream_), "kinetic energy");
+        *kinetic = neumaier(host) / 2.0;
+    }
+    if (potential != nullptr) {
+        check(launch_potential_rows(array(kX) + o, array(kY) + o, array(kZ) + o, array(kM) + o, n,
+                                    eps2_host_[system], terms_.data(), stream_),
+              "potential rows");
+        check(cudaMemcpyAsync(host.data(), terms_.data(), sizeof(double) * n,
+                              cudaMemcpyDeviceToHost, stream_),
+              "download");
+        check(cudaStreamSynchronize(stream_), "potential energy");
+        *potential = neumaier(host);
+    }
+}
+
+double Batch::autotune(BatchConfig &chosen) {
+    static const int shapes[][2] = {{128, 1}, {128, 2}, {128, 4}, {256, 1}, {256, 2}};
+    static const uint32_t chunks[] = {0, 16, 8, 4};
+    cudaEvent_t start, stop;
+    check(cudaEventCreate(&start), "event");
+    check(cudaEventCreate(&stop), "event");
+    const BatchConfig saved = config_;
+    double best = 1e300;
+    BatchConfig best_config = saved;
+    for (const auto &shape : shapes) {
+        for (const uint32_t chunk : chunks) {
+            const BatchConfig c{shape[0], shape[1], chunk};
+            build_items(c);
+            evaluate();
+            check(cudaEventRecord(start, stream_), "event");
+            evaluate();
+            evaluate();
+            check(cudaEventRecord(stop, stream_), "event");
+            check(cudaEventSynchronize(stop), "autotune timing");
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, start, stop), "autotune timing");
+            if (ms / 2.0 < best) {
+                best = ms / 2.0;
+                best_config = c;
+            }
+        }
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(stop);
+    build_items(best_config);
+    // The timing runs overwrote the carried accelerations: recompute them.
+    evaluate();
+    synchronize();
+    chosen = best_config;
+    return best;
+}
+
+} // namespace ob

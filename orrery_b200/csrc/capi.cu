@@ -10,6 +10,7 @@
 #include "common.cuh"
 #include "orrery_b200.h"
 #include "solver.hpp"
+#include "batch.hpp"
 #include "system.hpp"
 #include "tree.hpp"
 
@@ -390,6 +391,10 @@ struct ob_system {
     std::unique_ptr<ob::System> impl;
 };
 
+struct ob_batch {
+    std::unique_ptr<ob::Batch> impl;
+};
+
 using ob::guarded;
 using ob::require;
 
@@ -675,6 +680,123 @@ int ob_system_size(const ob_system *system, uint64_t *n) {
     return guarded([&] {
         require(system != nullptr && n != nullptr, "NULL argument");
         *n = system->impl->size();
+    });
+}
+
+int ob_batch_create(uint32_t systems, const uint64_t *counts, const double *softening_squared,
+                    ob_batch **out) {
+    return guarded([&] {
+        require(out != nullptr && counts != nullptr && softening_squared != nullptr,
+                "NULL argument");
+        *out = nullptr;
+        require(systems > 0, "a batch needs at least one system");
+        ob::require_device();
+        auto b = std::make_unique<ob_batch>();
+        b->impl = std::make_unique<ob::Batch>(systems, counts, softening_squared);
+        *out = b.release();
+    });
+}
+
+void ob_batch_destroy(ob_batch *batch) { delete batch; }
+
+int ob_batch_set_state(ob_batch *batch, uint32_t system, const double *x, const double *y,
+                       const double *z, const double *vx, const double *vy, const double *vz,
+                       const double *m) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        batch->impl->set_state(system, x, y, z, vx, vy, vz, m);
+    });
+}
+
+int ob_batch_get_state(ob_batch *batch, uint32_t system, double *x, double *y, double *z,
+                       double *vx, double *vy, double *vz, double *ax, double *ay, double *az) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        double *out[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+        batch->impl->get_state(system, out);
+    });
+}
+
+int ob_batch_refresh(ob_batch *batch) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        batch->impl->refresh();
+    });
+}
+
+int ob_batch_step(ob_batch *batch, int32_t integrator, double dt, uint64_t steps) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        require(std::isfinite(dt), "the timestep must be finite");
+        batch->impl->step_async(integrator, dt, steps);
+        batch->impl->synchronize();
+    });
+}
+
+int ob_batch_step_async(ob_batch *batch, int32_t integrator, double dt, uint64_t steps) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        require(std::isfinite(dt), "the timestep must be finite");
+        batch->impl->step_async(integrator, dt, steps);
+    });
+}
+
+int ob_batch_synchronize(ob_batch *batch) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        batch->impl->synchronize();
+    });
+}
+
+int ob_batch_energy(ob_batch *batch, uint32_t system, double *kinetic, double *potential) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        batch->impl->energy(system, kinetic, potential);
+    });
+}
+
+int ob_batch_autotune(ob_batch *batch, ob_batch_shape *chosen, double *best_ms) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        ob::BatchConfig c;
+        const double ms = batch->impl->autotune(c);
+        if (chosen != nullptr) {
+            *chosen = ob_batch_shape{c.threads, c.targets_per_thread, c.chunk_tiles, 0};
+        }
+        if (best_ms != nullptr) {
+            *best_ms = ms;
+        }
+    });
+}
+
+int ob_batch_set_shape(ob_batch *batch, const ob_batch_shape *shape) {
+    return guarded([&] {
+        require(batch != nullptr && shape != nullptr, "NULL argument");
+        const bool known = (shape->threads == 128 &&
+                            (shape->targets_per_thread == 1 || shape->targets_per_thread == 2 ||
+                             shape->targets_per_thread == 4)) ||
+                           (shape->threads == 256 &&
+                            (shape->targets_per_thread == 1 || shape->targets_per_thread == 2));
+        require(known, "the library implements no such batch kernel shape");
+        batch->impl->set_config(
+            ob::BatchConfig{shape->threads, shape->targets_per_thread, shape->chunk_tiles});
+    });
+}
+
+int ob_batch_stats(ob_batch *batch, uint64_t *pairs_per_evaluation, uint64_t *evaluations,
+                   uint32_t *items) {
+    return guarded([&] {
+        require(batch != nullptr, "batch is NULL");
+        if (pairs_per_evaluation != nullptr) *pairs_per_evaluation = batch->impl->pair_interactions();
+        if (evaluations != nullptr) *evaluations = batch->impl->evaluations();
+        if (items != nullptr) *items = batch->impl->items();
+    });
+}
+
+int ob_batch_stream(ob_batch *batch, void **stream) {
+    return guarded([&] {
+        require(batch != nullptr && stream != nullptr, "NULL argument");
+        *stream = batch->impl->stream();
     });
 }
 
