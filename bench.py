@@ -14,6 +14,10 @@ Workloads (seeded synthetic inputs with the shapes of the measured configs):
                            dt 1e-3. Metric: direct Gint/s, N(N-1) per step.
   direct-plummer-262144-fp32  Plummer N=262,144, FP32 direct, VV dt 1e-3: the
                            plain kernel at a size that fills the GPU.
+  batched-512              512 independent Plummer clusters, N log-uniform in
+                           [256, 16384], scale radius U[0.5, 2], eps = 0.01 x
+                           radius, split precision, all systems in one
+                           persistent launch, Yoshida-4 dt 1e-3 as one graph.
   direct-plummer-262144    the same at N=262,144 with the split-precision
                            kernel and Yoshida-4 dt 1e-3 (3 evaluations/step).
 
@@ -67,6 +71,9 @@ WORKLOADS = {
                                        integrator="vv", precision="fp32",
                                        metric="direct Gint/s", unit="Gint/s", higher=True,
                                        generator="plummer"),
+    "batched-512": dict(kind="batch", n=512, eps=0.01, dt=1e-3, integrator="yoshida4",
+                        precision="split", metric="batched Gint/s", unit="Gint/s", higher=True,
+                        generator="clusters"),
     "direct-plummer-262144": dict(kind="direct", n=262_144, eps=0.01, dt=1e-3,
                                   integrator="yoshida4", precision="split",
                                   metric="direct Gint/s", unit="Gint/s", higher=True,
@@ -75,9 +82,23 @@ WORKLOADS = {
 DEFAULT_WORKLOAD = "bh-collision-2m"
 
 
+def make_clusters(count, seed=20260813):
+    """512-cluster batch: sizes log-uniform in [256, 16384], radii U[0.5, 2]."""
+    from orrery_b200 import initial_conditions as ic
+
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(256), np.log(16384), count)).astype(np.int64)
+    radii = rng.uniform(0.5, 2.0, count)
+    systems = [ic.plummer_sphere(int(n), scale_radius=float(a), seed=seed + 1 + k)
+               for k, (n, a) in enumerate(zip(sizes, radii))]
+    return sizes, radii, systems
+
+
 def make_inputs(w, seed=20260811):
     from orrery_b200 import initial_conditions as ic
 
+    if w["generator"] == "clusters":
+        return make_clusters(w["n"])
     if w["generator"] == "plummer":
         return ic.plummer_sphere(w["n"], seed=seed)
     return ic.galaxy_collision(w["n"], softening=w["eps"], seed=seed)
@@ -235,6 +256,29 @@ def cpu_baseline(w, data, budget_s=20.0):
                        f"full {len(m)}-particle input = one VV step's force evaluation")
 
 
+def cpu_baseline_batch(w, sizes, radii, systems, budget_s=15.0):
+    """The reference's DirectSolver (AVX2, all host threads, one solver per
+    system with its own softening) on the clusters in order until the budget
+    is spent; the rate over the systems done stands for the batch."""
+    import oracle
+
+    ref = oracle.Reference()
+    threads = ref.worker_count()
+    done_pairs, spent, count = 0, 0.0, 0
+    for k, d in enumerate(systems):
+        sec = ref.direct_seconds(d["x"], d["y"], d["z"], d["m"], w["eps"] * radii[k], threads,
+                                 repeats=1)
+        n = int(sizes[k])
+        done_pairs += n * (n - 1)
+        spent += sec
+        count += 1
+        if spent > budget_s:
+            break
+    return dict(value=done_pairs / spent / 1e9, unit="Gint/s", cores=threads, kind="reference",
+                sample=f"one DirectSolver evaluation (AVX2, {threads} threads) of each of the "
+                       f"first {count} of {len(systems)} clusters")
+
+
 def run_reference(args, w):
     world, rank, local = dist_env()
     dist = init_dist(world, "gloo")
@@ -243,10 +287,17 @@ def run_reference(args, w):
         return
     data = make_inputs(w)
     steps = max(1, args.steps)
-    base = cpu_baseline(w, data, budget_s=min(60.0, 10.0 * steps))
+    if w["kind"] == "batch":
+        base = cpu_baseline_batch(w, *data, budget_s=min(60.0, 10.0 * steps))
+    else:
+        base = cpu_baseline(w, data, budget_s=min(60.0, 10.0 * steps))
     value = base["value"]
-    ms_per_step = value if w["unit"] == "ms/step" else \
-        step_units(w) / (value * 1e9) * 1e3
+    if w["kind"] == "batch":
+        pairs = sum(int(n) * (int(n) - 1) for n in data[0])
+        ms_per_step = pairs * evaluations_per_step(w) / (value * 1e9) * 1e3
+    else:
+        ms_per_step = value if w["unit"] == "ms/step" else \
+            step_units(w) / (value * 1e9) * 1e3
     line = {
         "impl": "reference", "metric": w["metric"], "value": value, "unit": w["unit"],
         "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
@@ -261,6 +312,9 @@ def run_reference(args, w):
 
 
 def config_of(args, w):
+    if w["kind"] == "batch":
+        return {"workload": args.workload, "systems": w["n"], "precision": w["precision"],
+                "integrator": w["integrator"], "dt": w["dt"], "replicas": args.gpus}
     c = {"workload": args.workload, "n": w["n"], "solver": w["kind"],
          "precision": w["precision"], "softening": w["eps"], "dt": w["dt"],
          "integrator": w["integrator"], "replicas": args.gpus,
@@ -323,6 +377,96 @@ def e2e_drop_in(ob, w, data, steps, torch):
     sec = (time.perf_counter() - t0) / steps
     evals = len(weights)
     return sec, evals * 4 * 8 * n, evals * 3 * 8 * n, solver
+
+
+def run_batch(args, w):
+    """The batched form: every cluster stepped by one replayed graph."""
+    import torch
+
+    import orrery_b200 as ob
+
+    world, rank, local = dist_env()
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    sizes, radii, systems = make_inputs(w)
+    batch = ob.DeviceBatch(sizes, w["eps"] * radii)
+    for k, d in enumerate(systems):
+        batch.set_state(k, d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+    batch.refresh()
+    shape, tuned_ms = batch.autotune()
+    batch.step(w["dt"], max(args.warmup, 3), w["integrator"])
+    pairs, _, items = batch.stats()
+    evals = evaluations_per_step(w)
+    stream = torch.cuda.ExternalStream(batch.stream(), device=device)
+    K = args.steps
+    sampler = ClockSampler(local)
+    barrier(dist)
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    batch.step_async(w["dt"], K, w["integrator"])
+    end.record(stream)
+    end.synchronize()
+    total_ms = start.elapsed_time(end)
+    batch.synchronize()
+    barrier(dist)
+    clocks = sampler.stop()
+    total_ms = reduce_max(dist, total_ms, device)
+    value = pairs * evals * K * world / (total_ms * 1e-3) / 1e9
+    if rank == 0:
+        ffma, rsq = ob.probe_fp32()
+        peak = min(ffma / 12.0, rsq) / 1e9
+        achieved = pairs * evals / (tuned_ms * 1e-3 * evals) / 1e9
+        # e2e through the public API with host buffers: each step uploads every
+        # system's state from pinned memory and downloads it again.
+        pinned = [{k: torch.from_numpy(np.ascontiguousarray(d[k])).pin_memory().numpy()
+                   for k in ("x", "y", "z", "vx", "vy", "vz", "m")} for d in systems]
+        e2e_steps = max(2, min(K, 5))
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            for k, d in enumerate(pinned):
+                batch.set_state(k, d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+            batch.step(w["dt"], 1, w["integrator"])
+            for k in range(len(pinned)):
+                batch.state(k)
+        sec = (time.perf_counter() - t0) / e2e_steps
+        total_n = int(sizes.sum())
+        line = {
+            "metric": w["metric"], "value": value, "unit": w["unit"], "n_gpus": world,
+            "steps": K, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / K,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "state_dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "systems": len(sizes),
+                       "particles": total_n, "pairs_per_evaluation": pairs,
+                       "precision": "split", "integrator": "yoshida4", "dt": w["dt"],
+                       "softening": "0.01 x scale radius", "work_items": items,
+                       "autotuned_shape": {"threads": shape[0], "targets_per_thread": shape[1],
+                                           "chunk_tiles": shape[2]},
+                       "l2": "inputs larger than L2"},
+            "roofline": {"bound": "fp32-fma-pipe", "achieved": achieved, "peak": peak,
+                         "unit": "Gint/s", "frac": achieved / peak, "traffic": None,
+                         "kernel_ms": tuned_ms,
+                         "note": "peak counts 12 FP32 operations per interaction (the plain "
+                                 "kernel); the split arithmetic issues about 30"},
+            "e2e": {"value": pairs * evals / sec / 1e9, "unit": w["unit"],
+                    "h2d_bytes_per_step": total_n * 7 * 8, "d2h_bytes_per_step": total_n * 9 * 8,
+                    "path": "ob_batch_set_state for every system, one step, ob_batch_get_state"},
+            # Per substep: kick-drift, pack, batched forces, (partial-sum
+            # reduction when sources are chunked), kick.
+            "gpu_launches": K * evals * (5 if shape[2] else 4),
+            "clocks": clocks,
+        }
+        if world == 1:
+            line["cpu_baseline"] = cpu_baseline_batch(w, sizes, radii, systems)
+        print(json.dumps(line), flush=True)
+    barrier(dist)
+    del batch
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def run_b200(args, w):
@@ -486,6 +630,8 @@ def main():
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w)
+    elif w["kind"] == "batch":
+        run_batch(args, w)
     else:
         run_b200(args, w)
 
