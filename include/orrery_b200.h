@@ -282,6 +282,87 @@ int ob_batch_stats(ob_batch *batch, uint64_t *pairs_per_evaluation, uint64_t *ev
                    uint32_t *items);
 int ob_batch_stream(ob_batch *batch, void **stream);
 
+/* ------------------------------------------------------------------------ */
+/* Server: a persistent request loop with continuous batching                */
+/* ------------------------------------------------------------------------ */
+/* Replaces the reference service's one-CLI-process-per-job worker
+ * (service/orrery_service/worker.py:262-300) and its concurrency and work
+ * limits (service/orrery_service/limits.py:38-167) for the force path: jobs
+ * are admitted from per-solver FIFO queues while their device memory fits the
+ * HBM budget and the direct work per step stays under a cap; each job's state
+ * stays on the device; all direct jobs with the same integrator and timestep
+ * step together in one batched launch (members join and leave between
+ * steps); each tree job steps on its own stream, overlapping the batch. */
+typedef struct ob_server ob_server;
+
+typedef struct ob_server_config {
+    uint64_t hbm_budget_bytes;       /* device memory the jobs may hold */
+    uint64_t direct_pairs_cap;       /* max sum N(N-1) of running direct jobs (0: none) */
+    uint64_t direct_arena_particles; /* padded particles per direct batch arena */
+    uint32_t max_tree_jobs;          /* tree jobs running at once */
+    int32_t fake_device;             /* nonzero: no GPU; steps take modelled time */
+    double fake_direct_gint_s;       /* fake mode: direct interactions per second / 1e9 */
+    double fake_tree_ns_per_particle;/* fake mode: tree step time per particle */
+} ob_server_config;
+
+typedef struct ob_job_spec {
+    int32_t kind;              /* OB_SOLVER_DIRECT (precision form) or OB_SOLVER_TREE */
+    int32_t integrator;        /* OB_INTEGRATOR_* */
+    uint64_t n;
+    uint64_t steps;
+    double dt;
+    double softening_squared;
+    double opening_angle;      /* tree jobs */
+    uint64_t leaf_capacity;    /* tree jobs */
+    int32_t quadrupole;        /* tree jobs */
+    int32_t reserved;
+} ob_job_spec;
+
+#define OB_JOB_QUEUED 0
+#define OB_JOB_RUNNING 1
+#define OB_JOB_DONE 2
+#define OB_JOB_FAILED 3
+#define OB_JOB_CANCELLED 4
+#define OB_JOB_REJECTED 5
+
+typedef struct ob_job_report {
+    uint64_t id;
+    int32_t status;            /* OB_JOB_* */
+    int32_t reserved;
+    uint64_t steps_done;
+    double submitted_s;        /* seconds since the server started */
+    double admitted_s;
+    double finished_s;
+} ob_job_report;
+
+typedef struct ob_server_summary {
+    uint64_t submitted, admitted, completed, failed, cancelled, rejected;
+    uint64_t queued, running;
+    double elapsed_s;
+    double jobs_per_s;                 /* completed / elapsed */
+    double job_latency_p50_s, job_latency_p99_s;   /* finish - submit, completed jobs */
+    double step_latency_p50_ms, step_latency_p99_ms; /* per advanced step, all jobs */
+    uint64_t hbm_in_use, hbm_peak;
+} ob_server_summary;
+
+int ob_server_create(const ob_server_config *config, ob_server **out);
+/* Stops the loop (running jobs are cancelled) and frees everything. */
+void ob_server_destroy(ob_server *server);
+/* Copies the initial state (vx..vz may be NULL = zero); returns the job id. A
+ * job that can never fit the budget is rejected (OB_ERROR_CAPACITY). */
+int ob_server_submit(ob_server *server, const ob_job_spec *spec, const double *x,
+                     const double *y, const double *z, const double *vx, const double *vy,
+                     const double *vz, const double *m, uint64_t *job_id);
+/* Waits up to timeout_s for the job to end (OB_ERROR_TIMEOUT otherwise), then
+ * fills the report and any non-NULL output arrays (n each). */
+int ob_server_wait(ob_server *server, uint64_t job_id, double timeout_s, ob_job_report *report,
+                   double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                   double *ax, double *ay, double *az);
+int ob_server_cancel(ob_server *server, uint64_t job_id);
+int ob_server_stats(ob_server *server, ob_server_summary *stats);
+/* Waits until no job is queued or running (OB_ERROR_TIMEOUT otherwise). */
+int ob_server_drain(ob_server *server, double timeout_s);
+
 /* Measured FP32 FFMA and SFU rsqrt lane operations per second on the current
  * device: the denominators of the direct kernel's roofline. No reference
  * counterpart in the library (the reference's probes are benchmark code,

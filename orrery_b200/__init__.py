@@ -76,6 +76,36 @@ class BatchShape(C.Structure):
                 ("chunk_tiles", C.c_uint32), ("reserved", C.c_int32)]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_uint64), ("direct_pairs_cap", C.c_uint64),
+                ("direct_arena_particles", C.c_uint64), ("max_tree_jobs", C.c_uint32),
+                ("fake_device", C.c_int32), ("fake_direct_gint_s", C.c_double),
+                ("fake_tree_ns_per_particle", C.c_double)]
+
+
+class JobSpec(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("integrator", C.c_int32), ("n", C.c_uint64),
+                ("steps", C.c_uint64), ("dt", C.c_double), ("softening_squared", C.c_double),
+                ("opening_angle", C.c_double), ("leaf_capacity", C.c_uint64),
+                ("quadrupole", C.c_int32), ("reserved", C.c_int32)]
+
+
+class JobReport(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("status", C.c_int32), ("reserved", C.c_int32),
+                ("steps_done", C.c_uint64), ("submitted_s", C.c_double),
+                ("admitted_s", C.c_double), ("finished_s", C.c_double)]
+
+
+class ServerSummary(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("admitted", C.c_uint64), ("completed", C.c_uint64),
+                ("failed", C.c_uint64), ("cancelled", C.c_uint64), ("rejected", C.c_uint64),
+                ("queued", C.c_uint64), ("running", C.c_uint64), ("elapsed_s", C.c_double),
+                ("jobs_per_s", C.c_double), ("job_latency_p50_s", C.c_double),
+                ("job_latency_p99_s", C.c_double), ("step_latency_p50_ms", C.c_double),
+                ("step_latency_p99_ms", C.c_double), ("hbm_in_use", C.c_uint64),
+                ("hbm_peak", C.c_uint64)]
+
+
 class Timings(C.Structure):
     _fields_ = [("transfer_in_ms", C.c_double), ("ordering_ms", C.c_double),
                 ("construction_ms", C.c_double), ("traversal_ms", C.c_double),
@@ -164,6 +194,15 @@ def load_library():
     lib.ob_batch_stats.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64),
                                    C.POINTER(C.c_uint32)]
     lib.ob_batch_stream.argtypes = [vp, C.POINTER(vp)]
+    lib.ob_server_create.argtypes = [C.POINTER(ServerConfig), C.POINTER(vp)]
+    lib.ob_server_destroy.argtypes = [vp]
+    lib.ob_server_destroy.restype = None
+    lib.ob_server_submit.argtypes = [vp, C.POINTER(JobSpec)] + [_dp] * 7 + [
+        C.POINTER(C.c_uint64)]
+    lib.ob_server_wait.argtypes = [vp, C.c_uint64, C.c_double, C.POINTER(JobReport)] + [_dp] * 9
+    lib.ob_server_cancel.argtypes = [vp, C.c_uint64]
+    lib.ob_server_stats.argtypes = [vp, C.POINTER(ServerSummary)]
+    lib.ob_server_drain.argtypes = [vp, C.c_double]
     _lib = lib
     return lib
 
@@ -574,6 +613,79 @@ class DeviceBatch:
         s = C.c_void_p()
         _check(self._lib.ob_batch_stream(self._handle, C.byref(s)))
         return s.value or 0
+
+
+JOB_QUEUED, JOB_RUNNING, JOB_DONE, JOB_FAILED, JOB_CANCELLED, JOB_REJECTED = range(6)
+
+
+class Server:
+    """The persistent serving loop (continuous batching, HBM-budget admission).
+
+    ``fake=True`` runs the same scheduler with no GPU: each step takes the time
+    a cost model gives (direct: pairs / fake_direct_gint_s; tree: N x
+    fake_tree_ns_per_particle)."""
+
+    def __init__(self, hbm_budget_bytes: int, direct_pairs_cap: int = 0,
+                 direct_arena_particles: int = 0, max_tree_jobs: int = 1, fake: bool = False,
+                 fake_direct_gint_s: float = 800.0, fake_tree_ns_per_particle: float = 12.0):
+        lib = load_library()
+        cfg = ServerConfig(int(hbm_budget_bytes), int(direct_pairs_cap),
+                           int(direct_arena_particles), int(max_tree_jobs), 1 if fake else 0,
+                           float(fake_direct_gint_s), float(fake_tree_ns_per_particle))
+        handle = C.c_void_p()
+        _check(lib.ob_server_create(C.byref(cfg), C.byref(handle)))
+        self._lib = lib
+        self._handle = handle
+        self._sizes = {}
+
+    def close(self) -> None:
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            self._lib.ob_server_destroy(h)
+            self._handle = None
+
+    def __del__(self):
+        self.close()
+
+    def submit(self, state: dict, steps: int, dt: float, softening: float, kind: str = "direct",
+               integrator: str = "yoshida4", opening_angle: float = 0.5,
+               leaf_capacity: int = 32, quadrupole: bool = True) -> int:
+        n = len(state["m"])
+        spec = JobSpec(SOLVER_DIRECT if kind == "direct" else SOLVER_TREE,
+                       _INTEGRATORS[integrator], n, int(steps), float(dt),
+                       float(softening) * float(softening), float(opening_angle),
+                       int(leaf_capacity), 1 if quadrupole else 0, 0)
+        arrs = [_f64(state[k]) if state.get(k) is not None else None
+                for k in ("x", "y", "z", "vx", "vy", "vz", "m")]
+        job = C.c_uint64()
+        _check(self._lib.ob_server_submit(self._handle, C.byref(spec),
+                                          *(_ptr(a) for a in arrs), C.byref(job)))
+        self._sizes[job.value] = n
+        return job.value
+
+    def wait(self, job: int, timeout: float = 600.0, outputs: bool = True):
+        """(report dict, final state dict or None)."""
+        n = self._sizes.get(job, 0)
+        outputs = outputs and n > 0
+        keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+        out = {k: np.empty(n) for k in keys} if outputs else None
+        rep = JobReport()
+        ptrs = [(_ptr(out[k]) if outputs else None) for k in keys]
+        _check(self._lib.ob_server_wait(self._handle, int(job), float(timeout), C.byref(rep),
+                                        *ptrs))
+        report = {k: getattr(rep, k) for k, _ in JobReport._fields_ if k != "reserved"}
+        return report, (out if outputs and rep.status == JOB_DONE else None)
+
+    def cancel(self, job: int) -> None:
+        _check(self._lib.ob_server_cancel(self._handle, int(job)))
+
+    def stats(self) -> dict:
+        s = ServerSummary()
+        _check(self._lib.ob_server_stats(self._handle, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerSummary._fields_}
+
+    def drain(self, timeout: float = 600.0) -> None:
+        _check(self._lib.ob_server_drain(self._handle, float(timeout)))
 
 
 def compute_accelerations(positions, masses, softening: float = 0.0, solver: str = "direct",

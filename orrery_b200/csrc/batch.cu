@@ -254,34 +254,18 @@ cudaError_t launch_batch_reduce(const BatchGroup *groups, uint32_t group_count,
 // Batch
 // ---------------------------------------------------------------------------
 
-Batch::Batch(uint32_t systems, const uint64_t *counts, const double *softening_squared) {
-    if (systems == 0) {
-        throw Error(OB_ERROR_INVALID_ARGUMENT, "a batch needs at least one system");
-    }
-    uint64_t total = 0;
-    count_.resize(systems);
-    offset_.resize(systems);
-    eps2_host_.resize(systems);
-    for (uint32_t s = 0; s < systems; ++s) {
-        if (counts[s] == 0 || counts[s] > 0xffffffffull) {
-            throw Error(OB_ERROR_INVALID_ARGUMENT, "every system needs 1 .. 2^32-1 particles");
-        }
-        if (!(softening_squared[s] > 0.0) || !std::isfinite(softening_squared[s])) {
-            throw Error(OB_ERROR_INVALID_ARGUMENT,
-                        "batched systems need a positive, finite softening");
-        }
-        count_[s] = static_cast<uint32_t>(counts[s]);
-        offset_[s] = static_cast<uint32_t>(total);
-        eps2_host_[s] = softening_squared[s];
-        total += static_cast<uint64_t>(ceil_div(counts[s], kDirectTile)) * kDirectTile;
-        pairs_ += counts[s] * (counts[s] - 1);
-    }
-    // Slack past the last system for target tiles that run over (<= 1024).
-    total += 1024;
+uint64_t Batch::footprint(uint32_t n) {
+    return static_cast<uint64_t>(ceil_div(n, kDirectTile)) * kDirectTile;
+}
+
+void Batch::init(uint64_t capacity) {
+    // Slack past the arena for target tiles that run over (<= 1024).
+    const uint64_t total = capacity + 1024;
     if (total > 0x7fffffffull) {
         throw Error(OB_ERROR_CAPACITY, "a batch holds at most 2^31 padded particles");
     }
     total_ = static_cast<uint32_t>(total);
+    free_regions_.assign(1, {0u, static_cast<uint32_t>(capacity)});
     int device = 0;
     check(cudaGetDevice(&device), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "SMs");
@@ -290,17 +274,30 @@ Batch::Batch(uint32_t systems, const uint64_t *counts, const double *softening_s
     check(cudaMemset(state_.data(), 0, state_.bytes()), "clearing state");
     hi_.reserve(total_);
     lo_.reserve(total_);
-    std::vector<float> eps2f(systems);
-    for (uint32_t s = 0; s < systems; ++s) {
-        eps2f[s] = static_cast<float>(eps2_host_[s]);
-    }
-    eps2_.reserve(systems);
-    check(cudaMemcpy(eps2_.data(), eps2f.data(), sizeof(float) * systems, cudaMemcpyHostToDevice),
-          "uploading softenings");
     queue_.reserve(1);
     status_.reserve(1);
     check(cudaMemset(status_.data(), 0, sizeof(unsigned)), "clearing status");
-    build_items(config_);
+}
+
+Batch::Batch(uint64_t capacity) { init(capacity); }
+
+Batch::Batch(uint32_t systems, const uint64_t *counts, const double *softening_squared) {
+    if (systems == 0) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "a batch needs at least one system");
+    }
+    uint64_t capacity = 0;
+    for (uint32_t s = 0; s < systems; ++s) {
+        if (counts[s] == 0 || counts[s] > 0xffffffffull) {
+            throw Error(OB_ERROR_INVALID_ARGUMENT, "every system needs 1 .. 2^32-1 particles");
+        }
+        capacity += footprint(static_cast<uint32_t>(counts[s]));
+    }
+    init(capacity);
+    for (uint32_t s = 0; s < systems; ++s) {
+        if (add(static_cast<uint32_t>(counts[s]), softening_squared[s]) < 0) {
+            throw Error(OB_ERROR_CAPACITY, "the batch arena could not place a system");
+        }
+    }
 }
 
 Batch::~Batch() {
@@ -317,24 +314,125 @@ void Batch::drop_graph() {
     }
 }
 
-void Batch::build_items(const BatchConfig &config) {
+bool Batch::active(uint32_t id) const noexcept {
+    return id < members_.size() && members_[id].active;
+}
+
+void Batch::check_member(uint32_t id) const {
+    if (!active(id)) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "no such system in the batch");
+    }
+}
+
+int64_t Batch::add(uint32_t n, double softening_squared) {
+    if (n == 0) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "every system needs 1 .. 2^32-1 particles");
+    }
+    if (!(softening_squared > 0.0) || !std::isfinite(softening_squared)) {
+        throw Error(OB_ERROR_INVALID_ARGUMENT, "batched systems need a positive, finite softening");
+    }
+    const uint64_t need = footprint(n);
+    // First fit over the free regions, lowest offset first.
+    for (size_t r = 0; r < free_regions_.size(); ++r) {
+        if (free_regions_[r].second >= need) {
+            Member m;
+            m.count = n;
+            m.offset = free_regions_[r].first;
+            m.padded = static_cast<uint32_t>(need);
+            m.eps2 = softening_squared;
+            m.active = true;
+            free_regions_[r].first += m.padded;
+            free_regions_[r].second -= m.padded;
+            if (free_regions_[r].second == 0) {
+                free_regions_.erase(free_regions_.begin() + static_cast<std::ptrdiff_t>(r));
+            }
+            uint32_t id;
+            if (!free_ids_.empty()) {
+                id = free_ids_.back();
+                free_ids_.pop_back();
+                members_[id] = m;
+            } else {
+                id = static_cast<uint32_t>(members_.size());
+                members_.push_back(m);
+            }
+            if (eps2_.size() < members_.size()) {
+                DeviceArray<float> grown;
+                grown.reserve(std::max<size_t>(64, 2 * members_.size()));
+                if (eps2_.size() > 0) {
+                    check(cudaMemcpyAsync(grown.data(), eps2_.data(), eps2_.bytes(),
+                                          cudaMemcpyDeviceToDevice, stream_),
+                          "growing softenings");
+                    check(cudaStreamSynchronize(stream_), "growing softenings");
+                }
+                eps2_ = std::move(grown);
+            }
+            const float e = static_cast<float>(softening_squared);
+            check(cudaMemcpyAsync(eps2_.data() + id, &e, sizeof(float), cudaMemcpyHostToDevice,
+                                  stream_),
+                  "uploading a softening");
+            check(cudaStreamSynchronize(stream_), "uploading a softening");
+            high_ = std::max(high_, m.offset + m.padded);
+            pairs_ += static_cast<uint64_t>(n) * (n - 1);
+            ++active_count_;
+            dirty_ = true;
+            return id;
+        }
+    }
+    return -1;
+}
+
+void Batch::remove(uint32_t id) {
+    check_member(id);
+    Member &m = members_[id];
+    for (int k = 0; k < 10; ++k) {
+        check(cudaMemsetAsync(array(k) + m.offset, 0, sizeof(double) * m.padded, stream_),
+              "clearing a region");
+    }
+    // Return the region, merging with free neighbours.
+    std::pair<uint32_t, uint32_t> region{m.offset, m.padded};
+    auto it = std::lower_bound(free_regions_.begin(), free_regions_.end(), region);
+    it = free_regions_.insert(it, region);
+    if (it + 1 != free_regions_.end() && it->first + it->second == (it + 1)->first) {
+        it->second += (it + 1)->second;
+        free_regions_.erase(it + 1);
+    }
+    if (it != free_regions_.begin() && (it - 1)->first + (it - 1)->second == it->first) {
+        (it - 1)->second += it->second;
+        free_regions_.erase(it);
+    }
+    pairs_ -= static_cast<uint64_t>(m.count) * (m.count - 1);
+    m.active = false;
+    free_ids_.push_back(id);
+    --active_count_;
+    high_ = 0;
+    for (const Member &other : members_) {
+        if (other.active) {
+            high_ = std::max(high_, other.offset + other.padded);
+        }
+    }
+    dirty_ = true;
+}
+
+std::vector<BatchItem> Batch::make_items(const BatchConfig &config,
+                                         const std::vector<uint32_t> &ids,
+                                         std::vector<BatchGroup> &groups, uint32_t &slots) const {
     const uint32_t bt = static_cast<uint32_t>(config.threads * config.targets_per_thread);
     std::vector<BatchItem> items;
-    std::vector<BatchGroup> groups;
-    uint32_t slots = 0;
-    for (uint32_t s = 0; s < count_.size(); ++s) {
-        const uint32_t tiles = ceil_div(count_[s], kDirectTile);
-        const uint32_t chunk = config.chunk_tiles == 0 ? tiles : std::min(config.chunk_tiles, tiles);
+    for (const uint32_t s : ids) {
+        const Member &m = members_[s];
+        const uint32_t tiles = ceil_div(m.count, kDirectTile);
+        const uint32_t chunk =
+            config.chunk_tiles == 0 ? tiles : std::min(config.chunk_tiles, tiles);
         const uint32_t chunks = ceil_div(tiles, chunk);
-        for (uint32_t t = 0; t < count_[s]; t += bt) {
-            const uint32_t n_targets = std::min(bt, count_[s] - t);
+        for (uint32_t t = 0; t < m.count; t += bt) {
+            const uint32_t n_targets = std::min(bt, m.count - t);
             if (chunks > 1) {
-                groups.push_back(BatchGroup{offset_[s] + t, n_targets, slots, chunks});
+                groups.push_back(BatchGroup{m.offset + t, n_targets, slots, chunks});
             }
             for (uint32_t c = 0; c < chunks; ++c) {
                 const uint32_t first = c * chunk;
-                items.push_back(BatchItem{s, offset_[s] + t, n_targets,
-                                          offset_[s] + first * kDirectTile,
+                items.push_back(BatchItem{s, m.offset + t, n_targets,
+                                          m.offset + first * kDirectTile,
                                           std::min(chunk, tiles - first),
                                           chunks > 1 ? slots + c : kDirectWrite});
             }
@@ -348,39 +446,70 @@ void Batch::build_items(const BatchConfig &config) {
         return static_cast<uint64_t>(l.target_count) * l.source_tiles >
                static_cast<uint64_t>(r.target_count) * r.source_tiles;
     });
-    items_.reserve(std::max<size_t>(1, items.size()));
-    check(cudaMemcpy(items_.data(), items.data(), sizeof(BatchItem) * items.size(),
-                     cudaMemcpyHostToDevice),
-          "uploading work items");
-    groups_.reserve(std::max<size_t>(1, groups.size()));
-    if (!groups.empty()) {
-        check(cudaMemcpy(groups_.data(), groups.data(), sizeof(BatchGroup) * groups.size(),
-                         cudaMemcpyHostToDevice),
-              "uploading reduction groups");
-    }
-    partial_.reserve(std::max<size_t>(1, static_cast<size_t>(slots) * 3 * bt));
-    item_count_ = static_cast<uint32_t>(items.size());
-    group_count_ = static_cast<uint32_t>(groups.size());
-    slots_ = slots;
-    config_ = config;
-    drop_graph();
+    return items;
 }
 
-void Batch::set_config(const BatchConfig &config) { build_items(config); }
-
-void Batch::set_state(uint32_t system, const double *x, const double *y, const double *z,
-                      const double *vx, const double *vy, const double *vz, const double *m) {
-    if (system >= count_.size()) {
-        throw Error(OB_ERROR_INVALID_ARGUMENT, "no such system in the batch");
+void Batch::upload_items(const std::vector<BatchItem> &items,
+                         const std::vector<BatchGroup> &groups, uint32_t slots) {
+    const uint32_t bt = static_cast<uint32_t>(config_.threads * config_.targets_per_thread);
+    const bool moved_items = items_.reserve(std::max<size_t>(1, items.size()));
+    const bool moved_groups = groups_.reserve(std::max<size_t>(1, groups.size()));
+    const bool moved_partial =
+        partial_.reserve(std::max<size_t>(1, static_cast<size_t>(slots) * 3 * bt));
+    if (moved_items || moved_groups || moved_partial) {
+        drop_graph();
     }
+    if (!items.empty()) {
+        check(cudaMemcpyAsync(items_.data(), items.data(), sizeof(BatchItem) * items.size(),
+                              cudaMemcpyHostToDevice, stream_),
+              "uploading work items");
+    }
+    if (!groups.empty()) {
+        check(cudaMemcpyAsync(groups_.data(), groups.data(), sizeof(BatchGroup) * groups.size(),
+                              cudaMemcpyHostToDevice, stream_),
+              "uploading reduction groups");
+    }
+    check(cudaStreamSynchronize(stream_), "uploading work items");
+    item_count_ = static_cast<uint32_t>(items.size());
+    group_count_ = static_cast<uint32_t>(groups.size());
+}
+
+void Batch::rebuild_if_needed() {
+    if (!dirty_) {
+        return;
+    }
+    std::vector<uint32_t> ids;
+    for (uint32_t s = 0; s < members_.size(); ++s) {
+        if (members_[s].active) {
+            ids.push_back(s);
+        }
+    }
+    std::vector<BatchGroup> groups;
+    uint32_t slots = 0;
+    const std::vector<BatchItem> items = make_items(config_, ids, groups, slots);
+    upload_items(items, groups, slots);
+    drop_graph();
+    dirty_ = false;
+}
+
+void Batch::set_config(const BatchConfig &config) {
+    config_ = config;
+    dirty_ = true;
+    rebuild_if_needed();
+}
+
+void Batch::set_state(uint32_t id, const double *x, const double *y, const double *z,
+                      const double *vx, const double *vy, const double *vz, const double *m) {
+    check_member(id);
     if (!x || !y || !z || !m) {
         throw Error(OB_ERROR_INVALID_ARGUMENT, "positions and masses are required");
     }
+    const Member &mb = members_[id];
     const double *in[7] = {x, y, z, vx, vy, vz, m};
     const int arrays[7] = {kX, kY, kZ, kVx, kVy, kVz, kM};
-    const size_t bytes = sizeof(double) * count_[system];
+    const size_t bytes = sizeof(double) * mb.count;
     for (int k = 0; k < 7; ++k) {
-        double *dst = array(arrays[k]) + offset_[system];
+        double *dst = array(arrays[k]) + mb.offset;
         if (in[k] == nullptr) {
             check(cudaMemsetAsync(dst, 0, bytes, stream_), "clearing");
         } else {
@@ -390,23 +519,26 @@ void Batch::set_state(uint32_t system, const double *x, const double *y, const d
     check(cudaStreamSynchronize(stream_), "uploading a system");
 }
 
-void Batch::get_state(uint32_t system, double *const *out) {
-    if (system >= count_.size()) {
-        throw Error(OB_ERROR_INVALID_ARGUMENT, "no such system in the batch");
-    }
+void Batch::get_state_async(uint32_t id, double *const *out) {
+    check_member(id);
+    const Member &mb = members_[id];
     for (int k = 0; k < 9; ++k) {
         if (out[k] != nullptr) {
-            check(cudaMemcpyAsync(out[k], array(k) + offset_[system],
-                                  sizeof(double) * count_[system], cudaMemcpyDeviceToHost,
-                                  stream_),
+            check(cudaMemcpyAsync(out[k], array(k) + mb.offset, sizeof(double) * mb.count,
+                                  cudaMemcpyDeviceToHost, stream_),
                   "download");
         }
     }
+}
+
+void Batch::get_state(uint32_t id, double *const *out) {
+    get_state_async(id, out);
     check(cudaStreamSynchronize(stream_), "downloading a system");
 }
 
 void Batch::evaluate() {
-    check(pack_sources(array(kX), array(kY), array(kZ), array(kM), total_, total_, hi_.data(),
+    rebuild_if_needed();
+    check(pack_sources(array(kX), array(kY), array(kZ), array(kM), high_, high_, hi_.data(),
                        lo_.data(), stream_),
           "packing sources");
     check(cudaMemsetAsync(queue_.data(), 0, sizeof(uint32_t), stream_), "resetting the queue");
@@ -426,6 +558,35 @@ void Batch::refresh() {
     synchronize();
 }
 
+void Batch::refresh_members(const std::vector<uint32_t> &ids) {
+    for (const uint32_t id : ids) {
+        check_member(id);
+    }
+    if (ids.empty()) {
+        return;
+    }
+    // Whole-system items (no partial slots) for just these members.
+    BatchConfig whole = config_;
+    whole.chunk_tiles = 0;
+    std::vector<BatchGroup> groups;
+    uint32_t slots = 0;
+    const std::vector<BatchItem> items = make_items(whole, ids, groups, slots);
+    side_items_.reserve(items.size()); // the step graph never reads side_items_
+    check(cudaMemcpyAsync(side_items_.data(), items.data(), sizeof(BatchItem) * items.size(),
+                          cudaMemcpyHostToDevice, stream_),
+          "uploading work items");
+    check(pack_sources(array(kX), array(kY), array(kZ), array(kM), high_, high_, hi_.data(),
+                       lo_.data(), stream_),
+          "packing sources");
+    check(cudaMemsetAsync(queue_.data(), 0, sizeof(uint32_t), stream_), "resetting the queue");
+    check(launch_batch_forces(hi_.data(), lo_.data(), eps2_.data(), side_items_.data(),
+                              static_cast<uint32_t>(items.size()), whole, array(kAx), array(kAy),
+                              array(kAz), partial_.data(), queue_.data(), status_.data(),
+                              sm_count_, stream_),
+          "batched forces");
+    check(cudaStreamSynchronize(stream_), "evaluating new members");
+}
+
 static void yoshida(double &outer, double &inner) {
     constexpr double cube_root_of_two = 1.2599210498948731647672106;
     outer = 1.0 / (2.0 - cube_root_of_two);
@@ -436,12 +597,12 @@ void Batch::enqueue_step(int integrator, double dt) {
     auto substep = [&](double h) {
         const double half = h / 2.0;
         check(launch_kick_drift(array(kX), array(kY), array(kZ), array(kVx), array(kVy),
-                                array(kVz), array(kAx), array(kAy), array(kAz), total_, half, h,
+                                array(kVz), array(kAx), array(kAy), array(kAz), high_, half, h,
                                 stream_),
               "kick and drift");
         evaluate();
         check(launch_kick(array(kVx), array(kVy), array(kVz), array(kAx), array(kAy), array(kAz),
-                          total_, half, stream_),
+                          high_, half, stream_),
               "kick");
     };
     if (integrator == OB_INTEGRATOR_YOSHIDA4) {
@@ -459,6 +620,10 @@ void Batch::step_async(int integrator, double dt, uint64_t steps) {
     if (integrator != OB_INTEGRATOR_VV && integrator != OB_INTEGRATOR_YOSHIDA4) {
         throw Error(OB_ERROR_INVALID_ARGUMENT, "unknown integrator");
     }
+    if (active_count_ == 0 || steps == 0) {
+        return;
+    }
+    rebuild_if_needed();
     if (graph_ == nullptr || graph_integrator_ != integrator || graph_dt_ != dt) {
         drop_graph();
         cudaGraph_t graph = nullptr;
@@ -507,12 +672,10 @@ static double neumaier(const std::vector<double> &terms) {
     return total + correction;
 }
 
-void Batch::energy(uint32_t system, double *kinetic, double *potential) {
-    if (system >= count_.size()) {
-        throw Error(OB_ERROR_INVALID_ARGUMENT, "no such system in the batch");
-    }
-    const uint32_t n = count_[system];
-    const uint32_t o = offset_[system];
+void Batch::energy(uint32_t id, double *kinetic, double *potential) {
+    check_member(id);
+    const uint32_t n = members_[id].count;
+    const uint32_t o = members_[id].offset;
     terms_.reserve(n);
     std::vector<double> host(n);
     if (kinetic != nullptr) {
@@ -527,7 +690,7 @@ void Batch::energy(uint32_t system, double *kinetic, double *potential) {
     }
     if (potential != nullptr) {
         check(launch_potential_rows(array(kX) + o, array(kY) + o, array(kZ) + o, array(kM) + o, n,
-                                    eps2_host_[system], terms_.data(), stream_),
+                                    members_[id].eps2, terms_.data(), stream_),
               "potential rows");
         check(cudaMemcpyAsync(host.data(), terms_.data(), sizeof(double) * n,
                               cudaMemcpyDeviceToHost, stream_),
@@ -543,13 +706,11 @@ double Batch::autotune(BatchConfig &chosen) {
     cudaEvent_t start, stop;
     check(cudaEventCreate(&start), "event");
     check(cudaEventCreate(&stop), "event");
-    const BatchConfig saved = config_;
     double best = 1e300;
-    BatchConfig best_config = saved;
+    BatchConfig best_config = config_;
     for (const auto &shape : shapes) {
         for (const uint32_t chunk : chunks) {
-            const BatchConfig c{shape[0], shape[1], chunk};
-            build_items(c);
+            set_config(BatchConfig{shape[0], shape[1], chunk});
             evaluate();
             check(cudaEventRecord(start, stream_), "event");
             evaluate();
@@ -560,13 +721,13 @@ double Batch::autotune(BatchConfig &chosen) {
             check(cudaEventElapsedTime(&ms, start, stop), "autotune timing");
             if (ms / 2.0 < best) {
                 best = ms / 2.0;
-                best_config = c;
+                best_config = config_;
             }
         }
     }
     cudaEventDestroy(start);
     cudaEventDestroy(stop);
-    build_items(best_config);
+    set_config(best_config);
     // The timing runs overwrote the carried accelerations: recompute them.
     evaluate();
     synchronize();

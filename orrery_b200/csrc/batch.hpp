@@ -9,6 +9,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -56,54 +57,96 @@ cudaError_t launch_batch_reduce(const BatchGroup *groups, uint32_t group_count,
                                 const double *partial, uint32_t bt, double *ax, double *ay,
                                 double *az, cudaStream_t stream);
 
+// A set of systems sharing one padded arena in HBM. Members can be added and
+// removed between steps (the serving loop's continuous batching); the work
+// items and the step graph are rebuilt when membership changes.
 class Batch {
 public:
+    // An empty batch whose arena holds `capacity` padded particles.
+    explicit Batch(uint64_t capacity);
+    // A batch of exactly these systems (ids 0 .. systems-1).
     Batch(uint32_t systems, const uint64_t *counts, const double *softening_squared);
     ~Batch();
     Batch(const Batch &) = delete;
     Batch &operator=(const Batch &) = delete;
 
-    void set_state(uint32_t system, const double *x, const double *y, const double *z,
+    // Reserves room for a system of n particles; returns its id, or -1 when
+    // the arena has no free region large enough. The region starts zeroed.
+    int64_t add(uint32_t n, double softening_squared);
+    // Frees a member's region (zeroed so it no longer contributes anything).
+    void remove(uint32_t id);
+    [[nodiscard]] bool active(uint32_t id) const noexcept;
+    [[nodiscard]] uint32_t count(uint32_t id) const noexcept { return members_[id].count; }
+    // Padded particles the arena would take for a system of n particles.
+    static uint64_t footprint(uint32_t n);
+    // Device bytes per padded particle of the arena.
+    static constexpr uint64_t kBytesPerParticle = 10 * 8 + 32;
+
+    void set_state(uint32_t id, const double *x, const double *y, const double *z,
                    const double *vx, const double *vy, const double *vz, const double *m);
-    void get_state(uint32_t system, double *const *out);
+    void get_state(uint32_t id, double *const *out);
+    // Enqueues the download of a member's 9 arrays (x y z vx vy vz ax ay az;
+    // NULL entries skipped) on the batch stream without waiting.
+    void get_state_async(uint32_t id, double *const *out);
+    // Evaluates the accelerations of every member, or of the listed members.
     void refresh();
+    void refresh_members(const std::vector<uint32_t> &ids);
     void step_async(int integrator, double dt, uint64_t steps);
     void synchronize();
-    void energy(uint32_t system, double *kinetic, double *potential);
+    void energy(uint32_t id, double *kinetic, double *potential);
     double autotune(BatchConfig &chosen);
     void set_config(const BatchConfig &config);
 
-    [[nodiscard]] uint32_t systems() const noexcept { return static_cast<uint32_t>(count_.size()); }
+    [[nodiscard]] uint32_t members() const noexcept { return active_count_; }
     [[nodiscard]] uint64_t pair_interactions() const noexcept { return pairs_; }
     [[nodiscard]] uint64_t evaluations() const noexcept { return evaluations_; }
     [[nodiscard]] cudaStream_t stream() const noexcept { return stream_; }
-    [[nodiscard]] uint32_t items() const noexcept { return item_count_; }
+    [[nodiscard]] uint32_t items() {
+        rebuild_if_needed();
+        return item_count_;
+    }
     [[nodiscard]] const BatchConfig &config() const noexcept { return config_; }
 
 private:
+    struct Member {
+        uint32_t count = 0;
+        uint32_t offset = 0;
+        uint32_t padded = 0;
+        double eps2 = 0.0;
+        bool active = false;
+    };
     enum Array { kX = 0, kY, kZ, kVx, kVy, kVz, kAx, kAy, kAz, kM };
     double *array(int k) const noexcept { return state_.data() + static_cast<size_t>(k) * total_; }
-    void build_items(const BatchConfig &config);
+    void init(uint64_t capacity);
+    void check_member(uint32_t id) const;
+    std::vector<BatchItem> make_items(const BatchConfig &config, const std::vector<uint32_t> &ids,
+                                      std::vector<BatchGroup> &groups, uint32_t &slots) const;
+    void rebuild_if_needed();
+    void upload_items(const std::vector<BatchItem> &items, const std::vector<BatchGroup> &groups,
+                      uint32_t slots);
     void evaluate();
     void enqueue_step(int integrator, double dt);
     void drop_graph();
 
-    std::vector<uint32_t> count_;    // particles per system
-    std::vector<uint32_t> offset_;   // padded start of each system
-    std::vector<double> eps2_host_;
-    uint32_t total_ = 0;             // padded particles of all systems
-    uint64_t pairs_ = 0;             // sum N(N-1) over systems
+    std::vector<Member> members_;
+    std::vector<uint32_t> free_ids_;
+    std::vector<std::pair<uint32_t, uint32_t>> free_regions_; // (offset, size), by offset
+    uint32_t active_count_ = 0;
+    uint32_t total_ = 0;  // arena capacity in padded particles (plus slack)
+    uint32_t high_ = 0;   // end of the highest active region
+    uint64_t pairs_ = 0;  // sum N(N-1) over active members
     uint64_t evaluations_ = 0;
     int sm_count_ = 148;
-    BatchConfig config_;
+    BatchConfig config_{256, 2, 8};
+    bool dirty_ = true;
     uint32_t item_count_ = 0;
     uint32_t group_count_ = 0;
-    uint32_t slots_ = 0;
     DeviceArray<double> state_;
     DeviceArray<float4> hi_;
     DeviceArray<float4> lo_;
     DeviceArray<float> eps2_;
     DeviceArray<BatchItem> items_;
+    DeviceArray<BatchItem> side_items_;
     DeviceArray<BatchGroup> groups_;
     DeviceArray<double> partial_;
     DeviceArray<uint32_t> queue_;

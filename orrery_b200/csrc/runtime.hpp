@@ -45,6 +45,14 @@ public:
     DeviceArray &operator=(const DeviceArray &) = delete;
     DeviceArray(DeviceArray &&o) noexcept : ptr_(std::exchange(o.ptr_, nullptr)),
                                            count_(std::exchange(o.count_, 0)) {}
+    DeviceArray &operator=(DeviceArray &&o) noexcept {
+        if (this != &o) {
+            release();
+            ptr_ = std::exchange(o.ptr_, nullptr);
+            count_ = std::exchange(o.count_, 0);
+        }
+        return *this;
+    }
     ~DeviceArray() { release(); }
 
     // Returns true when the storage moved (callers holding the old pointer,
