@@ -18,6 +18,12 @@ Workloads (seeded synthetic inputs with the shapes of the measured configs):
                            [256, 16384], scale radius U[0.5, 2], eps = 0.01 x
                            radius, split precision, all systems in one
                            persistent launch, Yoshida-4 dt 1e-3 as one graph.
+  serving                  a seeded Poisson stream of jobs at 20 jobs/s (70% direct
+                           Plummer N 1k..64k x 200..2000 Yoshida-4 steps, 30%
+                           Barnes-Hut collisions N 100k..4M x 100..500 VV steps)
+                           fed in real time for --window seconds to the serving
+                           loop and, separately, to the plain drop-in run
+                           serially; completed jobs/s and latencies of both.
   direct-plummer-262144    the same at N=262,144 with the split-precision
                            kernel and Yoshida-4 dt 1e-3 (3 evaluations/step).
 
@@ -74,6 +80,9 @@ WORKLOADS = {
     "batched-512": dict(kind="batch", n=512, eps=0.01, dt=1e-3, integrator="yoshida4",
                         precision="split", metric="batched Gint/s", unit="Gint/s", higher=True,
                         generator="clusters"),
+    "serving": dict(kind="serving", n=0, eps=0.01, dt=1e-3, integrator="yoshida4",
+                    precision="split", metric="served jobs/s", unit="jobs/s", higher=True,
+                    generator="stream"),
     "direct-plummer-262144": dict(kind="direct", n=262_144, eps=0.01, dt=1e-3,
                                   integrator="yoshida4", precision="split",
                                   metric="direct Gint/s", unit="Gint/s", higher=True,
@@ -469,6 +478,172 @@ def run_batch(args, w):
         dist.destroy_process_group()
 
 
+def make_stream(window, rate=20.0, seed=20260814):
+    """Arrival times and job parameters of the serving workload."""
+    rng = np.random.default_rng(seed)
+    jobs, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= window:
+            break
+        if rng.uniform() < 0.7:
+            n = int(np.exp(rng.uniform(np.log(1000), np.log(64000))))
+            jobs.append(dict(t=t, kind="direct", n=n, steps=int(rng.integers(200, 2001)),
+                             offset=int(rng.integers(0, 1 << 30))))
+        else:
+            n = int(np.exp(rng.uniform(np.log(100_000), np.log(4_000_000))))
+            jobs.append(dict(t=t, kind="tree", n=n, steps=int(rng.integers(100, 501)),
+                             offset=int(rng.integers(0, 1 << 30))))
+    return jobs
+
+
+class Templates:
+    """Job inputs cut from two pre-shuffled templates: a 65,536-particle
+    Plummer sphere and a 4,000,000-particle two-disc collision; a random subset
+    of N particles (masses rescaled to total 1) is a system of the same kind."""
+
+    def __init__(self):
+        from orrery_b200 import initial_conditions as ic
+
+        rng = np.random.default_rng(7)
+        self.direct = ic.plummer_sphere(65536, seed=20260815)
+        self.tree = ic.galaxy_collision(4_000_000, softening=0.02, seed=20260816)
+        self.dperm = rng.permutation(65536)
+        self.tperm = rng.permutation(4_000_000)
+
+    def state(self, job):
+        src, perm = (self.direct, self.dperm) if job["kind"] == "direct" else \
+            (self.tree, self.tperm)
+        total = len(perm)
+        idx = perm[(job["offset"] + np.arange(job["n"])) % total]
+        out = {k: np.ascontiguousarray(src[k][idx]) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        out["m"] = np.full(job["n"], 1.0 / job["n"])
+        return out
+
+
+def run_serving_arm(ob, jobs, templates, window):
+    """Feeds the stream to the serving loop in real time; returns its summary."""
+    import threading
+
+    server = ob.Server(hbm_budget_bytes=150 << 30, direct_pairs_cap=4_000_000_000,
+                       max_tree_jobs=1)
+    start = time.perf_counter()
+
+    def feed():
+        for job in jobs:
+            delay = job["t"] - (time.perf_counter() - start)
+            if delay > 0:
+                time.sleep(delay)
+            if time.perf_counter() - start >= window:
+                return
+            st = templates.state(job)
+            if job["kind"] == "direct":
+                server.submit(st, steps=job["steps"], dt=1e-3, softening=0.01)
+            else:
+                server.submit(st, steps=job["steps"], dt=5e-4, softening=0.02, kind="tree",
+                              integrator="vv", quadrupole=True)
+
+    feeder = threading.Thread(target=feed)
+    feeder.start()
+    feeder.join()
+    remaining = window - (time.perf_counter() - start)
+    if remaining > 0:
+        time.sleep(remaining)
+    stats = server.stats()
+    server.close()
+    return stats
+
+
+def run_plain_arm(ob, jobs, templates, window):
+    """The same stream through the plain drop-in, one job at a time in arrival
+    order: host integrator arithmetic + ob_solver_evaluate per evaluation
+    (FP32 direct kernel / Barnes-Hut), host buffers."""
+    c = 1.2599210498948731647672106
+    weights = {"yoshida4": [1.0 / (2.0 - c), -c / (2.0 - c), 1.0 / (2.0 - c)], "vv": [1.0]}
+    start = time.perf_counter()
+    done, latencies, step_times = 0, [], []
+    solvers = {"direct": ob.B200DirectSolver(0.01, "fp32"),
+               "tree": ob.B200TreeSolver(0.02, 0.5, 32, True)}
+    for job in jobs:
+        now = time.perf_counter() - start
+        if now >= window:
+            break
+        if job["t"] > now:
+            time.sleep(job["t"] - now)
+        st = templates.state(job)
+        solver = solvers[job["kind"]]
+        dt = 1e-3 if job["kind"] == "direct" else 5e-4
+        w = weights["yoshida4" if job["kind"] == "direct" else "vv"]
+        x, y, z, m = st["x"], st["y"], st["z"], st["m"]
+        vx, vy, vz = st["vx"], st["vy"], st["vz"]
+        ax, ay, az = (np.zeros(job["n"]) for _ in range(3))
+        solver.evaluate((x, y, z), m, (ax, ay, az))
+        finished = True
+        for _ in range(job["steps"]):
+            t0 = time.perf_counter()
+            for h in w:
+                h = h * dt
+                half = h / 2.0
+                vx += half * ax
+                vy += half * ay
+                vz += half * az
+                x += h * vx
+                y += h * vy
+                z += h * vz
+                solver.evaluate((x, y, z), m, (ax, ay, az))
+                vx += half * ax
+                vy += half * ay
+                vz += half * az
+            step_times.append(time.perf_counter() - t0)
+            if time.perf_counter() - start >= window:
+                finished = False
+                break
+        if not finished:
+            break
+        done += 1
+        latencies.append(time.perf_counter() - start - job["t"])
+    pct = lambda v, q: float(np.percentile(v, q)) if v else 0.0  # noqa: E731
+    return {"completed": done, "jobs_per_s": done / window,
+            "job_latency_p50_s": pct(latencies, 50), "job_latency_p99_s": pct(latencies, 99),
+            "step_latency_p50_ms": pct(step_times, 50) * 1e3,
+            "step_latency_p99_ms": pct(step_times, 99) * 1e3}
+
+
+def run_serving(args, w):
+    import torch
+
+    import orrery_b200 as ob
+
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    ob.load_library()
+    window = float(args.window)
+    jobs = make_stream(window)
+    templates = Templates()
+    served = run_serving_arm(ob, jobs, templates, window)
+    plain = run_plain_arm(ob, jobs, templates, window)
+    if rank == 0:
+        kinds = [j["kind"] for j in jobs]
+        line = {
+            "metric": w["metric"], "value": served["jobs_per_s"], "unit": "jobs/s",
+            "n_gpus": world, "steps": len(jobs), "warmup": 0, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "state_dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "window_s": window, "arrival_rate": 20.0,
+                       "jobs_arrived": len(jobs), "direct_jobs": kinds.count("direct"),
+                       "tree_jobs": kinds.count("tree"), "hbm_budget_gb": 150,
+                       "direct_arithmetic": "split (precision form)",
+                       "plain_direct_arithmetic": "fp32"},
+            "served": {k: served[k] for k in ("completed", "jobs_per_s", "job_latency_p50_s",
+                                              "job_latency_p99_s", "step_latency_p50_ms",
+                                              "step_latency_p99_ms", "hbm_peak")},
+            "plain": plain,
+            "served_over_plain": served["jobs_per_s"] / plain["jobs_per_s"]
+            if plain["jobs_per_s"] > 0 else None,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def run_b200(args, w):
     import torch
 
@@ -626,12 +801,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
+    ap.add_argument("--window", type=float, default=30.0,
+                    help="seconds of job stream per arm (serving workload)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, w)
     elif w["kind"] == "batch":
         run_batch(args, w)
+    elif w["kind"] == "serving":
+        run_serving(args, w)
     else:
         run_b200(args, w)
 
