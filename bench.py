@@ -479,7 +479,11 @@ def run_batch(args, w):
 
 
 def make_stream(window, rate=20.0, seed=20260814):
-    """Arrival times and job parameters of the serving workload."""
+    """Arrival times and parameters of the serving workload's jobs: a Poisson
+    stream at `rate` jobs/s over `window` seconds; 70% direct Plummer jobs (N
+    log-uniform in 1k..64k, 200..2000 Yoshida-4 steps, eps 0.01, dt 1e-3) and
+    30% Barnes-Hut collision jobs (N log-uniform in 100k..4M, 100..500 VV
+    steps, theta 0.5, quadrupoles, eps 0.02, dt 5e-4)."""
     rng = np.random.default_rng(seed)
     jobs, t = [], 0.0
     while True:
@@ -497,119 +501,151 @@ def make_stream(window, rate=20.0, seed=20260814):
     return jobs
 
 
-class Templates:
-    """Job inputs cut from two pre-shuffled templates: a 65,536-particle
-    Plummer sphere and a 4,000,000-particle two-disc collision; a random subset
-    of N particles (masses rescaled to total 1) is a system of the same kind."""
+def job_states(jobs):
+    """Every job's initial state, cut from two templates: a 65,536-particle
+    Plummer sphere and a 4,000,000-particle two-disc collision. A job of N
+    particles takes N consecutive entries of a fixed random permutation of its
+    template, from a per-job offset, with masses rescaled to total 1."""
+    from orrery_b200 import initial_conditions as ic
 
-    def __init__(self):
-        from orrery_b200 import initial_conditions as ic
-
-        rng = np.random.default_rng(7)
-        self.direct = ic.plummer_sphere(65536, seed=20260815)
-        self.tree = ic.galaxy_collision(4_000_000, softening=0.02, seed=20260816)
-        self.dperm = rng.permutation(65536)
-        self.tperm = rng.permutation(4_000_000)
-
-    def state(self, job):
-        src, perm = (self.direct, self.dperm) if job["kind"] == "direct" else \
-            (self.tree, self.tperm)
-        total = len(perm)
-        idx = perm[(job["offset"] + np.arange(job["n"])) % total]
-        out = {k: np.ascontiguousarray(src[k][idx]) for k in ("x", "y", "z", "vx", "vy", "vz")}
-        out["m"] = np.full(job["n"], 1.0 / job["n"])
-        return out
+    rng = np.random.default_rng(7)
+    templates = {"direct": ic.plummer_sphere(65536, seed=20260815),
+                 "tree": ic.galaxy_collision(4_000_000, softening=0.02, seed=20260816)}
+    perms = {"direct": rng.permutation(65536), "tree": rng.permutation(4_000_000)}
+    out = []
+    for job in jobs:
+        src, perm = templates[job["kind"]], perms[job["kind"]]
+        idx = perm[(job["offset"] + np.arange(job["n"])) % len(perm)]
+        st = {k: np.ascontiguousarray(src[k][idx]) for k in ("x", "y", "z", "vx", "vy", "vz")}
+        st["m"] = np.full(job["n"], 1.0 / job["n"])
+        out.append(st)
+    return out
 
 
-def run_serving_arm(ob, jobs, templates, window):
-    """Feeds the stream to the serving loop in real time; returns its summary."""
+JOB_PARAMS = {"direct": dict(dt=1e-3, softening=0.01, integrator="yoshida4"),
+              "tree": dict(dt=5e-4, softening=0.02, integrator="vv", theta=0.5, leaf=32)}
+
+
+def served_arm(ob, jobs, states, sample):
+    """The serving loop fed in real time (each job submitted at its arrival
+    offset) and then drained. Returns per-job (arrival, finish) in seconds from
+    the start of the stream, the loop's latency statistics and the final states
+    of the `sample` jobs."""
     import threading
 
-    server = ob.Server(hbm_budget_bytes=150 << 30, direct_pairs_cap=4_000_000_000,
-                       max_tree_jobs=1)
-    start = time.perf_counter()
+    server = ob.Server(hbm_budget_bytes=150 << 30, direct_pairs_cap=1 << 34, max_tree_jobs=2)
+    ids = [None] * len(jobs)
+    origin = {}
 
     def feed():
-        for job in jobs:
-            delay = job["t"] - (time.perf_counter() - start)
+        origin["t"] = time.perf_counter()
+        for k, job in enumerate(jobs):
+            delay = job["t"] - (time.perf_counter() - origin["t"])
             if delay > 0:
                 time.sleep(delay)
-            if time.perf_counter() - start >= window:
-                return
-            st = templates.state(job)
+            p = JOB_PARAMS[job["kind"]]
             if job["kind"] == "direct":
-                server.submit(st, steps=job["steps"], dt=1e-3, softening=0.01)
+                ids[k] = server.submit(states[k], steps=job["steps"], dt=p["dt"],
+                                       softening=p["softening"])
             else:
-                server.submit(st, steps=job["steps"], dt=5e-4, softening=0.02, kind="tree",
-                              integrator="vv", quadrupole=True)
+                ids[k] = server.submit(states[k], steps=job["steps"], dt=p["dt"],
+                                       softening=p["softening"], kind="tree", integrator="vv",
+                                       opening_angle=p["theta"], leaf_capacity=p["leaf"],
+                                       quadrupole=True)
 
+    t_query = time.perf_counter()
+    server_clock0 = server.stats()["elapsed_s"]
     feeder = threading.Thread(target=feed)
     feeder.start()
     feeder.join()
-    remaining = window - (time.perf_counter() - start)
-    if remaining > 0:
-        time.sleep(remaining)
+    server.drain(timeout=3600)
+    # Server clock -> stream clock.
+    shift = server_clock0 + (origin["t"] - t_query)
+    finishes, finals = [], {}
+    for k, job in enumerate(jobs):
+        report, final = server.wait(ids[k], timeout=60, outputs=k in sample)
+        assert report["status"] == ob.JOB_DONE, report
+        finishes.append(report["finished_s"] - shift)
+        if k in sample:
+            finals[k] = final
     stats = server.stats()
     server.close()
-    return stats
+    return finishes, stats, finals
 
 
-def run_plain_arm(ob, jobs, templates, window):
-    """The same stream through the plain drop-in, one job at a time in arrival
-    order: host integrator arithmetic + ob_solver_evaluate per evaluation
-    (FP32 direct kernel / Barnes-Hut), host buffers."""
+def plain_arm(ob, torch, jobs, states, precision, sample, horizon):
+    """The plain drop-in on the same stream, one job at a time in arrival
+    order, as the reference's Simulation drives a ForceSolver: host integrator
+    arithmetic on FP64 arrays in pinned memory and ob_solver_evaluate (host
+    buffers in, accelerations out) per force evaluation. Stops early once the
+    stream clock passes `horizon` seconds (jobs not reached are reported)."""
     c = 1.2599210498948731647672106
     weights = {"yoshida4": [1.0 / (2.0 - c), -c / (2.0 - c), 1.0 / (2.0 - c)], "vv": [1.0]}
-    start = time.perf_counter()
-    done, latencies, step_times = 0, [], []
-    solvers = {"direct": ob.B200DirectSolver(0.01, "fp32"),
+    solvers = {"direct": ob.B200DirectSolver(0.01, precision),
                "tree": ob.B200TreeSolver(0.02, 0.5, 32, True)}
-    for job in jobs:
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()  # noqa: E731
+    finishes, step_times, finals = [], [], {}
+    start = time.perf_counter()
+    for k, job in enumerate(jobs):
         now = time.perf_counter() - start
-        if now >= window:
+        if now > horizon:
             break
         if job["t"] > now:
             time.sleep(job["t"] - now)
-        st = templates.state(job)
+        p, st = JOB_PARAMS[job["kind"]], states[k]
         solver = solvers[job["kind"]]
-        dt = 1e-3 if job["kind"] == "direct" else 5e-4
-        w = weights["yoshida4" if job["kind"] == "direct" else "vv"]
-        x, y, z, m = st["x"], st["y"], st["z"], st["m"]
-        vx, vy, vz = st["vx"], st["vy"], st["vz"]
-        ax, ay, az = (np.zeros(job["n"]) for _ in range(3))
+        x, y, z, m = (pin(st[q]) for q in ("x", "y", "z", "m"))
+        vx, vy, vz = (pin(st[q]) for q in ("vx", "vy", "vz"))
+        ax, ay, az = (pin(np.zeros(job["n"])) for _ in range(3))
         solver.evaluate((x, y, z), m, (ax, ay, az))
-        finished = True
         for _ in range(job["steps"]):
             t0 = time.perf_counter()
-            for h in w:
-                h = h * dt
+            for wgt in weights[p["integrator"]]:
+                h = wgt * p["dt"]
                 half = h / 2.0
-                vx += half * ax
-                vy += half * ay
-                vz += half * az
-                x += h * vx
-                y += h * vy
-                z += h * vz
+                for v, a in ((vx, ax), (vy, ay), (vz, az)):
+                    v += half * a
+                for q, v in ((x, vx), (y, vy), (z, vz)):
+                    q += h * v
                 solver.evaluate((x, y, z), m, (ax, ay, az))
-                vx += half * ax
-                vy += half * ay
-                vz += half * az
+                for v, a in ((vx, ax), (vy, ay), (vz, az)):
+                    v += half * a
             step_times.append(time.perf_counter() - t0)
-            if time.perf_counter() - start >= window:
-                finished = False
-                break
-        if not finished:
-            break
-        done += 1
-        latencies.append(time.perf_counter() - start - job["t"])
-    pct = lambda v, q: float(np.percentile(v, q)) if v else 0.0  # noqa: E731
-    return {"completed": done, "jobs_per_s": done / window,
-            "job_latency_p50_s": pct(latencies, 50), "job_latency_p99_s": pct(latencies, 99),
-            "step_latency_p50_ms": pct(step_times, 50) * 1e3,
-            "step_latency_p99_ms": pct(step_times, 99) * 1e3}
+        finishes.append(time.perf_counter() - start)
+        if k in sample:
+            finals[k] = {"x": x.copy(), "y": y.copy(), "z": z.copy(), "ax": ax.copy(),
+                         "ay": ay.copy(), "az": az.copy()}
+    return finishes, step_times, finals
+
+
+def force_errors(ob, jobs, states, finals):
+    """Per-particle relative force error of the returned accelerations against
+    the FP64 direct solver (bit-identical to the reference's) at the returned
+    positions: median and max over the sampled direct jobs' particles."""
+    errs = []
+    for k, fin in finals.items():
+        exact = ob.B200DirectSolver(JOB_PARAMS["direct"]["softening"], "fp64")
+        n = jobs[k]["n"]
+        ex, ey, ez = (np.zeros(n) for _ in range(3))
+        exact.evaluate((fin["x"], fin["y"], fin["z"]), states[k]["m"], (ex, ey, ez))
+        num = np.sqrt((fin["ax"] - ex) ** 2 + (fin["ay"] - ey) ** 2 + (fin["az"] - ez) ** 2)
+        errs.append(num / np.sqrt(ex ** 2 + ey ** 2 + ez ** 2))
+    e = np.concatenate(errs) if errs else np.zeros(1)
+    return {"median": float(np.median(e)), "max": float(np.max(e)), "jobs": len(finals),
+            "particles": int(e.size)}
+
+
+def latency_summary(jobs, finishes):
+    done = len(finishes)
+    lat = [finishes[k] - jobs[k]["t"] for k in range(done)]
+    makespan = max(finishes) if finishes else float("inf")
+    pct = lambda v, q: float(np.percentile(v, q)) if v else None  # noqa: E731
+    return {"completed": done, "makespan_s": makespan, "jobs_per_s": done / makespan,
+            "job_latency_p50_s": pct(lat, 50), "job_latency_p99_s": pct(lat, 99)}
 
 
 def run_serving(args, w):
+    """The serving form against the plain drop-in on the same job stream."""
     import torch
 
     import orrery_b200 as ob
@@ -617,29 +653,61 @@ def run_serving(args, w):
     world, rank, local = dist_env()
     torch.cuda.set_device(local)
     ob.load_library()
-    window = float(args.window)
-    jobs = make_stream(window)
-    templates = Templates()
-    served = run_serving_arm(ob, jobs, templates, window)
-    plain = run_plain_arm(ob, jobs, templates, window)
+    jobs = make_stream(args.window)
+    states = job_states(jobs)
+    direct_ids = [k for k, j in enumerate(jobs) if j["kind"] == "direct"]
+    sample = set(sorted(direct_ids, key=lambda k: jobs[k]["n"])[:3])
+    sampler = ClockSampler(local)
+    sampler.start()
+    fin_s, stats, finals_s = served_arm(ob, jobs, states, sample)
+    served = latency_summary(jobs, fin_s)
+    served.update(step_latency_p50_ms=stats["step_latency_p50_ms"],
+                  step_latency_p99_ms=stats["step_latency_p99_ms"], hbm_peak=stats["hbm_peak"],
+                  force_error=force_errors(ob, jobs, states, finals_s),
+                  direct_arithmetic="split hi/lo FP32, Kahan, FP64 tile sums")
+    plains = {}
+    for precision in args.plain_precision.split(","):
+        horizon = args.plain_horizon_factor * served["makespan_s"]
+        fin_p, steps_p, finals_p = plain_arm(ob, torch, jobs, states, precision, sample, horizon)
+        p = latency_summary(jobs, fin_p)
+        pct = lambda v, q: float(np.percentile(v, q)) * 1e3 if v else None  # noqa: E731
+        p.update(step_latency_p50_ms=pct(steps_p, 50), step_latency_p99_ms=pct(steps_p, 99),
+                 force_error=force_errors(ob, jobs, states, finals_p),
+                 direct_arithmetic=precision)
+        if p["completed"] < len(jobs):
+            p["note"] = (f"stopped after {p['completed']} of {len(jobs)} jobs once the stream "
+                         f"clock passed {horizon:.0f} s; jobs/s is completed / makespan")
+        plains[precision] = p
+    clocks = sampler.stop()
     if rank == 0:
         kinds = [j["kind"] for j in jobs]
+        first = plains[args.plain_precision.split(",")[0]]
         line = {
             "metric": w["metric"], "value": served["jobs_per_s"], "unit": "jobs/s",
-            "n_gpus": world, "steps": len(jobs), "warmup": 0, "ms_per_step": None,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "state_dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "window_s": window, "arrival_rate": 20.0,
-                       "jobs_arrived": len(jobs), "direct_jobs": kinds.count("direct"),
-                       "tree_jobs": kinds.count("tree"), "hbm_budget_gb": 150,
-                       "direct_arithmetic": "split (precision form)",
-                       "plain_direct_arithmetic": "fp32"},
-            "served": {k: served[k] for k in ("completed", "jobs_per_s", "job_latency_p50_s",
-                                              "job_latency_p99_s", "step_latency_p50_ms",
-                                              "step_latency_p99_ms", "hbm_peak")},
-            "plain": plain,
-            "served_over_plain": served["jobs_per_s"] / plain["jobs_per_s"]
-            if plain["jobs_per_s"] > 0 else None,
+            "n_gpus": world, "steps": len(jobs), "warmup": 0,
+            "ms_per_step": served["step_latency_p50_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "state_dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": args.workload, "arrival_window_s": args.window,
+                       "arrival_rate_per_s": 20.0, "jobs": len(jobs),
+                       "direct_jobs": kinds.count("direct"), "tree_jobs": kinds.count("tree"),
+                       "direct_particles": sum(j["n"] for j in jobs if j["kind"] == "direct"),
+                       "tree_particles": sum(j["n"] for j in jobs if j["kind"] == "tree"),
+                       "hbm_budget_gb": 150, "max_tree_jobs": 2, "direct_pairs_cap": 1 << 34,
+                       "jobs_per_s": "jobs / (last completion - stream start); every arm "
+                                     "drains the whole stream"},
+            "served": served,
+            "plain": plains,
+            "served_over_plain": {k: served["jobs_per_s"] / v["jobs_per_s"]
+                                  for k, v in plains.items()},
+            "e2e": {"value": served["jobs_per_s"], "unit": "jobs/s",
+                    "h2d_bytes_per_step": 56 * sum(j["n"] for j in jobs) // len(jobs),
+                    "d2h_bytes_per_step": 72 * sum(j["n"] for j in jobs) // len(jobs),
+                    "step": "one job (its state in, its final state out)",
+                    "path": "ob_server_submit (host state in) .. ob_server_wait (host state out)"},
+            "vs_plain_" + args.plain_precision.split(",")[0]:
+                served["jobs_per_s"] / first["jobs_per_s"],
+            "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
 
@@ -801,8 +869,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
-    ap.add_argument("--window", type=float, default=30.0,
-                    help="seconds of job stream per arm (serving workload)")
+    ap.add_argument("--window", type=float, default=3.0,
+                    help="serving: seconds of Poisson arrivals (every arm drains them all)")
+    ap.add_argument("--plain-precision", default="fp32",
+                    help="serving: comma-separated direct precisions of the plain arms")
+    ap.add_argument("--plain-horizon-factor", type=float, default=4.0,
+                    help="serving: a plain arm stops once its clock passes this multiple "
+                         "of the served makespan")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":
