@@ -19,6 +19,7 @@
 
 #include "batch.hpp"
 #include "common.cuh"
+#include "split_math.cuh"
 
 namespace ob {
 namespace {
@@ -37,20 +38,17 @@ struct BatchArgs {
     unsigned *status;
 };
 
-__device__ __forceinline__ void kahan(float &sum, float &c, float f, float d) {
-    const float y = fmaf(f, d, -c);
-    const float t = sum + y;
-    c = (t - sum) - y;
-    sum = t;
-}
-
+// Targets r = 2p + h of a thread are packed in pairs p; the arithmetic is
+// the split form's, in FP32x2 instructions (split_math.cuh).
 template <int THREADS, int R>
 __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a) {
+    static_assert(R % 2 == 0, "targets are processed in packed pairs");
+    constexpr int P = R / 2;
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr uint32_t BT = THREADS * R;
-    float4 *tiles_hi = reinterpret_cast<float4 *>(smem);
-    float4 *tiles_lo = tiles_hi + 2 * kDirectTile;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 2 * kDirectTile);
+    float4 *tiles_hi = reinterpret_cast<float4 *>(smem);   // 2 buffers x 2*kDirectTile
+    float4 *tiles_lo = tiles_hi + 4 * kDirectTile;         // 2 buffers x 2*kDirectTile
+    uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 4 * kDirectTile);
     __shared__ uint32_t s_item;
     const uint32_t tid = threadIdx.x;
     if (tid == 0) {
@@ -59,13 +57,12 @@ __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a)
         fence_barrier_init();
     }
     __syncthreads();
-    constexpr uint32_t bytes = kDirectTile * sizeof(float4);
+    constexpr uint32_t bytes = 2 * kDirectTile * sizeof(float4);
     auto stage = [&](uint32_t tile, uint32_t buf) {
         mbar_arrive_expect_tx(&bars[buf], 2 * bytes);
-        bulk_copy_g2s(tiles_hi + buf * kDirectTile, a.hi + static_cast<size_t>(tile) * kDirectTile,
-                      bytes, &bars[buf]);
-        bulk_copy_g2s(tiles_lo + buf * kDirectTile, a.lo + static_cast<size_t>(tile) * kDirectTile,
-                      bytes, &bars[buf]);
+        const size_t off = 2ull * static_cast<size_t>(tile) * kDirectTile;
+        bulk_copy_g2s(tiles_hi + buf * 2 * kDirectTile, a.hi + off, bytes, &bars[buf]);
+        bulk_copy_g2s(tiles_lo + buf * 2 * kDirectTile, a.lo + off, bytes, &bars[buf]);
     };
 
     uint32_t sequence = 0; // tiles this CTA has consumed (pipeline phase)
@@ -81,20 +78,16 @@ __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a)
             break;
         }
         const BatchItem item = a.items[w];
-        const float eps2 = a.eps2[item.system];
-        float hx[R], hy[R], hz[R], lx[R], ly[R], lz[R];
+        const float2 eps2 = make_float2(a.eps2[item.system], a.eps2[item.system]);
+        SplitTargets tg[P];
         double sx[R], sy[R], sz[R];
 #pragma unroll
+        for (int p = 0; p < P; ++p) {
+            const size_t i0 = item.target_begin + (2 * p) * THREADS + tid;
+            tg[p] = load_split_targets(a.hi, a.lo, i0, i0 + THREADS);
+        }
+#pragma unroll
         for (int r = 0; r < R; ++r) {
-            const uint32_t i = item.target_begin + r * THREADS + tid;
-            const float4 p = a.hi[i];
-            const float4 q = a.lo[i];
-            hx[r] = p.x;
-            hy[r] = p.y;
-            hz[r] = p.z;
-            lx[r] = q.x;
-            ly[r] = q.y;
-            lz[r] = q.z;
             sx[r] = sy[r] = sz[r] = 0.0;
         }
         const uint32_t first_tile = item.source_begin / kDirectTile;
@@ -111,37 +104,38 @@ __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a)
                 ok = mbar_wait_bounded(&bars[buf], (g >> 1) & 1u, a.status);
             }
             if (ok) {
-                const float4 *th = tiles_hi + buf * kDirectTile;
-                const float4 *tl = tiles_lo + buf * kDirectTile;
-                float kx[R], ky[R], kz[R], cx[R], cy[R], cz[R];
+                const float4 *th = tiles_hi + buf * 2 * kDirectTile;
+                const float4 *tl = tiles_lo + buf * 2 * kDirectTile;
+                float2 kx[P], ky[P], kz[P], cx[P], cy[P], cz[P];
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    kx[r] = ky[r] = kz[r] = cx[r] = cy[r] = cz[r] = 0.0f;
+                for (int p = 0; p < P; ++p) {
+                    kx[p] = ky[p] = kz[p] = cx[p] = cy[p] = cz[p] = make_float2(0.0f, 0.0f);
                 }
 #pragma unroll 2
                 for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
-                    const float4 s = th[jj];
-                    const float4 l = tl[jj];
+                    const float4 h0 = th[2 * jj], h1 = th[2 * jj + 1];
+                    const float4 l0 = tl[2 * jj], l1 = tl[2 * jj + 1];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const float dx = (s.x - hx[r]) + (l.x - lx[r]);
-                        const float dy = (s.y - hy[r]) + (l.y - ly[r]);
-                        const float dz = (s.z - hz[r]) + (l.z - lz[r]);
-                        const float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-                        float y = rsqrt_approx(r2);
-                        const float e = fmaf(-r2, y * y, 1.0f);
-                        y = fmaf(0.5f * y, e, y);
-                        const float f = (s.w * y) * (y * y);
-                        kahan(kx[r], cx[r], f, dx);
-                        kahan(ky[r], cy[r], f, dy);
-                        kahan(kz[r], cz[r], f, dz);
+                    for (int p = 0; p < P; ++p) {
+                        float2 dx, dy, dz;
+                        split_offsets(tg[p], h0, h1, l0, l1, dx, dy, dz);
+                        const float2 r2 =
+                            __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
+                        const float2 y = refined_rsqrt2(r2);
+                        const float2 f = __fmul2_rn(__fmul2_rn(pair_high(h1), y), __fmul2_rn(y, y));
+                        kahan2(kx[p], cx[p], f, dx);
+                        kahan2(ky[p], cy[p], f, dy);
+                        kahan2(kz[p], cz[p], f, dz);
                     }
                 }
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    sx[r] += static_cast<double>(kx[r]) - static_cast<double>(cx[r]);
-                    sy[r] += static_cast<double>(ky[r]) - static_cast<double>(cy[r]);
-                    sz[r] += static_cast<double>(kz[r]) - static_cast<double>(cz[r]);
+                for (int p = 0; p < P; ++p) {
+                    sx[2 * p] += static_cast<double>(kx[p].x) + static_cast<double>(cx[p].x);
+                    sx[2 * p + 1] += static_cast<double>(kx[p].y) + static_cast<double>(cx[p].y);
+                    sy[2 * p] += static_cast<double>(ky[p].x) + static_cast<double>(cy[p].x);
+                    sy[2 * p + 1] += static_cast<double>(ky[p].y) + static_cast<double>(cy[p].y);
+                    sz[2 * p] += static_cast<double>(kz[p].x) + static_cast<double>(cz[p].x);
+                    sz[2 * p + 1] += static_cast<double>(kz[p].y) + static_cast<double>(cz[p].y);
                 }
             }
             __syncthreads();
@@ -196,7 +190,7 @@ __global__ void batch_reduce_kernel(const BatchGroup *__restrict__ groups, uint3
 
 template <int THREADS, int R>
 cudaError_t launch_batch_t(const BatchArgs &args, int sm_count, cudaStream_t stream) {
-    const size_t smem = 4 * kDirectTile * sizeof(float4) + 2 * sizeof(uint64_t);
+    const size_t smem = 8 * kDirectTile * sizeof(float4) + 2 * sizeof(uint64_t);
     auto kernel = batch_split_kernel<THREADS, R>;
     static const cudaError_t configured = cudaFuncSetAttribute(
         kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -230,11 +224,10 @@ cudaError_t launch_batch_forces(const float4 *hi, const float4 *lo, const float 
 #define OB_BATCH_CASE(T, RR)                                                                       \
     if (config.threads == T && config.targets_per_thread == RR)                                    \
         return launch_batch_t<T, RR>(args, sm_count, stream);
-    OB_BATCH_CASE(128, 1)
     OB_BATCH_CASE(128, 2)
     OB_BATCH_CASE(128, 4)
-    OB_BATCH_CASE(256, 1)
     OB_BATCH_CASE(256, 2)
+    OB_BATCH_CASE(256, 4)
 #undef OB_BATCH_CASE
     return cudaErrorInvalidValue;
 }
@@ -258,7 +251,7 @@ uint64_t Batch::footprint(uint32_t n) {
     return static_cast<uint64_t>(ceil_div(n, kDirectTile)) * kDirectTile;
 }
 
-void Batch::init(uint64_t capacity) {
+void Batch::init(uint64_t capacity, cudaStream_t stream) {
     // Slack past the arena for target tiles that run over (<= 1024).
     const uint64_t total = capacity + 1024;
     if (total > 0x7fffffffull) {
@@ -269,17 +262,22 @@ void Batch::init(uint64_t capacity) {
     int device = 0;
     check(cudaGetDevice(&device), "cudaGetDevice");
     check(cudaDeviceGetAttribute(&sm_count_, cudaDevAttrMultiProcessorCount, device), "SMs");
-    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a stream");
+    if (stream != nullptr) {
+        stream_ = stream;
+        owns_stream_ = false;
+    } else {
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a stream");
+    }
     state_.reserve(10ull * total_);
     check(cudaMemset(state_.data(), 0, state_.bytes()), "clearing state");
-    hi_.reserve(total_);
-    lo_.reserve(total_);
+    hi_.reserve(2ull * total_);
+    lo_.reserve(2ull * total_);
     queue_.reserve(1);
     status_.reserve(1);
     check(cudaMemset(status_.data(), 0, sizeof(unsigned)), "clearing status");
 }
 
-Batch::Batch(uint64_t capacity) { init(capacity); }
+Batch::Batch(uint64_t capacity, cudaStream_t stream) { init(capacity, stream); }
 
 Batch::Batch(uint32_t systems, const uint64_t *counts, const double *softening_squared) {
     if (systems == 0) {
@@ -292,7 +290,7 @@ Batch::Batch(uint32_t systems, const uint64_t *counts, const double *softening_s
         }
         capacity += footprint(static_cast<uint32_t>(counts[s]));
     }
-    init(capacity);
+    init(capacity, nullptr);
     for (uint32_t s = 0; s < systems; ++s) {
         if (add(static_cast<uint32_t>(counts[s]), softening_squared[s]) < 0) {
             throw Error(OB_ERROR_CAPACITY, "the batch arena could not place a system");
@@ -302,7 +300,7 @@ Batch::Batch(uint32_t systems, const uint64_t *counts, const double *softening_s
 
 Batch::~Batch() {
     drop_graph();
-    if (stream_ != nullptr) {
+    if (stream_ != nullptr && owns_stream_) {
         cudaStreamDestroy(stream_);
     }
 }
@@ -701,7 +699,7 @@ void Batch::energy(uint32_t id, double *kinetic, double *potential) {
 }
 
 double Batch::autotune(BatchConfig &chosen) {
-    static const int shapes[][2] = {{128, 1}, {128, 2}, {128, 4}, {256, 1}, {256, 2}};
+    static const int shapes[][2] = {{128, 2}, {128, 4}, {256, 2}, {256, 4}};
     static const uint32_t chunks[] = {0, 16, 8, 4};
     cudaEvent_t start, stop;
     check(cudaEventCreate(&start), "event");

@@ -43,7 +43,7 @@ struct BatchGroup {
 // Tile shape of the batched kernel.
 struct BatchConfig {
     int threads = 128;
-    int targets_per_thread = 2;
+    int targets_per_thread = 2; // even: targets are processed in packed pairs
     uint32_t chunk_tiles = 0; // source tiles per item; 0 = a whole system
 };
 
@@ -62,8 +62,10 @@ cudaError_t launch_batch_reduce(const BatchGroup *groups, uint32_t group_count,
 // items and the step graph are rebuilt when membership changes.
 class Batch {
 public:
-    // An empty batch whose arena holds `capacity` padded particles.
-    explicit Batch(uint64_t capacity);
+    // An empty batch whose arena holds `capacity` padded particles. With
+    // `stream` given, the batch issues all its work on that stream (and does
+    // not own it); otherwise it creates its own.
+    explicit Batch(uint64_t capacity, cudaStream_t stream = nullptr);
     // A batch of exactly these systems (ids 0 .. systems-1).
     Batch(uint32_t systems, const uint64_t *counts, const double *softening_squared);
     ~Batch();
@@ -80,7 +82,7 @@ public:
     // Padded particles the arena would take for a system of n particles.
     static uint64_t footprint(uint32_t n);
     // Device bytes per padded particle of the arena.
-    static constexpr uint64_t kBytesPerParticle = 10 * 8 + 32;
+    static constexpr uint64_t kBytesPerParticle = 10 * 8 + 64;
 
     void set_state(uint32_t id, const double *x, const double *y, const double *z,
                    const double *vx, const double *vy, const double *vz, const double *m);
@@ -117,7 +119,7 @@ private:
     };
     enum Array { kX = 0, kY, kZ, kVx, kVy, kVz, kAx, kAy, kAz, kM };
     double *array(int k) const noexcept { return state_.data() + static_cast<size_t>(k) * total_; }
-    void init(uint64_t capacity);
+    void init(uint64_t capacity, cudaStream_t stream);
     void check_member(uint32_t id) const;
     std::vector<BatchItem> make_items(const BatchConfig &config, const std::vector<uint32_t> &ids,
                                       std::vector<BatchGroup> &groups, uint32_t &slots) const;
@@ -153,6 +155,7 @@ private:
     DeviceArray<unsigned> status_;
     DeviceArray<double> terms_;
     cudaStream_t stream_ = nullptr;
+    bool owns_stream_ = true;
     cudaGraphExec_t graph_ = nullptr;
     int graph_integrator_ = -1;
     double graph_dt_ = 0.0;

@@ -66,11 +66,16 @@ int set_error(int code, const std::string &message) {
 // System
 // --------------------------------------------------------------------------
 
-System::System(const ob_solver_params &params, uint32_t n)
+System::System(const ob_solver_params &params, uint32_t n, cudaStream_t stream)
     : solver_(std::make_unique<Solver>(params)), n_(n) {
     state_.reserve(10ull * (n == 0 ? 1 : n));
     check(cudaMemset(state_.data(), 0, state_.bytes()), "clearing state");
-    check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a stream");
+    if (stream != nullptr) {
+        stream_ = stream;
+        owns_stream_ = false;
+    } else {
+        check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "creating a stream");
+    }
 }
 
 System::~System() {
@@ -81,7 +86,7 @@ System::~System() {
     for (auto e : ring_) {
         cudaEventDestroy(e);
     }
-    if (stream_ != nullptr) {
+    if (stream_ != nullptr && owns_stream_) {
         cudaStreamDestroy(stream_);
     }
 }
@@ -772,11 +777,8 @@ int ob_batch_autotune(ob_batch *batch, ob_batch_shape *chosen, double *best_ms) 
 int ob_batch_set_shape(ob_batch *batch, const ob_batch_shape *shape) {
     return guarded([&] {
         require(batch != nullptr && shape != nullptr, "NULL argument");
-        const bool known = (shape->threads == 128 &&
-                            (shape->targets_per_thread == 1 || shape->targets_per_thread == 2 ||
-                             shape->targets_per_thread == 4)) ||
-                           (shape->threads == 256 &&
-                            (shape->targets_per_thread == 1 || shape->targets_per_thread == 2));
+        const bool known = (shape->threads == 128 || shape->threads == 256) &&
+                           (shape->targets_per_thread == 2 || shape->targets_per_thread == 4);
         require(known, "the library implements no such batch kernel shape");
         batch->impl->set_config(
             ob::BatchConfig{shape->threads, shape->targets_per_thread, shape->chunk_tiles});

@@ -25,6 +25,7 @@
 
 #include "common.cuh"
 #include "internal.hpp"
+#include "split_math.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -253,39 +254,33 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
     finish_targets<THREADS, R, float>(a, t0, partial, sx, sy, sz);
 }
 
-// One Kahan step: (sum, c) += term, with c holding the negated lost low part.
-__device__ __forceinline__ void kahan_add(float &sum, float &c, float f, float d) {
-    const float y = fmaf(f, d, -c);
-    const float t = sum + y;
-    c = (t - sum) - y;
-    sum = t;
-}
-
+// Split (precision) form: targets r = 2p + h are packed in pairs p and every
+// operation is an FP32x2 instruction (split_math.cuh). Tiles carry 512 sources
+// of hi and lo parts (64 bytes per source).
 template <int THREADS, int R>
 __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs a) {
+    static_assert(R % 2 == 0, "targets are processed in packed pairs");
+    constexpr int P = R / 2;
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr uint32_t BT = THREADS * R;
-    float4 *tiles_hi = reinterpret_cast<float4 *>(smem);
-    float4 *tiles_lo = tiles_hi + 2 * kDirectTile;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 2 * kDirectTile);
+    float4 *tiles_hi = reinterpret_cast<float4 *>(smem);     // 2 buffers x 2*kDirectTile
+    float4 *tiles_lo = tiles_hi + 4 * kDirectTile;           // 2 buffers x 2*kDirectTile
+    uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 4 * kDirectTile);
     double *partial = reinterpret_cast<double *>(bars + 2);
 
     const uint32_t tid = threadIdx.x;
     const uint32_t t0 = blockIdx.y * BT;
-    const float eps2 = a.eps2;
+    const float2 eps2 = make_float2(a.eps2, a.eps2);
 
-    float hx[R], hy[R], hz[R], lx[R], ly[R], lz[R];
+    SplitTargets tg[P];
     double sx[R], sy[R], sz[R];
 #pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const size_t i0 = t0 + (2 * p) * THREADS + tid;
+        tg[p] = load_split_targets(a.hi, a.lo, i0, i0 + THREADS);
+    }
+#pragma unroll
     for (int r = 0; r < R; ++r) {
-        const float4 p = a.hi[t0 + r * THREADS + tid];
-        const float4 q = a.lo[t0 + r * THREADS + tid];
-        hx[r] = p.x;
-        hy[r] = p.y;
-        hz[r] = p.z;
-        lx[r] = q.x;
-        ly[r] = q.y;
-        lz[r] = q.z;
         sx[r] = sy[r] = sz[r] = 0.0;
     }
 
@@ -297,9 +292,16 @@ __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs 
         fence_barrier_init();
     }
     __syncthreads();
+    constexpr uint32_t tile_bytes = 2 * kDirectTile * sizeof(float4);
+    auto stage = [&](uint32_t k, uint32_t buf) {
+        mbar_arrive_expect_tx(&bars[buf], 2 * tile_bytes);
+        const size_t off = 2ull * static_cast<size_t>(k) * kDirectTile;
+        bulk_copy_g2s(tiles_hi + buf * 2 * kDirectTile, a.hi + off, tile_bytes, &bars[buf]);
+        bulk_copy_g2s(tiles_lo + buf * 2 * kDirectTile, a.lo + off, tile_bytes, &bars[buf]);
+    };
     if (tid == 0) {
         for (uint32_t k = tb; k < min(tb + 2, te); ++k) {
-            stage_tile<true>(a, tiles_hi, tiles_lo, bars, k, k - tb);
+            stage(k, k - tb);
         }
     }
 
@@ -311,58 +313,72 @@ __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs 
             ok = mbar_wait_bounded(&bars[buf], (it >> 1) & 1u, a.status);
         }
         if (ok) {
-            const float4 *th = tiles_hi + buf * kDirectTile;
-            const float4 *tl = tiles_lo + buf * kDirectTile;
+            const float4 *th = tiles_hi + buf * 2 * kDirectTile;
+            const float4 *tl = tiles_lo + buf * 2 * kDirectTile;
             const uint32_t j0 = k * kDirectTile;
             const bool masked = (j0 + kDirectTile > a.n) || (j0 < t0 + BT && t0 < j0 + kDirectTile);
-            float kx[R], ky[R], kz[R], cx[R], cy[R], cz[R];
+            float2 kx[P], ky[P], kz[P], cx[P], cy[P], cz[P];
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                kx[r] = ky[r] = kz[r] = cx[r] = cy[r] = cz[r] = 0.0f;
+            for (int p = 0; p < P; ++p) {
+                kx[p] = ky[p] = kz[p] = cx[p] = cy[p] = cz[p] = make_float2(0.0f, 0.0f);
             }
+            if (!masked) {
 #pragma unroll 2
-            for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
-                const float4 s = th[jj];
-                const float4 l = tl[jj];
-                const uint32_t j = j0 + jj;
+                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                    const float4 h0 = th[2 * jj], h1 = th[2 * jj + 1];
+                    const float4 l0 = tl[2 * jj], l1 = tl[2 * jj + 1];
 #pragma unroll
-                for (int r = 0; r < R; ++r) {
-                    // Coordinate differences from the split: the hi parts are
-                    // close, so their difference is exact or nearly; the lo
-                    // parts restore the bits FP32 positions would lose.
-                    const float dx = (s.x - hx[r]) + (l.x - lx[r]);
-                    const float dy = (s.y - hy[r]) + (l.y - ly[r]);
-                    const float dz = (s.z - hz[r]) + (l.z - lz[r]);
-                    float r2 = fmaf(dz, dz, fmaf(dy, dy, fmaf(dx, dx, eps2)));
-                    float w = s.w;
-                    if (masked) {
-                        const bool skip = (j == t0 + r * THREADS + tid) || (j >= a.n);
-                        r2 = skip ? 1.0f : r2;
-                        w = skip ? 0.0f : w;
+                    for (int p = 0; p < P; ++p) {
+                        float2 dx, dy, dz;
+                        split_offsets(tg[p], h0, h1, l0, l1, dx, dy, dz);
+                        const float2 r2 =
+                            __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
+                        const float2 y = refined_rsqrt2(r2);
+                        const float2 f = __fmul2_rn(__fmul2_rn(pair_high(h1), y), __fmul2_rn(y, y));
+                        kahan2(kx[p], cx[p], f, dx);
+                        kahan2(ky[p], cy[p], f, dy);
+                        kahan2(kz[p], cz[p], f, dz);
                     }
-                    // SFU estimate refined by one Newton-Raphson step,
-                    // y <- y + (y/2)(1 - r2 y^2), to about one ulp.
-                    float y = rsqrt_approx(r2);
-                    const float e = fmaf(-r2, y * y, 1.0f);
-                    y = fmaf(0.5f * y, e, y);
-                    const float f = (w * y) * (y * y);
-                    kahan_add(kx[r], cx[r], f, dx);
-                    kahan_add(ky[r], cy[r], f, dy);
-                    kahan_add(kz[r], cz[r], f, dz);
+                }
+            } else {
+                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                    const float4 h0 = th[2 * jj], h1 = th[2 * jj + 1];
+                    const float4 l0 = tl[2 * jj], l1 = tl[2 * jj + 1];
+                    const uint32_t j = j0 + jj;
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                        const uint32_t i0 = t0 + (2 * p) * THREADS + tid;
+                        const bool skip0 = (j == i0) || (j >= a.n);
+                        const bool skip1 = (j == i0 + THREADS) || (j >= a.n);
+                        float2 dx, dy, dz;
+                        split_offsets(tg[p], h0, h1, l0, l1, dx, dy, dz);
+                        float2 r2 =
+                            __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
+                        r2 = make_float2(skip0 ? 1.0f : r2.x, skip1 ? 1.0f : r2.y);
+                        const float2 w = make_float2(skip0 ? 0.0f : h1.z, skip1 ? 0.0f : h1.w);
+                        const float2 y = refined_rsqrt2(r2);
+                        const float2 f = __fmul2_rn(__fmul2_rn(w, y), __fmul2_rn(y, y));
+                        kahan2(kx[p], cx[p], f, dx);
+                        kahan2(ky[p], cy[p], f, dy);
+                        kahan2(kz[p], cz[p], f, dz);
+                    }
                 }
             }
             // Fold the tile's compensated FP32 partials into FP64.
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                sx[r] += static_cast<double>(kx[r]) - static_cast<double>(cx[r]);
-                sy[r] += static_cast<double>(ky[r]) - static_cast<double>(cy[r]);
-                sz[r] += static_cast<double>(kz[r]) - static_cast<double>(cz[r]);
+            for (int p = 0; p < P; ++p) {
+                sx[2 * p] += static_cast<double>(kx[p].x) + static_cast<double>(cx[p].x);
+                sx[2 * p + 1] += static_cast<double>(kx[p].y) + static_cast<double>(cx[p].y);
+                sy[2 * p] += static_cast<double>(ky[p].x) + static_cast<double>(cy[p].x);
+                sy[2 * p + 1] += static_cast<double>(ky[p].y) + static_cast<double>(cy[p].y);
+                sz[2 * p] += static_cast<double>(kz[p].x) + static_cast<double>(cz[p].x);
+                sz[2 * p + 1] += static_cast<double>(kz[p].y) + static_cast<double>(cz[p].y);
             }
         }
         __syncthreads();
         if (tid == 0 && ok && k + 2 < te) {
             fence_proxy_async_shared();
-            stage_tile<true>(a, tiles_hi, tiles_lo, bars, k + 2, buf);
+            stage(k + 2, buf);
         }
     }
     finish_targets<THREADS, R, double>(a, t0, partial, sx, sy, sz);
@@ -429,9 +445,9 @@ __global__ void __launch_bounds__(kF64Threads)
     }
 }
 
-// Packs FP64 SoA into the kernels' source layout. FP32 form (lo == nullptr):
-// two float4 per particle, (x, x, y, y) and (z, z, m, m). Split form: hi =
-// (x, y, z, m) rounded, lo = (x - hi, y - hi, z - hi, 0).
+// Packs FP64 SoA into the kernels' source layout: two float4 per particle,
+// (x, x, y, y) and (z, z, m, m) rounded to FP32, and in the split form (lo
+// given) two more, (x', x', y', y') and (z', z', 0, 0) with x' = x - FP32(x).
 __global__ void pack_kernel(const double *__restrict__ x, const double *__restrict__ y,
                             const double *__restrict__ z, const double *__restrict__ m,
                             uint32_t n, uint32_t padded, float4 *hi, float4 *lo) {
@@ -443,21 +459,21 @@ __global__ void pack_kernel(const double *__restrict__ x, const double *__restri
         const float hy = __double2float_rn(Y);
         const float hz = __double2float_rn(Z);
         const float hm = real ? __double2float_rn(m[i]) : 0.0f;
-        if (lo == nullptr) {
-            hi[2ull * i] = make_float4(hx, hx, hy, hy);
-            hi[2ull * i + 1] = make_float4(hz, hz, hm, hm);
-        } else {
-            hi[i] = make_float4(hx, hy, hz, hm);
+        hi[2ull * i] = make_float4(hx, hx, hy, hy);
+        hi[2ull * i + 1] = make_float4(hz, hz, hm, hm);
+        if (lo != nullptr) {
             // X - hx is exact in FP64; rounding it gives the low part.
-            lo[i] = make_float4(__double2float_rn(X - static_cast<double>(hx)),
-                                __double2float_rn(Y - static_cast<double>(hy)),
-                                __double2float_rn(Z - static_cast<double>(hz)), 0.0f);
+            const float lx = __double2float_rn(X - static_cast<double>(hx));
+            const float ly = __double2float_rn(Y - static_cast<double>(hy));
+            const float lz = __double2float_rn(Z - static_cast<double>(hz));
+            lo[2ull * i] = make_float4(lx, lx, ly, ly);
+            lo[2ull * i + 1] = make_float4(lz, lz, 0.0f, 0.0f);
         }
     }
 }
 
 template <int THREADS, int R, bool SPLIT> size_t direct_smem_bytes() {
-    const size_t tiles = 4 * kDirectTile * sizeof(float4);
+    const size_t tiles = (SPLIT ? 8 : 4) * kDirectTile * sizeof(float4);
     const size_t partial = 3 * THREADS * R * (SPLIT ? sizeof(double) : sizeof(float));
     return tiles + 2 * sizeof(uint64_t) + partial;
 }
@@ -507,10 +523,7 @@ cudaError_t dispatch_direct(const DirectArgs &args, const DirectConfig &c, cudaS
     OB_DIRECT_CASE(128, 4)
     OB_DIRECT_CASE(256, 2)
     OB_DIRECT_CASE(256, 4)
-    if constexpr (SPLIT) {
-        OB_DIRECT_CASE(128, 1)
-        OB_DIRECT_CASE(256, 1)
-    } else {
+    if constexpr (!SPLIT) {
         OB_DIRECT_CASE(128, 8)
         OB_DIRECT_CASE(256, 8)
     }
@@ -580,12 +593,11 @@ cudaError_t launch_direct_f64(const double *x, const double *y, const double *z,
 }
 
 int direct_candidates(bool split, DirectConfig *out, int capacity) {
-    static const int split_shapes[][2] = {{128, 1}, {128, 2}, {128, 4},
-                                          {256, 1}, {256, 2}, {256, 4}};
+    static const int split_shapes[][2] = {{128, 2}, {128, 4}, {256, 2}, {256, 4}};
     static const int fp32_shapes[][2] = {{128, 2}, {128, 4}, {128, 8},
                                          {256, 2}, {256, 4}, {256, 8}};
     const int(*shapes)[2] = split ? split_shapes : fp32_shapes;
-    const int shape_count = 6;
+    const int shape_count = split ? 4 : 6;
     static const int splits[] = {1, 2, 4, 8};
     int count = 0;
     for (int s = 0; s < shape_count; ++s) {
@@ -606,9 +618,9 @@ DirectConfig direct_default_config(uint32_t n, bool split, int sm_count) {
     // shapes the autotuner picks on B200 follow this pattern).
     const uint32_t sms = static_cast<uint32_t>(sm_count > 0 ? sm_count : 148);
     DirectConfig c;
-    c.threads = split ? 256 : 256;
+    c.threads = 256;
     c.targets_per_thread = split ? 4 : 8;
-    const int smallest = split ? 1 : 2;
+    const int smallest = 2;
     const uint32_t tiles = ceil_div(n, kDirectTile);
     auto blocks = [&]() {
         return ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread));

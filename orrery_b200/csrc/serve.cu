@@ -3,13 +3,19 @@
 //
 // One host thread owns every device object. API threads only touch the job
 // table and the queues, under one mutex, and wait on a condition variable.
-// The loop never blocks on the device while work is in flight: it polls the
-// streams (cudaStreamQuery), retires finished steps and launches the next ones:
+// The loop never blocks on the device while steps are in flight: it polls one
+// event per running entity, retires finished steps and launches the next ones:
 //   * direct jobs are grouped by (integrator, dt); each group is one Batch
 //     whose step is a replayed graph; members join or leave only while the
-//     group's stream is idle, so membership changes fall between steps;
+//     group has no step in flight, so membership changes fall between steps;
 //   * each tree job is a System (the full Barnes-Hut pipeline captured as one
-//     graph per step) on its own stream.
+//     graph per step).
+// Every entity issues its work on the server's single device stream. Each
+// step runs the whole GPU (the batched kernel is persistent: its CTAs hold
+// every SM until its queue drains), so steps of different entities are
+// ordered on one stream, not interleaved kernel by kernel: an entity puts its
+// next step at the back of the stream when its previous one retires, which
+// gives round-robin service with the stream never empty while work remains.
 // With fake_device set, nothing touches CUDA: a step "runs" for a modelled
 // time, so the admission, queueing and latency logic is testable on a CPU.
 #include <algorithm>
@@ -46,9 +52,11 @@ double percentile(std::vector<double> v, double q) {
     return v[lo] + (v[hi] - v[lo]) * (pos - static_cast<double>(lo));
 }
 
-// Device bytes a tree job holds: state (80 B), ordering and scratch (~80 B)
-// and node records for about 0.75 N nodes at 188 B, per particle.
-uint64_t tree_job_bytes(uint64_t n) { return n * 80 + n * 80 + (n * 3 / 4 + 1024) * 188; }
+// Device bytes a tree job holds: state (80 B per particle), ordering, sorted
+// copy and leaf records (88 B per particle) and about 0.75 N + 1024 nodes at
+// 188 B (FP64 node 64, quadrupole 48, walk record 64, first particle 4, child
+// and arrival counts 8).
+uint64_t tree_job_bytes(uint64_t n) { return n * 80 + n * 88 + (n * 3 / 4 + 1024) * 188; }
 
 uint64_t direct_job_bytes(uint64_t n) {
     return Batch::footprint(static_cast<uint32_t>(n)) * Batch::kBytesPerParticle;
@@ -70,6 +78,7 @@ struct Job {
     bool in_flight = false;
     Clock::time_point launched;
     double fake_end = 0;            // fake mode: when the step in flight ends
+    cudaEvent_t done = nullptr;     // recorded after the step in flight
 };
 
 struct Group {
@@ -80,6 +89,7 @@ struct Group {
     Clock::time_point launched;
     double fake_end = 0;
     uint64_t pairs = 0;             // sum N(N-1) of members (fake-mode cost)
+    cudaEvent_t done = nullptr;     // recorded after the step in flight
 };
 
 } // namespace
@@ -250,6 +260,9 @@ private:
     void loop() {
         if (!config_.fake_device) {
             cudaSetDevice(device_);
+            if (cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking) != cudaSuccess) {
+                stream_ = nullptr;
+            }
         }
         while (true) {
             {
@@ -317,7 +330,8 @@ private:
             const auto key = std::make_tuple(job->spec.integrator, job->spec.dt);
             Group &g = groups_[key];
             if (!g.batch && !config_.fake_device) {
-                g.batch = std::make_unique<Batch>(config_.direct_arena_particles);
+                g.batch = std::make_unique<Batch>(config_.direct_arena_particles, device_stream());
+                check(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming), "an event");
             }
             g.joining.push_back(job);
         }
@@ -352,7 +366,8 @@ private:
         if (!config_.fake_device) {
             ob_solver_params p{OB_SOLVER_TREE, OB_PRECISION_FP32, s.softening_squared,
                                s.opening_angle, s.leaf_capacity, s.quadrupole, 0};
-            job->system = std::make_unique<System>(p, static_cast<uint32_t>(s.n));
+            job->system = std::make_unique<System>(p, static_cast<uint32_t>(s.n), device_stream());
+            check(cudaEventCreateWithFlags(&job->done, cudaEventDisableTiming), "an event");
             const size_t n = s.n;
             const double *in = job->input.data();
             job->system->set_state(in, in + n, in + 2 * n, in + 3 * n, in + 4 * n, in + 5 * n,
@@ -370,19 +385,34 @@ private:
                                         config_.fake_tree_ns_per_particle * 1e-9;
         } else {
             job->system->step_async(job->spec.integrator, job->spec.dt, 1);
+            check(cudaEventRecord(job->done, device_stream()), "recording a step");
         }
     }
 
-    bool step_done(cudaStream_t stream, double fake_end) const {
+    cudaStream_t device_stream() const {
+        if (stream_ == nullptr) {
+            throw Error(OB_ERROR_CUDA, "the server has no device stream");
+        }
+        return stream_;
+    }
+
+    bool step_done(cudaEvent_t done, double fake_end) const {
         if (config_.fake_device) {
             return now() >= fake_end;
         }
-        const cudaError_t q = cudaStreamQuery(stream);
+        const cudaError_t q = cudaEventQuery(done);
         if (q == cudaErrorNotReady) {
             return false;
         }
         check(q, "a serving step");
         return true;
+    }
+
+    static void release(cudaEvent_t &event) {
+        if (event != nullptr) {
+            cudaEventDestroy(event);
+            event = nullptr;
+        }
     }
 
     bool service_trees() {
@@ -398,7 +428,7 @@ private:
             }
         }
         for (Job *job : running) {
-            if (!step_done(job->system ? job->system->stream() : nullptr, job->fake_end)) {
+            if (!step_done(job->done, job->fake_end)) {
                 continue;
             }
             progress = true;
@@ -421,6 +451,7 @@ private:
                     fake_output(job);
                 }
                 job->system.reset();
+                release(job->done);
                 finish(job, finished ? OB_JOB_DONE : OB_JOB_CANCELLED);
                 std::lock_guard<std::mutex> lock(mutex_);
                 --running_trees_;
@@ -454,7 +485,7 @@ private:
             const int integrator = std::get<0>(entry.first);
             const double dt = std::get<1>(entry.first);
             if (g.in_flight) {
-                if (!step_done(g.batch ? g.batch->stream() : nullptr, g.fake_end)) {
+                if (!step_done(g.done, g.fake_end)) {
                     continue;
                 }
                 g.in_flight = false;
@@ -472,8 +503,8 @@ private:
                         }
                     }
                 }
-                if (g.batch) {
-                    g.batch->synchronize();
+                if (g.batch && !leaving.empty()) {
+                    g.batch->synchronize(); // also reports a device-side wait that ran out
                 }
                 for (Job *job : leaving) {
                     const bool done = job->steps_done >= job->spec.steps;
@@ -529,6 +560,7 @@ private:
                 g.in_flight = true;
                 if (g.batch) {
                     g.batch->step_async(integrator, dt, 1);
+                    check(cudaEventRecord(g.done, device_stream()), "recording a step");
                 } else {
                     const double evals = integrator == OB_INTEGRATOR_YOSHIDA4 ? 3.0 : 1.0;
                     g.fake_end = now() + evals * static_cast<double>(g.pairs) /
@@ -574,6 +606,9 @@ private:
                 direct_pairs_ -= job->spec.n * (job->spec.n - 1);
             }
         }
+        for (auto &entry : groups_) {
+            release(entry.second.done);
+        }
         groups_.clear();
         std::vector<Job *> trees;
         {
@@ -587,6 +622,7 @@ private:
         }
         for (Job *job : trees) {
             job->system.reset();
+            release(job->done);
             finish(job, OB_JOB_FAILED);
             std::lock_guard<std::mutex> lock(mutex_);
             --running_trees_;
@@ -608,25 +644,29 @@ private:
                 }
             }
         }
-        for (auto &entry : groups_) {
-            if (entry.second.batch) {
-                cudaStreamSynchronize(entry.second.batch->stream());
-            }
+        if (stream_ != nullptr) {
+            cudaStreamSynchronize(stream_);
         }
         for (Job *j : running) {
-            if (j->system) {
-                cudaStreamSynchronize(j->system->stream());
-                j->system.reset();
-            }
+            j->system.reset();
+            release(j->done);
             finish(j, OB_JOB_CANCELLED);
         }
+        for (auto &entry : groups_) {
+            release(entry.second.done);
+        }
         groups_.clear();
+        if (stream_ != nullptr) {
+            cudaStreamDestroy(stream_);
+            stream_ = nullptr;
+        }
         cv_.notify_all();
     }
 
     ob_server_config config_;
     Clock::time_point start_;
     int device_ = 0;
+    cudaStream_t stream_ = nullptr; // the device stream of every entity (loop thread)
     std::thread worker_;
     std::mutex mutex_;
     std::condition_variable cv_;

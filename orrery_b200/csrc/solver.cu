@@ -138,10 +138,10 @@ void Solver::evaluate_direct(uint32_t n, const double *x, const double *y, const
     const bool split = params_.precision == OB_PRECISION_SPLIT;
     const DirectConfig config = direct_config(n);
     const uint32_t padded = direct_padded_count(n, config);
-    if (hi_.reserve(split ? padded : 2ull * padded)) {
+    if (hi_.reserve(2ull * padded)) {
         ++generation_;
     }
-    if (split && lo_.reserve(padded)) {
+    if (split && lo_.reserve(2ull * padded)) {
         ++generation_;
     }
     check(pack_sources(x, y, z, m, n, padded, hi_.data(), split ? lo_.data() : nullptr, stream),
@@ -195,9 +195,9 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
             continue;
         }
         const uint32_t padded = direct_padded_count(n, c);
-        hi_.reserve(split ? padded : 2ull * padded);
+        hi_.reserve(2ull * padded);
         if (split) {
-            lo_.reserve(padded);
+            lo_.reserve(2ull * padded);
         }
         ++generation_;
         check(pack_sources(d, d + n, d + 2ull * n, d + 3ull * n, n, padded, hi_.data(),

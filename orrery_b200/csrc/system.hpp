@@ -21,7 +21,9 @@ class System {
 public:
     enum Array { kX = 0, kY, kZ, kVx, kVy, kVz, kAx, kAy, kAz, kM };
 
-    System(const ob_solver_params &params, uint32_t n);
+    // With `stream` given, the system issues all its work on that stream (and
+    // does not own it); otherwise it creates its own.
+    System(const ob_solver_params &params, uint32_t n, cudaStream_t stream = nullptr);
     ~System();
     System(const System &) = delete;
     System &operator=(const System &) = delete;
@@ -63,6 +65,7 @@ private:
     DeviceArray<double> state_;
     DeviceArray<double> terms_;
     cudaStream_t stream_ = nullptr;
+    bool owns_stream_ = true;
     cudaGraph_t template_ = nullptr;  // kept so its event nodes can be retargeted
     cudaGraphExec_t graph_ = nullptr;
     int graph_integrator_ = -1;

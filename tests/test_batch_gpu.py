@@ -52,8 +52,8 @@ def test_every_system_matches_the_fp64_oracle(b200, restatement):
     assert pairs == sum(int(n) * (int(n) - 1) for n in sizes) and evals == 1
 
 
-@pytest.mark.parametrize("shape", [(128, 1, 0), (128, 2, 4), (128, 4, 1), (256, 2, 0),
-                                   (256, 1, 2)])
+@pytest.mark.parametrize("shape", [(128, 2, 0), (128, 2, 4), (128, 4, 1), (256, 2, 0),
+                                   (256, 4, 2)])
 def test_every_shape_computes_the_same_sums(b200, restatement, shape):
     sizes, radii, systems = _systems(9, 5, hi=6000)
     batch = b200.DeviceBatch(sizes, 0.01 * radii)
