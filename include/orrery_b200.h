@@ -210,6 +210,17 @@ int ob_system_step(ob_system *system, int32_t integrator, double dt, uint64_t st
 
 /* The same, enqueued without waiting (sync with ob_system_synchronize). */
 int ob_system_step_async(ob_system *system, int32_t integrator, double dt, uint64_t steps);
+
+/* Integrator::step over host-resident particle data (integrator.hpp:65 with
+ * ParticleData, include/orrery/core/particle_data.hpp): uploads positions,
+ * velocities, carried accelerations and masses (all required), advances
+ * `steps` steps on the device and writes positions, velocities and
+ * accelerations back into the same arrays. Synchronous; no force evaluation
+ * beyond the steps' own (the accelerations passed in are those the previous
+ * step left, as the reference's integrators carry them). */
+int ob_system_step_host(ob_system *system, int32_t integrator, double dt, uint64_t steps,
+                        double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                        double *ax, double *ay, double *az, const double *m);
 int ob_system_synchronize(ob_system *system);
 
 /* Energies in FP64 on the device (core::kinetic_energy / potential_energy,

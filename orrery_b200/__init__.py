@@ -162,6 +162,7 @@ def load_library():
     lib.ob_system_set_state.argtypes = [vp] + [_dp] * 7
     lib.ob_system_set_accelerations.argtypes = [vp] + [_dp] * 3
     lib.ob_system_get_state.argtypes = [vp] + [_dp] * 9
+    lib.ob_system_step_host.argtypes = [vp, C.c_int32, C.c_double, C.c_uint64] + [_dp] * 10
     lib.ob_system_step.argtypes = [vp, C.c_int32, C.c_double, C.c_uint64]
     lib.ob_system_step_async.argtypes = [vp, C.c_int32, C.c_double, C.c_uint64]
     lib.ob_system_synchronize.argtypes = [vp]
@@ -468,6 +469,17 @@ class DeviceSystem:
     def step(self, dt: float, steps: int = 1, integrator: str = "vv") -> None:
         _check(self._lib.ob_system_step(self._handle, _INTEGRATORS[integrator], float(dt),
                                         int(steps)))
+
+    def step_host(self, state: dict, dt: float, steps: int = 1, integrator: str = "vv") -> None:
+        """Integrator::step over host arrays: state holds x y z vx vy vz ax ay az m
+        (contiguous FP64, updated in place)."""
+        keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
+        for k in keys:
+            a = state[k]
+            if a.dtype != np.float64 or not a.flags.c_contiguous or len(a) != self.n:
+                raise OrreryError(ERROR_INVALID_ARGUMENT, f"{k} must be contiguous FP64 of n")
+        _check(self._lib.ob_system_step_host(self._handle, _INTEGRATORS[integrator], float(dt),
+                                             int(steps), *(_ptr(state[k]) for k in keys)))
 
     def step_async(self, dt: float, steps: int = 1, integrator: str = "vv") -> None:
         _check(self._lib.ob_system_step_async(self._handle, _INTEGRATORS[integrator], float(dt),

@@ -330,6 +330,20 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
     solver_->account(steps * evaluations_per_step(integrator), n_);
 }
 
+void System::step_host(int integrator, double dt, uint64_t steps, double *const *io,
+                       const double *m) {
+    for (int k = 0; k < 9; ++k) {
+        require(n_ == 0 || io[k] != nullptr, "every state array is required");
+    }
+    require(n_ == 0 || m != nullptr, "masses are required");
+    const double *in[9] = {io[0], io[1], io[2], io[3], io[4], io[5], io[6], io[7], io[8]};
+    upload(kX, 9, in);
+    upload(kM, 1, &m);
+    step_async(integrator, dt, steps);
+    get_state(io);
+    synchronize();
+}
+
 void System::synchronize() {
     check(cudaStreamSynchronize(stream_), "integrating");
     solver_->check_status(stream_);
@@ -587,6 +601,16 @@ int ob_system_set_accelerations(ob_system *system, const double *ax, const doubl
     return guarded([&] {
         require(system != nullptr, "system is NULL");
         system->impl->set_accelerations(ax, ay, az);
+    });
+}
+
+int ob_system_step_host(ob_system *system, int32_t integrator, double dt, uint64_t steps,
+                        double *x, double *y, double *z, double *vx, double *vy, double *vz,
+                        double *ax, double *ay, double *az, const double *m) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        double *io[9] = {x, y, z, vx, vy, vz, ax, ay, az};
+        system->impl->step_host(integrator, dt, steps, io, m);
     });
 }
 

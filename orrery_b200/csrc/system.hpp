@@ -34,6 +34,8 @@ public:
     void get_state(double *const *out); // x y z vx vy vz ax ay az, NULL entries skipped
     void refresh();
     void step_async(int integrator, double dt, uint64_t steps);
+    // Uploads x y z vx vy vz ax ay az (io) and m, steps, downloads io.
+    void step_host(int integrator, double dt, uint64_t steps, double *const *io, const double *m);
     void synchronize();
     void energy(double *kinetic, double *potential);
 

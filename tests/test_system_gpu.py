@@ -55,6 +55,22 @@ def test_steps_split_across_calls_equal_one_call(b200, golden_trajectory):
     assert all(np.array_equal(sa[k], sb[k]) for k in KEYS)
 
 
+@pytest.mark.parametrize("integrator", ["vv", "yoshida4"])
+def test_host_state_steps_equal_resident_steps(b200, golden_trajectory, integrator):
+    # Integrator::step over host arrays (upload, device step, download) is the
+    # resident step: the carried accelerations make each call independent.
+    g = golden_trajectory
+    a = _system(b200, g, "fp64")
+    a.step(1e-3, 3, integrator)
+    b = _system(b200, g, "fp64")
+    host = b.state()
+    host["m"] = np.ascontiguousarray(g["m"], dtype=np.float64)
+    for _ in range(3):
+        b.step_host(host, 1e-3, 1, integrator)
+    sa = a.state()
+    assert all(np.array_equal(sa[k], host[k]) for k in KEYS)
+
+
 def test_energies_are_bit_identical(b200, golden_plummer):
     g = golden_plummer
     s = b200.DeviceSystem(len(g["m"]), 0.01, precision="fp64")
