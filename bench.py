@@ -339,6 +339,21 @@ def config_of(args, w):
 # The B200 arm
 # ---------------------------------------------------------------------------
 
+# DRAM bytes (read + write) per launch of each dominant kernel, from one ncu
+# capture each, scaled to the workload by the units one launch processes
+# (the captures and commands are in profiles/):
+#   walk: 31.34 MB for 500,000 targets (L2-resident case; lower bound at 2M);
+#   direct FP32 / split at 262,144: 8.47 MB / 17.20 MB, reads of the packed
+#   sources through L2, proportional to N;
+#   batch: 258.9 MB for 1.742e10 pairs (sources re-read per target tile).
+TRAFFIC_BYTES = {
+    ("walk", "fp32"): lambda n: 31.34e6 * n / 500_000,
+    ("direct", "fp32"): lambda n: 8.47e6 * n / 262_144,
+    ("direct", "split"): lambda n: 17.20e6 * n / 262_144,
+    ("batch", "split"): lambda pairs: 258.9e6 * pairs / 1.7416705824e10,
+}
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -444,7 +459,7 @@ def run_batch(args, w):
     value = pairs * evals * K * world / (total_ms * 1e-3) / 1e9
     if rank == 0:
         ffma, rsq = ob.probe_fp32()
-        peak = min(ffma / 12.0, rsq) / 1e9
+        peak = min(ffma / 31.0, rsq) / 1e9
         achieved = pairs * evals / (tuned_ms * 1e-3 * evals) / 1e9
         # e2e through the public API with host buffers: each step uploads every
         # system's state from pinned memory and downloads it again.
@@ -473,10 +488,11 @@ def run_batch(args, w):
                                            "chunk_tiles": shape[2]},
                        "l2": "inputs larger than L2"},
             "roofline": {"bound": "fp32-fma-pipe", "achieved": achieved, "peak": peak,
-                         "unit": "Gint/s", "frac": achieved / peak, "traffic": None,
+                         "unit": "Gint/s", "frac": achieved / peak,
+                         "traffic": TRAFFIC_BYTES[("batch", "split")](pairs),
                          "kernel_ms": tuned_ms,
-                         "note": "peak counts 12 FP32 operations per interaction (the plain "
-                                 "kernel); the split arithmetic issues about 30"},
+                         "peak_source": "measured FFMA lane rate / 31 FP32 operations per "
+                                        "interaction of the split arithmetic"},
             "e2e": {"value": pairs * evals / sec / 1e9, "unit": w["unit"],
                     "h2d_bytes_per_step": total_n * 7 * 8, "d2h_bytes_per_step": total_n * 9 * 8,
                     "path": "ob_batch_set_state for every system, one step, ob_batch_get_state"},
@@ -810,17 +826,19 @@ def run_b200(args, w):
     if w["kind"] == "direct":
         ffma, rsq = ob.probe_fp32()
         # FP32 interaction peak: the FMA pipe carries 12 lane operations per
-        # interaction (3 sub, 3 fma for r^2, 3 mul, 3 fma); the SFU one rsqrt.
-        peak_gint = min(ffma / 12.0, rsq) / 1e9
+        # interaction in FP32 (3 sub, 3 fma for r^2, 3 mul, 3 fma) and 31 in
+        # the split arithmetic (9 hi/lo differences, 3 r^2, 4 Newton, 3 m y^3,
+        # 12 Kahan); the SFU one rsqrt either way.
+        ops = 31.0 if w["precision"] == "split" else 12.0
+        peak_gint = min(ffma / ops, rsq) / 1e9
         achieved = n * (n - 1) / (kernel_ms * 1e-3) / 1e9
         roofline = {"bound": "fp32-fma-pipe", "achieved": achieved, "peak": peak_gint,
-                    "unit": "Gint/s", "frac": achieved / peak_gint, "traffic": None,
-                    "peak_source": "measured FFMA lane rate / 12 FP32 operations per "
+                    "unit": "Gint/s", "frac": achieved / peak_gint,
+                    "traffic": TRAFFIC_BYTES.get(("direct", w["precision"]), lambda n: None)(n),
+                    "peak_source": f"measured FFMA lane rate / {ops:.0f} FP32 operations per "
                                    f"interaction (FFMA {ffma / 1e12:.2f} T lane-op/s, SFU "
-                                   f"rsqrt {rsq / 1e12:.2f} T/s) on this GPU; with 13 issue "
-                                   "slots per interaction (no packed FP32x2) the bound is "
-                                   f"{ffma / 13.0 / 1e9:.0f} Gint/s",
-                    "gflops_20_per_interaction": achieved * 20.0,
+                                   f"rsqrt {rsq / 1e12:.2f} T/s) on this GPU",
+                    "fp32_interaction_peak_gint_s": min(ffma / 12.0, rsq) / 1e9,
                     "kernel_ms": kernel_ms}
     else:
         # The walk keeps its nodes and leaf sources in L2 and is bound by the
@@ -837,7 +855,8 @@ def run_b200(args, w):
         roofline = {"bound": "fp32-fma-pipe", "achieved": achieved_t, "peak": ffma / 1e12,
                     "unit": "T FP32 op/s", "frac": achieved_t / (ffma / 1e12),
                     "peak_source": "measured FFMA lane rate on this GPU (ob_probe_fp32)",
-                    "algorithmic_fp32_ops": ops, "kernel_ms": kernel_ms, "traffic": None,
+                    "algorithmic_fp32_ops": ops, "kernel_ms": kernel_ms,
+                    "traffic": TRAFFIC_BYTES[("walk", "fp32")](n),
                     "hbm": {"peak": hbm, "unit": "GB/s",
                             "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs, a copy "
                                            "kernel)"}}
