@@ -288,14 +288,92 @@ def cpu_baseline_batch(w, sizes, radii, systems, budget_s=15.0):
                        f"first {count} of {len(systems)} clusters")
 
 
+def cpu_baseline_serving(w, budget_s):
+    """The reference's CPU solvers (all host threads) on the serving stream in
+    arrival order: one timed force evaluation per job until the budget is
+    spent, each job's time taken as that evaluation times its evaluation count
+    (its own steps x evaluations per step, plus the initial one)."""
+    import oracle
+
+    ref = oracle.Reference()
+    threads = ref.worker_count()
+    jobs = make_stream(3.0)
+    states = job_states(jobs)
+    projected, spent, done = 0.0, 0.0, 0
+    for job, st in zip(jobs, states):
+        p = JOB_PARAMS[job["kind"]]
+        if job["kind"] == "direct":
+            sec = ref.direct_seconds(st["x"], st["y"], st["z"], st["m"], p["softening"], threads,
+                                     repeats=1)
+            evals = 1 + 3 * job["steps"]
+        else:
+            sec = ref.barnes_hut_seconds(st["x"], st["y"], st["z"], st["m"], p["softening"],
+                                         p["theta"], p["leaf"], True, threads, repeats=1)
+            evals = 1 + job["steps"]
+        projected += sec * evals
+        spent += sec
+        done += 1
+        if spent > budget_s:
+            break
+    return dict(value=done / projected, unit="jobs/s", cores=threads, kind="reference",
+                sample=f"one timed force evaluation of each of the stream's first {done} jobs "
+                       f"(of {len(jobs)}), scaled by each job's evaluation count; jobs run "
+                       "serially")
+
+
+def reference_gpu(w, data):
+    """The reference's own CUDA solvers (its .cu kernels built for sm_100a by
+    oracle/Makefile) on the same input and device, when built and a device is
+    present: per-evaluation wall time of its host-buffer evaluate and its
+    kernel time."""
+    import oracle
+
+    if w["kind"] not in ("direct", "tree") or not oracle.ReferenceCuda.built():
+        return None
+    try:
+        ref = oracle.ReferenceCuda()
+        if not ref.available():
+            return None
+        x, y, z, m = (np.ascontiguousarray(data[k]) for k in ("x", "y", "z", "m"))
+        n = len(m)
+        if w["kind"] == "direct":
+            wall, kern, _ = ref.direct_timed(x, y, z, m, w["eps"], repeats=3)
+            return {"solver": "CudaDirectSolver (FP64 Real, the reference's direct_kernel)",
+                    "kernel_gint_s": n * (n - 1) / kern / 1e9,
+                    "evaluate_gint_s": n * (n - 1) / wall / 1e9,
+                    "kernel_ms": kern * 1e3, "evaluate_ms": wall * 1e3}
+        threads = oracle.Reference().worker_count() if oracle.Reference.available() else 1
+        wall, kern, _, counts = ref.tree_timed(x, y, z, m, w["eps"], w["theta"], w["leaf"],
+                                               w["quadrupole"], threads, repeats=1)
+        return {"solver": "CudaTreeSolver (host sort and build on "
+                          f"{threads} threads, coherent traversal on the device)",
+                "evaluate_ms": wall * 1e3, "kernel_ms": kern * 1e3,
+                "pairs": counts[0], "cells": counts[1]}
+    except (OSError, RuntimeError) as err:
+        return {"unavailable": str(err)}
+
+
 def run_reference(args, w):
     world, rank, local = dist_env()
     dist = init_dist(world, "gloo")
     if rank != 0:
         barrier(dist)
         return
-    data = make_inputs(w)
     steps = max(1, args.steps)
+    if w["kind"] == "serving":
+        base = cpu_baseline_serving(w, budget_s=min(60.0, 10.0 * steps))
+        line = {"impl": "reference", "metric": w["metric"], "value": base["value"],
+                "unit": "jobs/s", "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+                "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "arrival_window_s": 3.0},
+                "cpu_baseline": base,
+                "e2e": {"value": base["value"], "unit": "jobs/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        barrier(dist)
+        return
+    data = make_inputs(w)
     if w["kind"] == "batch":
         base = cpu_baseline_batch(w, *data, budget_s=min(60.0, 10.0 * steps))
     else:
@@ -316,6 +394,9 @@ def run_reference(args, w):
         "e2e": {"value": value, "unit": w["unit"], "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    gpu = reference_gpu(w, data) if w["kind"] != "batch" else None
+    if gpu is not None:
+        line["reference_gpu"] = gpu
     print(json.dumps(line), flush=True)
     barrier(dist)
 
@@ -860,7 +941,6 @@ def run_b200(args, w):
                     "hbm": {"peak": hbm, "unit": "GB/s",
                             "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs, a copy "
                                            "kernel)"}}
-    line = None
     line = None
     if rank == 0:
         e2e_steps = max(2, min(K, 10 if w["kind"] == "tree" else 50))

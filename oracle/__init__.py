@@ -7,6 +7,9 @@ Two libraries, both built by ``oracle/Makefile``:
 * ``reference`` -- ``_ref/libref_orrery.so``, the reference's own CPU sources
   compiled where they lie, behind a small C shim (ref_shim.cpp). Present only
   where it was built (it travels with the repository snapshot as a built file).
+* ``reference CUDA`` -- ``_ref/libref_orrery_cuda.so``, the same plus the
+  reference's CUDA solvers (its .cu kernels compiled for sm_100a), behind
+  ref_cuda_shim.cpp: the reference's GPU path, timed beside this backend's.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
 ``bench.py`` may import this package. The product never does.
@@ -22,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_PATH = os.path.join(HERE, "_lib", "liboracle.so")
 REFERENCE_PATH = os.path.join(HERE, "_ref", "libref_orrery.so")
+REFERENCE_CUDA_PATH = os.path.join(HERE, "_ref", "libref_orrery_cuda.so")
 
 _dp = C.POINTER(C.c_double)
 _u64p = C.POINTER(C.c_uint64)
@@ -40,7 +44,8 @@ def build(reference_root: str | None = None, with_reference: bool = True) -> Non
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
     root = reference_root or os.environ.get("ORRERY_REFERENCE_ROOT", "/root/reference")
     if with_reference and os.path.isdir(os.path.join(root, "src", "solvers")):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={root}"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "ref_cuda", f"REF={root}"],
+                       check=True)
 
 
 class Counts(C.Structure):
@@ -378,3 +383,54 @@ class Reference:
 
     def kinetic_energy(self, vx, vy, vz, m):
         return self.lib.ref_kinetic_energy(len(m), _d(vx), _d(vy), _d(vz), _d(m))
+
+
+class ReferenceCuda:
+    """ctypes binding of ref_cuda_shim.cpp: the reference's CudaDirectSolver and
+    CudaTreeSolver (its own GPU path) on this machine's device."""
+
+    @staticmethod
+    def built() -> bool:
+        return os.path.exists(REFERENCE_CUDA_PATH)
+
+    def __init__(self, path: str = REFERENCE_CUDA_PATH):
+        lib = C.CDLL(path)
+        lib.ref_cuda_direct_timed.argtypes = [C.c_size_t] + [_dp] * 4 + [
+            C.c_double, C.c_int, _dp, _dp, _dp, _dp, _dp]
+        lib.ref_cuda_tree_timed.argtypes = [C.c_size_t] + [_dp] * 4 + [
+            C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp,
+            _dp, _u64p]
+        self.lib = lib
+
+    def available(self) -> bool:
+        return bool(self.lib.ref_cuda_available())
+
+    def direct_timed(self, x, y, z, m, softening, repeats=3):
+        """(wall s per evaluation, kernel s per evaluation, accelerations (n, 3))."""
+        x, y, z, m = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, m))
+        n = len(m)
+        a = [np.zeros(n) for _ in range(3)]
+        wall, kern = C.c_double(), C.c_double()
+        rc = self.lib.ref_cuda_direct_timed(n, _d(x), _d(y), _d(z), _d(m), softening,
+                                            int(repeats), C.byref(wall), C.byref(kern),
+                                            *(_d(v) for v in a))
+        if rc != 0:
+            raise RuntimeError("the reference's CUDA direct solver found no device")
+        return wall.value, kern.value, np.stack(a, axis=1)
+
+    def tree_timed(self, x, y, z, m, softening, opening_angle, leaf_capacity, quadrupole,
+                   threads, repeats=1):
+        """(wall s, kernel s, accelerations (n, 3), (pairs, cells)) per evaluation."""
+        x, y, z, m = (np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, m))
+        n = len(m)
+        a = [np.zeros(n) for _ in range(3)]
+        counts = np.zeros(2, np.uint64)
+        wall, kern = C.c_double(), C.c_double()
+        rc = self.lib.ref_cuda_tree_timed(n, _d(x), _d(y), _d(z), _d(m), softening,
+                                          opening_angle, int(leaf_capacity),
+                                          1 if quadrupole else 0, int(threads), int(repeats),
+                                          C.byref(wall), C.byref(kern), *(_d(v) for v in a),
+                                          _u(counts))
+        if rc != 0:
+            raise RuntimeError("the reference's CUDA tree solver found no device")
+        return wall.value, kern.value, np.stack(a, axis=1), (int(counts[0]), int(counts[1]))
