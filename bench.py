@@ -844,6 +844,10 @@ def run_b200(args, w):
                              quadrupole=w.get("quadrupole", False))
     system.set_state(data["x"], data["y"], data["z"], data["vx"], data["vy"], data["vz"],
                      data["m"])
+    # The precision form states its energy drift from t = 0 (FP64 energies
+    # on the device, outside the timed region).
+    track_accuracy = w["kind"] == "direct" and w["precision"] == "split"
+    energy0 = sum(system.energy()) if track_accuracy else None
     tuned = None
     if w["kind"] == "direct" and w["precision"] != "fp64":
         tuned = system.autotune()
@@ -897,6 +901,23 @@ def run_b200(args, w):
     cell_count = counts_end.particle_cell - counts_start.particle_cell
 
     ms_per_step = total_ms / K
+    accuracy = None
+    if track_accuracy:
+        extra = max(0, args.accuracy_steps - max(args.warmup, 3) - K)
+        if extra:
+            system.step(w["dt"], extra, w["integrator"])
+        energy1 = sum(system.energy())
+        st = system.state()
+        exact = ob.B200DirectSolver(w["eps"], "fp64").evaluate((st["x"], st["y"], st["z"]),
+                                                               data["m"])
+        got = np.stack([st["ax"], st["ay"], st["az"]], axis=1)
+        err = np.linalg.norm(got - exact, axis=1) / np.linalg.norm(exact, axis=1)
+        accuracy = {"steps": max(args.warmup, 3) + K + extra,
+                    "relative_energy_drift": (energy1 - energy0) / abs(energy0),
+                    "force_error_vs_fp64": {"median": float(np.median(err)),
+                                            "max": float(np.max(err)),
+                                            "at": "the final state, against the bit-exact "
+                                                  "FP64 direct solver"}}
     if w["unit"] == "ms/step":
         value = ms_per_step / world  # whole-job time per 2M step across replicas
     else:
@@ -982,6 +1003,7 @@ def run_b200(args, w):
             "autotuned_shape": None if tuned is None else
             {"threads": tuned[0][0], "targets_per_thread": tuned[0][1], "split": tuned[0][2]},
             "roofline": roofline,
+            "accuracy": accuracy,
             "e2e": {"value": e2e_value, "unit": w["unit"], "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h,
                     "path": "ob_system_step_host: Integrator::step over pinned host particle "
@@ -1013,6 +1035,9 @@ def main():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default=DEFAULT_WORKLOAD)
     ap.add_argument("--window", type=float, default=3.0,
                     help="serving: seconds of Poisson arrivals (every arm drains them all)")
+    ap.add_argument("--accuracy-steps", type=int, default=0,
+                    help="split direct workloads: total steps after which energy drift and "
+                         "force error are stated (default: the warm-up and timed steps)")
     ap.add_argument("--plain-precision", default="fp32",
                     help="serving: comma-separated direct precisions of the plain arms")
     ap.add_argument("--plain-horizon-factor", type=float, default=4.0,

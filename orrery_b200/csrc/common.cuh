@@ -11,6 +11,8 @@ namespace ob {
 // the host turns the bit into OB_ERROR_TIMEOUT after the next synchronisation.
 constexpr unsigned kStatusTimeout = 1u;
 constexpr unsigned kStatusOverflow = 2u;
+// An index a valid data structure never holds was found and its access skipped.
+constexpr unsigned kStatusInvalid = 4u;
 
 // Upper bound on polls of one mbarrier phase (each poll of try_wait already
 // suspends for a hardware-defined interval); well above any legitimate wait.

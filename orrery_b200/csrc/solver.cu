@@ -319,6 +319,9 @@ bool Solver::grew_after_overflow(cudaStream_t stream) {
     if (status & kStatusTimeout) {
         throw Error(OB_ERROR_TIMEOUT, "a device-side wait ran out of its bound");
     }
+    if (status & kStatusInvalid) {
+        throw Error(OB_ERROR_CUDA, "a kernel met an index its data structure cannot hold");
+    }
     if ((status & kStatusOverflow) && tree_) {
         const uint32_t required = tree_->meta().required;
         tree_->grow_nodes(required + required / 4 + 1024);
@@ -334,6 +337,9 @@ void Solver::check_status(cudaStream_t stream) {
     const unsigned status = read_and_clear_status(status_.data(), stream);
     if (status & kStatusTimeout) {
         throw Error(OB_ERROR_TIMEOUT, "a device-side wait ran out of its bound");
+    }
+    if (status & kStatusInvalid) {
+        throw Error(OB_ERROR_CUDA, "a kernel met an index its data structure cannot hold");
     }
     if (status & kStatusOverflow) {
         throw Error(OB_ERROR_CAPACITY, "a device-side buffer bound was exceeded");

@@ -607,7 +607,7 @@ void TreePipeline::evaluate(uint32_t n, const double *x, const double *y, const 
     check(launch_walk(nodes_.data(), walk_nodes_.data(), first_of_.data(), leaf_rel_.data(),
                       sorted_.data(), perm, n, params_.softening_squared,
                       params_.quadrupole != 0, ax, ay, az, meta_.data(), counters_.data(),
-                      stream),
+                      status, stream),
           "tree walk");
 }
 

@@ -87,6 +87,6 @@ cudaError_t launch_walk(const DeviceNode *nodes, const WalkNode *walk_nodes,
                         const uint32_t *first_of, const float4 *leaf_rel, const double *sorted,
                         const uint32_t *perm, uint32_t n, double eps2, bool quadrupole,
                         double *ax, double *ay, double *az, TreeMeta *meta,
-                        unsigned long long *counters, cudaStream_t stream);
+                        unsigned long long *counters, unsigned *status, cudaStream_t stream);
 
 } // namespace ob

@@ -8,37 +8,110 @@
 // a pair sum that skips the target itself; an opened internal node is
 // descended. Pair and cell counts are the reference's.
 //
-// The warp walks the union of its lanes' walks: each lane keeps its own
-// cursor, the warp visits the smallest cursor any lane holds, and only lanes
-// whose cursor is that node act on it. Every lane loads the same node, so the
-// loads are broadcasts. When lanes open a leaf, the warp stages the leaf's
-// particles in shared memory once and each interested lane sums them.
+// Group traversal. The warp walks the tree once for its 32 targets, carrying
+// with every node the mask of targets whose own walks reach it (those that
+// opened all its ancestors). A node is classified against the FP64 bounding
+// box of the targets: with d_min / d_max the per-axis distances from the
+// centre of mass to the nearest / farthest box face, computed with the
+// reference's FP64 operations in its order, every target's own |d|^2 lies in
+// [d_min^2, d_max^2] because rounding is monotone, so
+//   d_min^2 >= r2  ->  every target accepts the cell (exactly the reference);
+//   d_max^2 <  r2  ->  every target opens it;
+//   otherwise      ->  mixed: each target decides for itself (an FP32 hi/lo
+//                      test with a 4e-6 relative margin, the reference's FP64
+//                      test inside the margin).
+// Lanes take different nodes of a depth-first stack of (node, reach mask,
+// end of the parent's range) items, 32 per round; an item pushes its next
+// sibling and, when opened, its first child. Accepted cells and opened leaves
+// go to per-warp lists with their target masks, which are evaluated in
+// batches: every lane evaluates every entry for its own target (a lane outside
+// an entry's mask contributes exactly zero), two entries per packed FP32x2
+// instruction, reading the entries as shared-memory broadcasts.
 //
 // Arithmetic. Positions and centres of mass are carried as FP32 hi + lo pairs
 // (exact to ~2^-48 relative), so the offset to a cell comes out in FP32 to
-// about 2e-7 relative with no FP64 work and no conversions. The accept test is
-// decided in FP32 whenever |d^2 - r2| is clearly larger than the FP32 error
-// bound (a relative margin of 4e-6 against a worst case of about 6e-7); only
-// the rare cells inside the margin repeat the reference's FP64 test exactly.
-// Force terms are FP32, accumulated in FP32 between leaf visits and flushed
-// into FP64 per-lane sums.
+// about 2e-7 relative with no FP64 work. Force terms are FP32, summed in FP32
+// within a batch (or leaf) and flushed into FP64 per-target sums.
+//
+// If a warp's stack would overflow its fixed shared-memory capacity (never
+// seen: 121 items at most against 256 on the 2M collision), the warp discards
+// its partial sums and walks its targets with the per-target union walk
+// (union_walk below), which gives the same counts.
+//
+// Warp discipline. Between the warp's votes and barriers there is no
+// lane-divergent stretch of work: lanes outside a leaf's or cell's mask run
+// the same arithmetic with zero weight, and the FP64 accept test runs on
+// every lane once any lane needs it. (Votes and warp barriers of the same kind
+// may be satisfied by lanes standing at different instructions, so a warp
+// whose lanes spent long, different times in divergent code was seen to fall
+// out of step: lanes of different rounds then shared one vote.) Node and
+// particle indices are checked before every gather; an index out of range
+// (which a valid tree never produces) sets kStatusInvalid and is skipped.
 #include "common.cuh"
 #include "tree_kernels.hpp"
 
 namespace ob {
 namespace {
 
-constexpr int kWalkThreads = 128;
-constexpr int kWalkWarps = kWalkThreads / 32;
+constexpr int kWalkWarps = 4;
+constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr float kAcceptMargin = 4e-6f;
+constexpr uint32_t kFull = 0xffffffffu;
 
-__device__ __forceinline__ uint32_t warp_min(uint32_t v) {
-    return __reduce_min_sync(0xffffffffu, v);
+// Per-warp shared-memory capacities (entries). A round adds at most 64 stack
+// items (32 siblings, 32 first children), 64 cells (32 accepted by all, 32
+// accepted by some of a mixed node) and 64 leaves.
+constexpr uint32_t kStackCap = 256;
+constexpr uint32_t kCellCap = 128;
+constexpr uint32_t kLeafCap = 96;
+
+struct GroupItem {
+    uint32_t node;
+    uint32_t mask; // targets whose walks reach the node
+    uint32_t end;  // end of the parent's subtree: the next sibling exists below it
+};
+
+// Cell fields staged for a batch of 32 cells, structure of arrays of packed
+// pairs: entry j is component j % 2 of pair j / 2 (17 pairs: an odd count
+// reads one zero partner past its end).
+enum CellField { kHx = 0, kHy, kHz, kMass, kLx, kLy, kLz, kQxx, kQxy, kQxz, kQyy, kQyz, kQzz,
+                 kCellFields };
+enum LeafField { kSx = 0, kSy, kSz, kSm, kLeafFields };
+
+struct __align__(16) WarpSpace {
+    GroupItem stack[kStackCap];
+    GroupItem mixed[32];    // this round's mixed items
+    uint2 cells[kCellCap];  // (node, target mask)
+    uint2 leaves[kLeafCap]; // (node, target mask)
+    float2 cell_pairs[kCellFields][17];
+    uint2 mask_pairs[17];
+    float2 leaf_pairs[kLeafFields][17];
+    float4 union_staged[32]; // the union walk's leaf staging
+};
+
+// Writes entry j of a pair array (component j % 2 of pair j / 2).
+__device__ __forceinline__ void put(float2 *pairs, uint32_t j, float v) {
+    if (j & 1u) {
+        pairs[j >> 1].y = v;
+    } else {
+        pairs[j >> 1].x = v;
+    }
 }
+__device__ __forceinline__ void put(uint2 *pairs, uint32_t j, uint32_t v) {
+    if (j & 1u) {
+        pairs[j >> 1].y = v;
+    } else {
+        pairs[j >> 1].x = v;
+    }
+}
+
+__device__ __forceinline__ uint32_t warp_min(uint32_t v) { return __reduce_min_sync(kFull, v); }
+
+__device__ __forceinline__ uint32_t lanes_below(uint32_t lane) { return (1u << lane) - 1u; }
 
 // The reference's accept test in FP64 (tree_walk.cpp:44-46), for cells whose
 // FP32 test fell inside the margin.
-__device__ __noinline__ bool exact_accept(const DeviceNode *nodes, uint32_t cur,
+__device__ __forceinline__ bool exact_accept(const DeviceNode *nodes, uint32_t cur,
                                           const double *sorted, uint32_t n, uint32_t i) {
     const double px = sorted[i];
     const double py = sorted[static_cast<size_t>(n) + i];
@@ -51,38 +124,42 @@ __device__ __noinline__ bool exact_accept(const DeviceNode *nodes, uint32_t cur,
     return d2 >= nodes[cur].r2;
 }
 
-template <bool QUAD>
-__global__ void __launch_bounds__(kWalkThreads)
-    walk_kernel(const DeviceNode *__restrict__ nodes, const WalkNode *__restrict__ walk,
-                const uint32_t *__restrict__ first_of, const float4 *__restrict__ leaf_rel,
-                const double *__restrict__ sorted, const uint32_t *__restrict__ perm, uint32_t n,
-                float eps2, double *ax, double *ay, double *az, const TreeMeta *meta,
-                unsigned long long *counters) {
-    __shared__ float4 staged[kWalkWarps][32];
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = threadIdx.x >> 5;
-    const uint32_t i = (blockIdx.x * kWalkWarps + warp) * 32u + lane;
-    const bool active = i < n;
-    const uint32_t node_count = meta->node_count;
-
-    float pxh = 0.0f, pyh = 0.0f, pzh = 0.0f, pxl = 0.0f, pyl = 0.0f, pzl = 0.0f;
-    if (active) {
-        const double X = sorted[i];
-        const double Y = sorted[static_cast<size_t>(n) + i];
-        const double Z = sorted[2ull * n + i];
-        pxh = __double2float_rn(X);
-        pyh = __double2float_rn(Y);
-        pzh = __double2float_rn(Z);
-        pxl = __double2float_rn(X - static_cast<double>(pxh));
-        pyl = __double2float_rn(Y - static_cast<double>(pyh));
-        pzl = __double2float_rn(Z - static_cast<double>(pzh));
+// One target's FP32 accept test of a walk record, with the FP64 fallback
+// inside the margin. Also returns the FP32 offset d = com - target.
+__device__ __forceinline__ bool lane_accepts(const float4 A, const float4 B, float pxh, float pyh,
+                                             float pzh, float pxl, float pyl, float pzl,
+                                             const DeviceNode *nodes, uint32_t cur,
+                                             const double *sorted, uint32_t n, uint32_t i,
+                                             float &dx, float &dy, float &dz) {
+    dx = (A.x - pxh) + (B.x - pxl);
+    dy = (A.y - pyh) + (B.y - pyl);
+    dz = (A.z - pzh) + (B.z - pzl);
+    const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+    const float r2 = B.w;
+    if (d2 >= r2 * (1.0f + kAcceptMargin) && r2 > 1e-30f) {
+        return true;
     }
+    if (d2 <= r2 * (1.0f - kAcceptMargin)) {
+        return false;
+    }
+    return exact_accept(nodes, cur, sorted, n, i);
+}
 
-    double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0; // FP64 sums
-    float cx32 = 0.0f, cy32 = 0.0f, cz32 = 0.0f;   // FP32 cell terms since the last flush
-    uint32_t pairs = 0, cells = 0;
+// The per-target union walk: the warp visits the smallest cursor any lane
+// holds and only lanes whose cursor is that node act on it. Used when the
+// group traversal's stack would overflow. Sums go to acc (FP64, including all
+// FP32 partials), counts to pairs / cells.
+template <bool QUAD>
+__device__ void union_walk(const DeviceNode *__restrict__ nodes,
+                           const WalkNode *__restrict__ walk, const uint32_t *__restrict__ first_of,
+                           const float4 *__restrict__ leaf_rel, const double *__restrict__ sorted,
+                           uint32_t n, uint32_t node_count, float eps2, uint32_t i, bool active,
+                           float pxh, float pyh, float pzh, float pxl, float pyl, float pzl,
+                           float4 *staged, double &acc_x, double &acc_y, double &acc_z,
+                           uint32_t &pairs, uint32_t &cells) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float cx32 = 0.0f, cy32 = 0.0f, cz32 = 0.0f;
     uint32_t cursor = active ? 0u : 0xffffffffu;
-
     while (true) {
         const uint32_t cur = warp_min(cursor);
         if (cur >= node_count) {
@@ -96,27 +173,16 @@ __global__ void __launch_bounds__(kWalkThreads)
         bool open_leaf = false;
         float dx = 0.0f, dy = 0.0f, dz = 0.0f;
         if (cursor == cur) {
-            dx = (A.x - pxh) + (B.x - pxl);
-            dy = (A.y - pyh) + (B.y - pyl);
-            dz = (A.z - pzh) + (B.z - pzl);
-            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            const float r2 = B.w;
-            bool accept;
-            if (d2 >= r2 * (1.0f + kAcceptMargin) && r2 > 1e-30f) {
-                accept = true;
-            } else if (d2 <= r2 * (1.0f - kAcceptMargin)) {
-                accept = false;
-            } else {
-                accept = exact_accept(nodes, cur, sorted, n, i);
-            }
+            const bool accept = lane_accepts(A, B, pxh, pyh, pzh, pxl, pyl, pzl, nodes, cur,
+                                             sorted, n, i, dx, dy, dz);
             if (accept) {
-                const float r2e = d2 + eps2;
+                const float r2e = fmaf(dz, dz, fmaf(dy, dy, dx * dx)) + eps2;
                 const float inv = rsqrt_approx(r2e);
                 const float inv2 = inv * inv;
                 const float f = (A.w * inv) * inv2;
                 float gx = dx * f, gy = dy * f, gz = dz * f;
                 if (QUAD) {
-                    const float4 C = walk[cur].c; // (xx, xy, xz, yy); D.xy = (yz, zz)
+                    const float4 C = walk[cur].c;
                     const float qx = fmaf(C.x, dx, fmaf(C.y, dy, C.z * dz));
                     const float qy = fmaf(C.y, dx, fmaf(C.w, dy, D.x * dz));
                     const float qz = fmaf(C.z, dx, fmaf(D.x, dy, D.y * dz));
@@ -139,50 +205,32 @@ __global__ void __launch_bounds__(kWalkThreads)
                 cursor = cur + 1;
             }
         }
-        if (__any_sync(0xffffffffu, open_leaf)) {
+        if (__any_sync(kFull, open_leaf)) {
             const uint32_t first = first_of[cur];
-            // Target relative to the leaf's centre of mass: -d.
-            const float tx = -dx, ty = -dy, tz = -dz;
             const bool own = open_leaf && i >= first && i < first + count;
-            const bool masked = __any_sync(0xffffffffu, own);
+            const bool masked = __any_sync(kFull, own);
             float sx = 0.0f, sy = 0.0f, sz = 0.0f;
             for (uint32_t base = 0; base < count; base += 32) {
                 if (base + lane < count) {
-                    staged[warp][lane] = leaf_rel[first + base + lane];
+                    staged[lane] = leaf_rel[first + base + lane];
                 }
                 __syncwarp();
                 if (open_leaf) {
                     const uint32_t chunk = min(32u, count - base);
-                    if (!masked) {
-#pragma unroll 4
-                        for (uint32_t j = 0; j < chunk; ++j) {
-                            const float4 s = staged[warp][j];
-                            const float ex = s.x - tx;
-                            const float ey = s.y - ty;
-                            const float ez = s.z - tz;
-                            const float r2 = fmaf(ez, ez, fmaf(ey, ey, fmaf(ex, ex, eps2)));
-                            const float inv = rsqrt_approx(r2);
-                            const float f = (s.w * inv) * (inv * inv);
-                            sx = fmaf(f, ex, sx);
-                            sy = fmaf(f, ey, sy);
-                            sz = fmaf(f, ez, sz);
-                        }
-                    } else {
-                        for (uint32_t j = 0; j < chunk; ++j) {
-                            const float4 s = staged[warp][j];
-                            const bool self = first + base + j == i;
-                            const float ex = s.x - tx;
-                            const float ey = s.y - ty;
-                            const float ez = s.z - tz;
-                            const float r2 =
-                                self ? 1.0f : fmaf(ez, ez, fmaf(ey, ey, fmaf(ex, ex, eps2)));
-                            const float w = self ? 0.0f : s.w;
-                            const float inv = rsqrt_approx(r2);
-                            const float f = (w * inv) * (inv * inv);
-                            sx = fmaf(f, ex, sx);
-                            sy = fmaf(f, ey, sy);
-                            sz = fmaf(f, ez, sz);
-                        }
+                    for (uint32_t j = 0; j < chunk; ++j) {
+                        const float4 s = staged[j];
+                        const bool self = masked && first + base + j == i;
+                        const float ex = s.x + dx;
+                        const float ey = s.y + dy;
+                        const float ez = s.z + dz;
+                        const float r2 =
+                            self ? 1.0f : fmaf(ez, ez, fmaf(ey, ey, fmaf(ex, ex, eps2)));
+                        const float w = self ? 0.0f : s.w;
+                        const float inv = rsqrt_approx(r2);
+                        const float f = (w * inv) * (inv * inv);
+                        sx = fmaf(f, ex, sx);
+                        sy = fmaf(f, ey, sy);
+                        sz = fmaf(f, ez, sz);
                     }
                 }
                 __syncwarp();
@@ -196,17 +244,417 @@ __global__ void __launch_bounds__(kWalkThreads)
             }
         }
     }
+    acc_x += static_cast<double>(cx32);
+    acc_y += static_cast<double>(cy32);
+    acc_z += static_cast<double>(cz32);
+}
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+// Evaluates the warp's cell list: every lane sums every cell for its target
+// (zero outside the cell's mask), two cells per FP32x2 instruction.
+template <bool QUAD>
+__device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
+                                            const WalkNode *__restrict__ walk, float2 nhx,
+                                            float2 nhy, float2 nhz, float2 nlx, float2 nly,
+                                            float2 nlz, float2 eps2, uint32_t lane_bit,
+                                            double &acc_x, double &acc_y, double &acc_z,
+                                            uint32_t &cells, uint32_t node_count,
+                                            unsigned *status) {
+    const uint32_t lane = threadIdx.x & 31u;
+    float2 gx = f2(0.0f, 0.0f), gy = gx, gz = gx;
+    for (uint32_t base = 0; base < count; base += 32) {
+        const uint32_t chunk = min(32u, count - base);
+        float2(*cp)[17] = ws.cell_pairs;
+        if (lane < chunk) {
+            uint2 e = ws.cells[base + lane];
+            if (e.x >= node_count) {
+                atomicOr(status, kStatusInvalid);
+                e = make_uint2(0u, 0u); // no target: contributes nothing
+            }
+            const WalkNode *w = walk + e.x;
+            const float4 A = w->a;
+            const float4 B = w->b;
+            put(cp[kHx], lane, A.x);
+            put(cp[kHy], lane, A.y);
+            put(cp[kHz], lane, A.z);
+            put(cp[kMass], lane, A.w);
+            put(cp[kLx], lane, B.x);
+            put(cp[kLy], lane, B.y);
+            put(cp[kLz], lane, B.z);
+            put(ws.mask_pairs, lane, e.y);
+            if (QUAD) {
+                const float4 C = w->c;
+                const float4 D = w->d;
+                put(cp[kQxx], lane, C.x);
+                put(cp[kQxy], lane, C.y);
+                put(cp[kQxz], lane, C.z);
+                put(cp[kQyy], lane, C.w);
+                put(cp[kQyz], lane, D.x);
+                put(cp[kQzz], lane, D.y);
+            }
+        } else if (lane == chunk) {
+            // The odd entry's partner: no target, zero mass, at the origin.
+            for (int k = 0; k < kCellFields; ++k) {
+                put(cp[k], lane, 0.0f);
+            }
+            put(ws.mask_pairs, lane, 0u);
+        }
+        __syncwarp();
+        for (uint32_t j = 0; j < chunk; j += 2) {
+            const uint32_t p = j >> 1;
+            const float2 dx = __fadd2_rn(__fadd2_rn(cp[kHx][p], nhx), __fadd2_rn(cp[kLx][p], nlx));
+            const float2 dy = __fadd2_rn(__fadd2_rn(cp[kHy][p], nhy), __fadd2_rn(cp[kLy][p], nly));
+            const float2 dz = __fadd2_rn(__fadd2_rn(cp[kHz][p], nhz), __fadd2_rn(cp[kLz][p], nlz));
+            const uint2 mk = ws.mask_pairs[p];
+            const bool in0 = (mk.x & lane_bit) != 0u;
+            const bool in1 = (mk.y & lane_bit) != 0u;
+            cells += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
+            const float2 r2e =
+                __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
+            const float inv0 = rsqrt_approx(r2e.x);
+            const float inv1 = rsqrt_approx(r2e.y);
+            const float2 inv = f2(in0 ? inv0 : 0.0f, in1 ? inv1 : 0.0f);
+            const float2 inv2 = __fmul2_rn(inv, inv);
+            const float2 f = __fmul2_rn(__fmul2_rn(cp[kMass][p], inv), inv2);
+            float2 tx = __fmul2_rn(dx, f), ty = __fmul2_rn(dy, f), tz = __fmul2_rn(dz, f);
+            if (QUAD) {
+                const float2 xx = cp[kQxx][p], xy = cp[kQxy][p];
+                const float2 xz = cp[kQxz][p], yy = cp[kQyy][p];
+                const float2 yz = cp[kQyz][p], zz = cp[kQzz][p];
+                const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
+                const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
+                const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
+                const float2 quadratic =
+                    __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
+                const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
+                const float2 s = __fmul2_rn(__fmul2_rn(f2(2.5f, 2.5f), quadratic),
+                                            __fmul2_rn(inv5, inv2));
+                const float2 ninv5 = f2(-inv5.x, -inv5.y);
+                tx = __ffma2_rn(qx, ninv5, __ffma2_rn(dx, s, tx));
+                ty = __ffma2_rn(qy, ninv5, __ffma2_rn(dy, s, ty));
+                tz = __ffma2_rn(qz, ninv5, __ffma2_rn(dz, s, tz));
+            }
+            gx = __fadd2_rn(gx, tx);
+            gy = __fadd2_rn(gy, ty);
+            gz = __fadd2_rn(gz, tz);
+        }
+        __syncwarp();
+    }
+    acc_x += static_cast<double>(gx.x) + static_cast<double>(gx.y);
+    acc_y += static_cast<double>(gy.x) + static_cast<double>(gy.y);
+    acc_z += static_cast<double>(gz.x) + static_cast<double>(gz.y);
+}
+
+// Evaluates the warp's leaf list: for each opened leaf, the lanes in its mask
+// sum its particles (staged in shared memory once per chunk of 32), two
+// sources per FP32x2 instruction, skipping the target itself.
+__device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
+                                             const WalkNode *__restrict__ walk,
+                                             const uint32_t *__restrict__ first_of,
+                                             const float4 *__restrict__ leaf_rel, float pxh,
+                                             float pyh, float pzh, float pxl, float pyl,
+                                             float pzl, float eps2, uint32_t i,
+                                             uint32_t lane_bit, double &acc_x, double &acc_y,
+                                             double &acc_z, uint32_t &pairs, uint32_t node_count,
+                                             uint32_t n, unsigned *status) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const float2 e2 = f2(eps2, eps2);
+    for (uint32_t k = 0; k < count; ++k) {
+        const uint2 e = ws.leaves[k];
+        if (e.x >= node_count) {
+            if (lane == 0) {
+                atomicOr(status, kStatusInvalid);
+            }
+            continue; // uniform: every lane reads the same entry
+        }
+        const WalkNode *w = walk + e.x;
+        const float4 A = w->a;
+        const float4 B = w->b;
+        const uint32_t size = __float_as_uint(w->d.w);
+        const uint32_t first = first_of[e.x];
+        if (first > n || size > n - first) {
+            if (lane == 0) {
+                atomicOr(status, kStatusInvalid);
+            }
+            continue;
+        }
+        const bool in = (e.y & lane_bit) != 0u;
+        const bool own = in && i >= first && i < first + size;
+        const bool masked = __any_sync(kFull, own);
+        // Offset leaf centre of mass - target; source - target = source + d.
+        const float dx = (A.x - pxh) + (B.x - pxl);
+        const float dy = (A.y - pyh) + (B.y - pyl);
+        const float dz = (A.z - pzh) + (B.z - pzl);
+        const float2 dx2 = f2(dx, dx), dy2 = f2(dy, dy), dz2 = f2(dz, dz);
+        float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
+        for (uint32_t base = 0; base < size; base += 32) {
+            const uint32_t chunk = min(32u, size - base);
+            float2(*lp)[17] = ws.leaf_pairs;
+            if (lane < chunk) {
+                const float4 src = leaf_rel[first + base + lane];
+                put(lp[kSx], lane, src.x);
+                put(lp[kSy], lane, src.y);
+                put(lp[kSz], lane, src.z);
+                put(lp[kSm], lane, src.w);
+            } else if (lane == chunk) {
+                for (int q = 0; q < kLeafFields; ++q) {
+                    put(lp[q], lane, 0.0f);
+                }
+            }
+            __syncwarp();
+            for (uint32_t j = 0; j < chunk; j += 2) {
+                const uint32_t p = j >> 1;
+                const float2 ex = __fadd2_rn(lp[kSx][p], dx2);
+                const float2 ey = __fadd2_rn(lp[kSy][p], dy2);
+                const float2 ez = __fadd2_rn(lp[kSz][p], dz2);
+                float2 r2 = __ffma2_rn(ez, ez, __ffma2_rn(ey, ey, __ffma2_rn(ex, ex, e2)));
+                float2 m = lp[kSm][p];
+                // The target itself, the zero partner of an odd count and
+                // lanes outside the mask contribute nothing.
+                const uint32_t index = first + base + j;
+                const bool skip0 = !in || (masked && index == i);
+                const bool skip1 = !in || j + 1 >= chunk || (masked && index + 1 == i);
+                r2 = f2(skip0 ? 1.0f : r2.x, skip1 ? 1.0f : r2.y);
+                m = f2(skip0 ? 0.0f : m.x, skip1 ? 0.0f : m.y);
+                const float2 inv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                const float2 f = __fmul2_rn(__fmul2_rn(m, inv), __fmul2_rn(inv, inv));
+                sx = __ffma2_rn(f, ex, sx);
+                sy = __ffma2_rn(f, ey, sy);
+                sz = __ffma2_rn(f, ez, sz);
+            }
+            __syncwarp();
+        }
+        if (in) {
+            acc_x += static_cast<double>(sx.x) + static_cast<double>(sx.y);
+            acc_y += static_cast<double>(sy.x) + static_cast<double>(sy.y);
+            acc_z += static_cast<double>(sz.x) + static_cast<double>(sz.y);
+            pairs += size - (own ? 1u : 0u);
+        }
+    }
+}
+
+template <bool QUAD>
+__global__ void __launch_bounds__(kWalkThreads)
+    walk_kernel(const DeviceNode *__restrict__ nodes, const WalkNode *__restrict__ walk,
+                const uint32_t *__restrict__ first_of, const float4 *__restrict__ leaf_rel,
+                const double *__restrict__ sorted, const uint32_t *__restrict__ perm, uint32_t n,
+                float eps2, double *ax, double *ay, double *az, const TreeMeta *meta,
+                unsigned long long *counters, unsigned *status) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = threadIdx.x >> 5;
+    WarpSpace &ws = reinterpret_cast<WarpSpace *>(smem)[warp];
+    const uint32_t i = (blockIdx.x * kWalkWarps + warp) * 32u + lane;
+    const bool active = i < n;
+    const uint32_t live = __ballot_sync(kFull, active);
+    if (live == 0u) {
+        return; // the whole warp lies past the last target
+    }
+    const uint32_t node_count = meta->node_count;
+    const uint32_t lane_bit = 1u << lane;
+
+    double X = 0.0, Y = 0.0, Z = 0.0;
+    float pxh = 0.0f, pyh = 0.0f, pzh = 0.0f, pxl = 0.0f, pyl = 0.0f, pzl = 0.0f;
+    if (active) {
+        X = sorted[i];
+        Y = sorted[static_cast<size_t>(n) + i];
+        Z = sorted[2ull * n + i];
+        pxh = __double2float_rn(X);
+        pyh = __double2float_rn(Y);
+        pzh = __double2float_rn(Z);
+        pxl = __double2float_rn(X - static_cast<double>(pxh));
+        pyl = __double2float_rn(Y - static_cast<double>(pyh));
+        pzl = __double2float_rn(Z - static_cast<double>(pzh));
+    }
+    const float2 nhx = f2(-pxh, -pxh), nhy = f2(-pyh, -pyh), nhz = f2(-pzh, -pzh);
+    const float2 nlx = f2(-pxl, -pxl), nly = f2(-pyl, -pyl), nlz = f2(-pzl, -pzl);
+    const float2 eps2v = f2(eps2, eps2);
+
+    // FP64 bounding box of the warp's targets.
+    const double inf = __longlong_as_double(0x7ff0000000000000ll);
+    double lox = active ? X : inf, loy = active ? Y : inf, loz = active ? Z : inf;
+    double hix = active ? X : -inf, hiy = active ? Y : -inf, hiz = active ? Z : -inf;
+    for (int off = 16; off > 0; off >>= 1) {
+        lox = fmin(lox, __shfl_xor_sync(kFull, lox, off));
+        loy = fmin(loy, __shfl_xor_sync(kFull, loy, off));
+        loz = fmin(loz, __shfl_xor_sync(kFull, loz, off));
+        hix = fmax(hix, __shfl_xor_sync(kFull, hix, off));
+        hiy = fmax(hiy, __shfl_xor_sync(kFull, hiy, off));
+        hiz = fmax(hiz, __shfl_xor_sync(kFull, hiz, off));
+    }
+
+    double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
+    uint32_t pairs = 0, cells = 0;
+    uint32_t size = 1, ncell = 0, nleaf = 0;
+    bool overflow = false;
+    uint32_t rounds = 0;
+    if (lane == 0) {
+        ws.stack[0] = GroupItem{0u, live, node_count};
+    }
+    __syncwarp();
+    while (size > 0) {
+        const uint32_t take = min(size, 32u);
+        // A valid tree visits each node at most once, so more rounds than
+        // nodes (or a full stack) hands the warp to the union walk, whose
+        // cursors only move forward.
+        if (size - take + 64u > kStackCap || ++rounds > node_count + 1u) {
+            overflow = true;
+            break;
+        }
+        size -= take;
+        const bool has = lane < take;
+        GroupItem item{0u, 0u, 0u};
+        if (has) {
+            item = ws.stack[size + lane];
+            if (item.node >= node_count) {
+                atomicOr(status, kStatusInvalid);
+                item.node = node_count; // skipped below
+            }
+        }
+        __syncwarp();
+
+        // Classify the lane's node against the box (FP64, the reference's
+        // operations and order).
+        bool sibling = false, child = false, cell = false, leaf = false, mixed = false;
+        uint32_t next = 0;
+        if (has && item.node < node_count) {
+            const DeviceNode *nd = nodes + item.node;
+            const double cx = nd->com_x, cy = nd->com_y, cz = nd->com_z, r2 = nd->r2;
+            next = nd->next;
+            const uint32_t count = nd->count;
+            sibling = next < item.end;
+            const double nx = fmax(fmax(__dsub_rn(lox, cx), __dsub_rn(cx, hix)), 0.0);
+            const double ny = fmax(fmax(__dsub_rn(loy, cy), __dsub_rn(cy, hiy)), 0.0);
+            const double nz = fmax(fmax(__dsub_rn(loz, cz), __dsub_rn(cz, hiz)), 0.0);
+            const double near2 =
+                __dadd_rn(__dadd_rn(__dmul_rn(nx, nx), __dmul_rn(ny, ny)), __dmul_rn(nz, nz));
+            const double fx = fmax(fabs(__dsub_rn(cx, lox)), fabs(__dsub_rn(cx, hix)));
+            const double fy = fmax(fabs(__dsub_rn(cy, loy)), fabs(__dsub_rn(cy, hiy)));
+            const double fz = fmax(fabs(__dsub_rn(cz, loz)), fabs(__dsub_rn(cz, hiz)));
+            const double far2 =
+                __dadd_rn(__dadd_rn(__dmul_rn(fx, fx), __dmul_rn(fy, fy)), __dmul_rn(fz, fz));
+            if (near2 >= r2) {
+                cell = true;
+            } else if (far2 < r2) {
+                leaf = count > 0;
+                child = count == 0;
+            } else {
+                mixed = true;
+            }
+        }
+        const uint32_t below = lanes_below(lane);
+        const uint32_t bs = __ballot_sync(kFull, sibling);
+        const uint32_t bc = __ballot_sync(kFull, child);
+        if (sibling) {
+            ws.stack[size + __popc(bs & below)] = GroupItem{next, item.mask, item.end};
+        }
+        if (child) {
+            ws.stack[size + __popc(bs) + __popc(bc & below)] =
+                GroupItem{item.node + 1u, item.mask, next};
+        }
+        size += __popc(bs) + __popc(bc);
+        const uint32_t ba = __ballot_sync(kFull, cell);
+        if (cell) {
+            ws.cells[ncell + __popc(ba & below)] = make_uint2(item.node, item.mask);
+        }
+        ncell += __popc(ba);
+        const uint32_t bl = __ballot_sync(kFull, leaf);
+        if (leaf) {
+            ws.leaves[nleaf + __popc(bl & below)] = make_uint2(item.node, item.mask);
+        }
+        nleaf += __popc(bl);
+
+        // Mixed nodes: each target in the mask decides for itself.
+        const uint32_t bm = __ballot_sync(kFull, mixed);
+        if (mixed) {
+            ws.mixed[__popc(bm & below)] = item;
+        }
+        __syncwarp();
+        const uint32_t nmixed = __popc(bm);
+        for (uint32_t k = 0; k < nmixed; ++k) {
+            const GroupItem mi = ws.mixed[k];
+            const uint32_t v = mi.node;
+            const uint32_t mask = mi.mask;
+            const float4 A = walk[v].a;
+            const float4 B = walk[v].b;
+            const float4 D = walk[v].d;
+            // FP32 test on every lane; the FP64 test, when any lane of the
+            // mask falls inside the margin, on every lane too.
+            const bool reach = (mask & lane_bit) != 0u;
+            const float dx = (A.x - pxh) + (B.x - pxl);
+            const float dy = (A.y - pyh) + (B.y - pyl);
+            const float dz = (A.z - pzh) + (B.z - pzl);
+            const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
+            const float r2 = B.w;
+            const bool sure_accept = d2 >= r2 * (1.0f + kAcceptMargin) && r2 > 1e-30f;
+            const bool sure_open = d2 <= r2 * (1.0f - kAcceptMargin);
+            bool accept = reach && sure_accept;
+            const bool unsure = reach && !sure_accept && !sure_open;
+            if (__any_sync(kFull, unsure)) {
+                const bool exact = exact_accept(nodes, v, sorted, n, active ? i : 0u);
+                accept = accept || (unsure && exact);
+            }
+            const uint32_t accepted = __ballot_sync(kFull, accept) & mask;
+            const uint32_t opened = mask & ~accepted;
+            const uint32_t vnext = __float_as_uint(D.z);
+            const uint32_t vcount = __float_as_uint(D.w);
+            if (lane == 0) {
+                if (accepted != 0u) {
+                    ws.cells[ncell] = make_uint2(v, accepted);
+                }
+                if (opened != 0u) {
+                    if (vcount > 0u) {
+                        ws.leaves[nleaf] = make_uint2(v, opened);
+                    } else {
+                        ws.stack[size] = GroupItem{v + 1u, opened, vnext};
+                    }
+                }
+            }
+            ncell += accepted != 0u ? 1u : 0u;
+            if (opened != 0u) {
+                if (vcount > 0u) {
+                    ++nleaf;
+                } else {
+                    ++size;
+                }
+            }
+        }
+        __syncwarp();
+        if (ncell > kCellCap - 64u) {
+            flush_cells<QUAD>(ws, ncell, walk, nhx, nhy, nhz, nlx, nly, nlz, eps2v, lane_bit,
+                              acc_x, acc_y, acc_z, cells, node_count, status);
+            ncell = 0;
+        }
+        if (nleaf > kLeafCap - 64u) {
+            flush_leaves(ws, nleaf, walk, first_of, leaf_rel, pxh, pyh, pzh, pxl, pyl, pzl, eps2,
+                         i, lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
+            nleaf = 0;
+        }
+    }
+    if (overflow) {
+        acc_x = acc_y = acc_z = 0.0;
+        pairs = cells = 0;
+        union_walk<QUAD>(nodes, walk, first_of, leaf_rel, sorted, n, node_count, eps2, i, active,
+                         pxh, pyh, pzh, pxl, pyl, pzl, ws.union_staged, acc_x, acc_y, acc_z, pairs,
+                         cells);
+    } else {
+        flush_cells<QUAD>(ws, ncell, walk, nhx, nhy, nhz, nlx, nly, nlz, eps2v, lane_bit, acc_x,
+                          acc_y, acc_z, cells, node_count, status);
+        flush_leaves(ws, nleaf, walk, first_of, leaf_rel, pxh, pyh, pzh, pxl, pyl, pzl, eps2, i,
+                     lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
+    }
 
     if (active) {
         const uint32_t j = perm[i];
-        ax[j] = acc_x + static_cast<double>(cx32);
-        ay[j] = acc_y + static_cast<double>(cy32);
-        az[j] = acc_z + static_cast<double>(cz32);
+        ax[j] = acc_x;
+        ay[j] = acc_y;
+        az[j] = acc_z;
     }
-    unsigned long long p = pairs, c = cells;
+    unsigned long long p = active ? pairs : 0u, c = active ? cells : 0u;
     for (int off = 16; off > 0; off >>= 1) {
-        p += __shfl_down_sync(0xffffffffu, p, off);
-        c += __shfl_down_sync(0xffffffffu, c, off);
+        p += __shfl_down_sync(kFull, p, off);
+        c += __shfl_down_sync(kFull, c, off);
     }
     if (lane == 0 && (p | c) != 0ull) {
         atomicAdd(&counters[0], p);
@@ -220,20 +668,21 @@ cudaError_t launch_walk(const DeviceNode *nodes, const WalkNode *walk_nodes,
                         const uint32_t *first_of, const float4 *leaf_rel, const double *sorted,
                         const uint32_t *perm, uint32_t n, double eps2, bool quadrupole,
                         double *ax, double *ay, double *az, TreeMeta *meta,
-                        unsigned long long *counters, cudaStream_t stream) {
+                        unsigned long long *counters, unsigned *status, cudaStream_t stream) {
     if (n == 0) {
         return cudaSuccess;
     }
-    const uint32_t blocks = ceil_div(n, kWalkThreads);
+    const uint32_t blocks = ceil_div(n, static_cast<uint32_t>(kWalkThreads));
     const float eps2f = static_cast<float>(eps2);
+    const size_t smem = kWalkWarps * sizeof(WarpSpace);
     if (quadrupole) {
-        walk_kernel<true><<<blocks, kWalkThreads, 0, stream>>>(
+        walk_kernel<true><<<blocks, kWalkThreads, smem, stream>>>(
             nodes, walk_nodes, first_of, leaf_rel, sorted, perm, n, eps2f, ax, ay, az, meta,
-            counters);
+            counters, status);
     } else {
-        walk_kernel<false><<<blocks, kWalkThreads, 0, stream>>>(
+        walk_kernel<false><<<blocks, kWalkThreads, smem, stream>>>(
             nodes, walk_nodes, first_of, leaf_rel, sorted, perm, n, eps2f, ax, ay, az, meta,
-            counters);
+            counters, status);
     }
     return cudaGetLastError();
 }
