@@ -58,12 +58,15 @@ constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr float kAcceptMargin = 4e-6f;
 constexpr uint32_t kFull = 0xffffffffu;
 
-// Per-warp shared-memory capacities (entries). A round adds at most 64 stack
-// items (32 siblings, 32 first children), 64 cells (32 accepted by all, 32
-// accepted by some of a mixed node) and 64 leaves.
-constexpr uint32_t kStackCap = 256;
-constexpr uint32_t kCellCap = 128;
-constexpr uint32_t kLeafCap = 96;
+// Per-warp shared-memory capacities (entries). A round processes at most 32
+// items; each adds at most two stack items (its next sibling and, opened, its
+// first child) and at most one cell or one leaf, so a round of t items adds at
+// most 2t stack items, t cells and t leaves. A round takes at most
+// kStackCap - size items, so the stack cannot overflow while it has room.
+// Sized so that 8 CTAs of 4 warps fit in an SM's shared memory.
+constexpr uint32_t kStackCap = 160;
+constexpr uint32_t kCellCap = 96;
+constexpr uint32_t kLeafCap = 64;
 
 struct GroupItem {
     uint32_t node;
@@ -71,37 +74,41 @@ struct GroupItem {
     uint32_t end;  // end of the parent's subtree: the next sibling exists below it
 };
 
-// Cell fields staged for a batch of 32 cells, structure of arrays of packed
-// pairs: entry j is component j % 2 of pair j / 2 (17 pairs: an odd count
-// reads one zero partner past its end).
-enum CellField { kHx = 0, kHy, kHz, kMass, kLx, kLy, kLz, kQxx, kQxy, kQxz, kQyy, kQyz, kQzz,
-                 kCellFields };
-enum LeafField { kSx = 0, kSy, kSz, kSm, kLeafFields };
+// Entries staged for a batch of 32 cells (or one leaf chunk), as float4
+// quads of packed pairs: quad f of pair p holds (a_j, a_j+1, b_j, b_j+1) for
+// the two fields a, b of group f and the entries j = 2p, 2p+1, so one 16-byte
+// shared load yields two FP32x2 operands. 17 pairs: an odd count reads one
+// neutral partner past its end.
+//   cells:  (hi x, hi y) (hi z, mass) (lo x, lo y) (lo z, target mask bits)
+//           (Qxx, Qxy) (Qxz, Qyy) (Qyz, Qzz)
+//   leaves: (x, y) (z, mass), leaf-relative
+constexpr int kCellQuads = 7;
+constexpr int kLeafQuads = 2;
+// Offset given to lanes outside a leaf's mask and to the neutral partner: the
+// terms it produces underflow to exactly zero in FP32.
+constexpr float kFar = 1e18f;
 
 struct __align__(16) WarpSpace {
     GroupItem stack[kStackCap];
     GroupItem mixed[32];    // this round's mixed items
     uint2 cells[kCellCap];  // (node, target mask)
     uint2 leaves[kLeafCap]; // (node, target mask)
-    float2 cell_pairs[kCellFields][17];
-    uint2 mask_pairs[17];
-    float2 leaf_pairs[kLeafFields][17];
-    float4 union_staged[32]; // the union walk's leaf staging
+    union {
+        float4 cell_quads[kCellQuads][17];
+        float4 union_staged[32]; // the union walk's leaf staging (after a fallback)
+    };
+    float4 leaf_quads[kLeafQuads][17];
 };
 
-// Writes entry j of a pair array (component j % 2 of pair j / 2).
-__device__ __forceinline__ void put(float2 *pairs, uint32_t j, float v) {
+// Writes entry j's two fields a, b into quad array q (see cell_quads).
+__device__ __forceinline__ void put(float4 *q, uint32_t j, float a, float b) {
+    float4 &slot = q[j >> 1];
     if (j & 1u) {
-        pairs[j >> 1].y = v;
+        slot.y = a;
+        slot.w = b;
     } else {
-        pairs[j >> 1].x = v;
-    }
-}
-__device__ __forceinline__ void put(uint2 *pairs, uint32_t j, uint32_t v) {
-    if (j & 1u) {
-        pairs[j >> 1].y = v;
-    } else {
-        pairs[j >> 1].x = v;
+        slot.x = a;
+        slot.z = b;
     }
 }
 
@@ -265,7 +272,7 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
     float2 gx = f2(0.0f, 0.0f), gy = gx, gz = gx;
     for (uint32_t base = 0; base < count; base += 32) {
         const uint32_t chunk = min(32u, count - base);
-        float2(*cp)[17] = ws.cell_pairs;
+        float4(*cq)[17] = ws.cell_quads;
         if (lane < chunk) {
             uint2 e = ws.cells[base + lane];
             if (e.x >= node_count) {
@@ -275,40 +282,32 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
             const WalkNode *w = walk + e.x;
             const float4 A = w->a;
             const float4 B = w->b;
-            put(cp[kHx], lane, A.x);
-            put(cp[kHy], lane, A.y);
-            put(cp[kHz], lane, A.z);
-            put(cp[kMass], lane, A.w);
-            put(cp[kLx], lane, B.x);
-            put(cp[kLy], lane, B.y);
-            put(cp[kLz], lane, B.z);
-            put(ws.mask_pairs, lane, e.y);
+            put(cq[0], lane, A.x, A.y);
+            put(cq[1], lane, A.z, A.w);
+            put(cq[2], lane, B.x, B.y);
+            put(cq[3], lane, B.z, __uint_as_float(e.y));
             if (QUAD) {
                 const float4 C = w->c;
                 const float4 D = w->d;
-                put(cp[kQxx], lane, C.x);
-                put(cp[kQxy], lane, C.y);
-                put(cp[kQxz], lane, C.z);
-                put(cp[kQyy], lane, C.w);
-                put(cp[kQyz], lane, D.x);
-                put(cp[kQzz], lane, D.y);
+                put(cq[4], lane, C.x, C.y);
+                put(cq[5], lane, C.z, C.w);
+                put(cq[6], lane, D.x, D.y);
             }
         } else if (lane == chunk) {
             // The odd entry's partner: no target, zero mass, at the origin.
-            for (int k = 0; k < kCellFields; ++k) {
-                put(cp[k], lane, 0.0f);
+            for (int q = 0; q < kCellQuads; ++q) {
+                put(cq[q], lane, 0.0f, 0.0f);
             }
-            put(ws.mask_pairs, lane, 0u);
         }
         __syncwarp();
         for (uint32_t j = 0; j < chunk; j += 2) {
             const uint32_t p = j >> 1;
-            const float2 dx = __fadd2_rn(__fadd2_rn(cp[kHx][p], nhx), __fadd2_rn(cp[kLx][p], nlx));
-            const float2 dy = __fadd2_rn(__fadd2_rn(cp[kHy][p], nhy), __fadd2_rn(cp[kLy][p], nly));
-            const float2 dz = __fadd2_rn(__fadd2_rn(cp[kHz][p], nhz), __fadd2_rn(cp[kLz][p], nlz));
-            const uint2 mk = ws.mask_pairs[p];
-            const bool in0 = (mk.x & lane_bit) != 0u;
-            const bool in1 = (mk.y & lane_bit) != 0u;
+            const float4 q0 = cq[0][p], q1 = cq[1][p], q2 = cq[2][p], q3 = cq[3][p];
+            const float2 dx = __fadd2_rn(__fadd2_rn(f2(q0.x, q0.y), nhx), __fadd2_rn(f2(q2.x, q2.y), nlx));
+            const float2 dy = __fadd2_rn(__fadd2_rn(f2(q0.z, q0.w), nhy), __fadd2_rn(f2(q2.z, q2.w), nly));
+            const float2 dz = __fadd2_rn(__fadd2_rn(f2(q1.x, q1.y), nhz), __fadd2_rn(f2(q3.x, q3.y), nlz));
+            const bool in0 = (__float_as_uint(q3.z) & lane_bit) != 0u;
+            const bool in1 = (__float_as_uint(q3.w) & lane_bit) != 0u;
             cells += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
             const float2 r2e =
                 __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
@@ -316,12 +315,13 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
             const float inv1 = rsqrt_approx(r2e.y);
             const float2 inv = f2(in0 ? inv0 : 0.0f, in1 ? inv1 : 0.0f);
             const float2 inv2 = __fmul2_rn(inv, inv);
-            const float2 f = __fmul2_rn(__fmul2_rn(cp[kMass][p], inv), inv2);
+            const float2 f = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
             float2 tx = __fmul2_rn(dx, f), ty = __fmul2_rn(dy, f), tz = __fmul2_rn(dz, f);
             if (QUAD) {
-                const float2 xx = cp[kQxx][p], xy = cp[kQxy][p];
-                const float2 xz = cp[kQxz][p], yy = cp[kQyy][p];
-                const float2 yz = cp[kQyz][p], zz = cp[kQzz][p];
+                const float4 q4 = cq[4][p], q5 = cq[5][p], q6 = cq[6][p];
+                const float2 xx = f2(q4.x, q4.y), xy = f2(q4.z, q4.w);
+                const float2 xz = f2(q5.x, q5.y), yy = f2(q5.z, q5.w);
+                const float2 yz = f2(q6.x, q6.y), zz = f2(q6.z, q6.w);
                 const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
                 const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
                 const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
@@ -383,45 +383,62 @@ __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
         const bool own = in && i >= first && i < first + size;
         const bool masked = __any_sync(kFull, own);
         // Offset leaf centre of mass - target; source - target = source + d.
-        const float dx = (A.x - pxh) + (B.x - pxl);
-        const float dy = (A.y - pyh) + (B.y - pyl);
-        const float dz = (A.z - pzh) + (B.z - pzl);
+        // Lanes outside the mask sit far away: their terms are exactly zero.
+        const float dx = in ? (A.x - pxh) + (B.x - pxl) : kFar;
+        const float dy = in ? (A.y - pyh) + (B.y - pyl) : kFar;
+        const float dz = in ? (A.z - pzh) + (B.z - pzl) : kFar;
         const float2 dx2 = f2(dx, dx), dy2 = f2(dy, dy), dz2 = f2(dz, dz);
         float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
         for (uint32_t base = 0; base < size; base += 32) {
             const uint32_t chunk = min(32u, size - base);
-            float2(*lp)[17] = ws.leaf_pairs;
+            float4(*lq)[17] = ws.leaf_quads;
             if (lane < chunk) {
                 const float4 src = leaf_rel[first + base + lane];
-                put(lp[kSx], lane, src.x);
-                put(lp[kSy], lane, src.y);
-                put(lp[kSz], lane, src.z);
-                put(lp[kSm], lane, src.w);
+                put(lq[0], lane, src.x, src.y);
+                put(lq[1], lane, src.z, src.w);
             } else if (lane == chunk) {
-                for (int q = 0; q < kLeafFields; ++q) {
-                    put(lp[q], lane, 0.0f);
-                }
+                // Neutral partner: far away and massless.
+                put(lq[0], lane, kFar, kFar);
+                put(lq[1], lane, kFar, 0.0f);
             }
             __syncwarp();
-            for (uint32_t j = 0; j < chunk; j += 2) {
-                const uint32_t p = j >> 1;
-                const float2 ex = __fadd2_rn(lp[kSx][p], dx2);
-                const float2 ey = __fadd2_rn(lp[kSy][p], dy2);
-                const float2 ez = __fadd2_rn(lp[kSz][p], dz2);
-                float2 r2 = __ffma2_rn(ez, ez, __ffma2_rn(ey, ey, __ffma2_rn(ex, ex, e2)));
-                float2 m = lp[kSm][p];
-                // The target itself, the zero partner of an odd count and
-                // lanes outside the mask contribute nothing.
-                const uint32_t index = first + base + j;
-                const bool skip0 = !in || (masked && index == i);
-                const bool skip1 = !in || j + 1 >= chunk || (masked && index + 1 == i);
-                r2 = f2(skip0 ? 1.0f : r2.x, skip1 ? 1.0f : r2.y);
-                m = f2(skip0 ? 0.0f : m.x, skip1 ? 0.0f : m.y);
-                const float2 inv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-                const float2 f = __fmul2_rn(__fmul2_rn(m, inv), __fmul2_rn(inv, inv));
-                sx = __ffma2_rn(f, ex, sx);
-                sy = __ffma2_rn(f, ey, sy);
-                sz = __ffma2_rn(f, ez, sz);
+            // Every lane runs the loop (no divergent region).
+            if (!masked) {
+                for (uint32_t j = 0; j < chunk; j += 2) {
+                    const uint32_t p = j >> 1;
+                    const float4 s0 = lq[0][p], s1 = lq[1][p];
+                    const float2 ex = __fadd2_rn(f2(s0.x, s0.y), dx2);
+                    const float2 ey = __fadd2_rn(f2(s0.z, s0.w), dy2);
+                    const float2 ez = __fadd2_rn(f2(s1.x, s1.y), dz2);
+                    const float2 r2 =
+                        __ffma2_rn(ez, ez, __ffma2_rn(ey, ey, __ffma2_rn(ex, ex, e2)));
+                    const float2 inv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                    const float2 f =
+                        __fmul2_rn(__fmul2_rn(f2(s1.z, s1.w), inv), __fmul2_rn(inv, inv));
+                    sx = __ffma2_rn(f, ex, sx);
+                    sy = __ffma2_rn(f, ey, sy);
+                    sz = __ffma2_rn(f, ez, sz);
+                }
+            } else {
+                for (uint32_t j = 0; j < chunk; j += 2) {
+                    const uint32_t p = j >> 1;
+                    const float4 s0 = lq[0][p], s1 = lq[1][p];
+                    const float2 ex = __fadd2_rn(f2(s0.x, s0.y), dx2);
+                    const float2 ey = __fadd2_rn(f2(s0.z, s0.w), dy2);
+                    const float2 ez = __fadd2_rn(f2(s1.x, s1.y), dz2);
+                    float2 r2 = __ffma2_rn(ez, ez, __ffma2_rn(ey, ey, __ffma2_rn(ex, ex, e2)));
+                    // The target itself contributes nothing.
+                    const uint32_t index = first + base + j;
+                    const bool skip0 = index == i;
+                    const bool skip1 = index + 1 == i;
+                    r2 = f2(skip0 ? 1.0f : r2.x, skip1 ? 1.0f : r2.y);
+                    const float2 m = f2(skip0 ? 0.0f : s1.z, skip1 ? 0.0f : s1.w);
+                    const float2 inv = f2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+                    const float2 f = __fmul2_rn(__fmul2_rn(m, inv), __fmul2_rn(inv, inv));
+                    sx = __ffma2_rn(f, ex, sx);
+                    sy = __ffma2_rn(f, ey, sy);
+                    sz = __ffma2_rn(f, ez, sz);
+                }
             }
             __syncwarp();
         }
@@ -435,7 +452,7 @@ __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
 }
 
 template <bool QUAD>
-__global__ void __launch_bounds__(kWalkThreads)
+__global__ void __launch_bounds__(kWalkThreads, 8)
     walk_kernel(const DeviceNode *__restrict__ nodes, const WalkNode *__restrict__ walk,
                 const uint32_t *__restrict__ first_of, const float4 *__restrict__ leaf_rel,
                 const double *__restrict__ sorted, const uint32_t *__restrict__ perm, uint32_t n,
@@ -494,11 +511,12 @@ __global__ void __launch_bounds__(kWalkThreads)
     }
     __syncwarp();
     while (size > 0) {
-        const uint32_t take = min(size, 32u);
+        // Popping t items and pushing up to 2t needs size + t <= kStackCap.
+        const uint32_t take = min(min(size, 32u), kStackCap - min(size, kStackCap));
         // A valid tree visits each node at most once, so more rounds than
         // nodes (or a full stack) hands the warp to the union walk, whose
         // cursors only move forward.
-        if (size - take + 64u > kStackCap || ++rounds > node_count + 1u) {
+        if (take == 0u || ++rounds > node_count + 1u) {
             overflow = true;
             break;
         }
@@ -621,12 +639,12 @@ __global__ void __launch_bounds__(kWalkThreads)
             }
         }
         __syncwarp();
-        if (ncell > kCellCap - 64u) {
+        if (ncell > kCellCap - 32u) {
             flush_cells<QUAD>(ws, ncell, walk, nhx, nhy, nhz, nlx, nly, nlz, eps2v, lane_bit,
                               acc_x, acc_y, acc_z, cells, node_count, status);
             ncell = 0;
         }
-        if (nleaf > kLeafCap - 64u) {
+        if (nleaf > kLeafCap - 32u) {
             flush_leaves(ws, nleaf, walk, first_of, leaf_rel, pxh, pyh, pzh, pxl, pyl, pzl, eps2,
                          i, lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
             nleaf = 0;
