@@ -321,6 +321,48 @@ def cpu_baseline_serving(w, budget_s):
                        "serially")
 
 
+def reference_gpu_serving(budget_s):
+    """The reference's own CUDA solvers on the serving stream in arrival order:
+    one timed host-buffer evaluation per job (after one warm-up evaluation)
+    until the budget is spent, each job's time taken as that evaluation times
+    its evaluation count; jobs serial. None without the library or a device."""
+    import oracle
+
+    if not oracle.ReferenceCuda.built():
+        return None
+    try:
+        ref = oracle.ReferenceCuda()
+        if not ref.available():
+            return None
+        threads = oracle.Reference().worker_count() if oracle.Reference.available() else 1
+        jobs = make_stream(3.0)
+        states = job_states(jobs)
+        projected, spent, done = 0.0, 0.0, 0
+        for job, st in zip(jobs, states):
+            p = JOB_PARAMS[job["kind"]]
+            if job["kind"] == "direct":
+                wall, _, _ = ref.direct_timed(st["x"], st["y"], st["z"], st["m"], p["softening"],
+                                              repeats=1)
+                evals = 1 + 3 * job["steps"]
+            else:
+                wall, _, _, _ = ref.tree_timed(st["x"], st["y"], st["z"], st["m"], p["softening"],
+                                               p["theta"], p["leaf"], True, threads, repeats=1)
+                evals = 1 + job["steps"]
+            projected += wall * evals
+            spent += 2 * wall
+            done += 1
+            if spent > budget_s:
+                break
+        return {"solvers": "CudaDirectSolver (FP64) and CudaTreeSolver (host build on "
+                           f"{threads} threads), the reference's own GPU path",
+                "value": done / projected, "unit": "jobs/s",
+                "sample": f"one timed evaluation of each of the stream's first {done} jobs "
+                          f"(of {len(jobs)}), scaled by each job's evaluation count; jobs "
+                          "run serially"}
+    except (OSError, RuntimeError) as err:
+        return {"unavailable": str(err)}
+
+
 def reference_gpu(w, data):
     """The reference's own CUDA solvers (its .cu kernels built for sm_100a by
     oracle/Makefile) on the same input and device, when built and a device is
@@ -370,6 +412,9 @@ def run_reference(args, w):
                 "cpu_baseline": base,
                 "e2e": {"value": base["value"], "unit": "jobs/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": 0}}
+        gpu = reference_gpu_serving(budget_s=min(120.0, 20.0 * steps))
+        if gpu is not None:
+            line["reference_gpu"] = gpu
         print(json.dumps(line), flush=True)
         barrier(dist)
         return
