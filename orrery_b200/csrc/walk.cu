@@ -33,10 +33,11 @@
 // about 2e-7 relative with no FP64 work. Force terms are FP32, summed in FP32
 // within a batch (or leaf) and flushed into FP64 per-target sums.
 //
-// If a warp's stack would overflow its fixed shared-memory capacity (never
-// seen: 121 items at most against 256 on the 2M collision), the warp discards
-// its partial sums and walks its targets with the per-target union walk
-// (union_walk below), which gives the same counts.
+// A round takes no more items than the stack has room to push back, so the
+// stack (160 entries per warp; the 2M collision needs about 120) only stops
+// the traversal if it is completely full; the warp then discards its partial
+// sums and walks its targets with the per-target union walk (union_walk
+// below), which gives the same counts.
 //
 // Warp discipline. Between the warp's votes and barriers there is no
 // lane-divergent stretch of work: lanes outside a leaf's or cell's mask run
