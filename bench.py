@@ -667,8 +667,12 @@ def job_states(jobs):
     from orrery_b200 import initial_conditions as ic
 
     rng = np.random.default_rng(7)
-    templates = {"direct": ic.plummer_sphere(65536, seed=20260815),
-                 "tree": ic.galaxy_collision(4_000_000, softening=0.02, seed=20260816)}
+    kinds = {j["kind"] for j in jobs}
+    templates = {}
+    if "direct" in kinds:
+        templates["direct"] = ic.plummer_sphere(65536, seed=20260815)
+    if "tree" in kinds:
+        templates["tree"] = ic.galaxy_collision(4_000_000, softening=0.02, seed=20260816)
     perms = {"direct": rng.permutation(65536), "tree": rng.permutation(4_000_000)}
     out = []
     for job in jobs:
