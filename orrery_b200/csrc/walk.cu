@@ -80,10 +80,10 @@ struct GroupItem {
 // the two fields a, b of group f and the entries j = 2p, 2p+1, so one 16-byte
 // shared load yields two FP32x2 operands. 17 pairs: an odd count reads one
 // neutral partner past its end.
-//   cells:  (hi x, hi y) (hi z, mass) (lo x, lo y) (lo z, target mask bits)
-//           (Qxx, Qxy) (Qxz, Qyy) (Qyz, Qzz)
+//   cells:  (x, y) (z, mass) (target mask bits, 0) (Qxx, Qxy) (Qxz, Qyy)
+//           (Qyz, Qzz), centres relative to the warp's box centre
 //   leaves: (x, y) (z, mass), leaf-relative
-constexpr int kCellQuads = 7;
+constexpr int kCellQuads = 6;
 constexpr int kLeafQuads = 2;
 // Offset given to lanes outside a leaf's mask and to the neutral partner: the
 // terms it produces underflow to exactly zero in FP32.
@@ -99,6 +99,7 @@ struct __align__(16) WarpSpace {
         float4 union_staged[32]; // the union walk's leaf staging (after a fallback)
     };
     float4 leaf_quads[kLeafQuads][17];
+    double box[9]; // lo xyz, hi xyz and centre G of the warp's targets (FP64)
 };
 
 // Writes entry j's two fields a, b into quad array q (see cell_quads).
@@ -260,17 +261,22 @@ __device__ void union_walk(const DeviceNode *__restrict__ nodes,
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 // Evaluates the warp's cell list: every lane sums every cell for its target
-// (zero outside the cell's mask), two cells per FP32x2 instruction.
+// (zero outside the cell's mask), two cells per FP32x2 instruction. Cell
+// centres are staged relative to the warp's box centre G (rounded to FP32
+// once, from FP64), and each lane holds its target relative to G, so the
+// offset to a cell is one subtraction; both are within the box's reach of the
+// cell, so the offset keeps about FP32 relative accuracy.
 template <bool QUAD>
 __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
-                                            const WalkNode *__restrict__ walk, float2 nhx,
-                                            float2 nhy, float2 nhz, float2 nlx, float2 nly,
-                                            float2 nlz, float2 eps2, uint32_t lane_bit,
+                                            const DeviceNode *__restrict__ nodes,
+                                            const WalkNode *__restrict__ walk, float2 ntx,
+                                            float2 nty,
+                                            float2 ntz, float2 eps2, uint32_t lane_bit,
                                             double &acc_x, double &acc_y, double &acc_z,
                                             uint32_t &cells, uint32_t node_count,
                                             unsigned *status) {
     const uint32_t lane = threadIdx.x & 31u;
-    float2 gx = f2(0.0f, 0.0f), gy = gx, gz = gx;
+    float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
     for (uint32_t base = 0; base < count; base += 32) {
         const uint32_t chunk = min(32u, count - base);
         float4(*cq)[17] = ws.cell_quads;
@@ -280,22 +286,23 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
                 atomicOr(status, kStatusInvalid);
                 e = make_uint2(0u, 0u); // no target: contributes nothing
             }
-            const WalkNode *w = walk + e.x;
-            const float4 A = w->a;
-            const float4 B = w->b;
-            put(cq[0], lane, A.x, A.y);
-            put(cq[1], lane, A.z, A.w);
-            put(cq[2], lane, B.x, B.y);
-            put(cq[3], lane, B.z, __uint_as_float(e.y));
+            const DeviceNode *nd = nodes + e.x;
+            const float cx = __double2float_rn(nd->com_x - ws.box[6]);
+            const float cy = __double2float_rn(nd->com_y - ws.box[7]);
+            const float cz = __double2float_rn(nd->com_z - ws.box[8]);
+            const float m = walk[e.x].a.w;
+            put(cq[0], lane, cx, cy);
+            put(cq[1], lane, cz, m);
+            put(cq[2], lane, __uint_as_float(e.y), 0.0f);
             if (QUAD) {
-                const float4 C = w->c;
-                const float4 D = w->d;
-                put(cq[4], lane, C.x, C.y);
-                put(cq[5], lane, C.z, C.w);
-                put(cq[6], lane, D.x, D.y);
+                const float4 C = walk[e.x].c; // (xx, xy, xz, yy)
+                const float4 D = walk[e.x].d; // (yz, zz, next, count)
+                put(cq[3], lane, C.x, C.y);
+                put(cq[4], lane, C.z, C.w);
+                put(cq[5], lane, D.x, D.y);
             }
         } else if (lane == chunk) {
-            // The odd entry's partner: no target, zero mass, at the origin.
+            // The odd entry's partner: no target, zero mass, at G.
             for (int q = 0; q < kCellQuads; ++q) {
                 put(cq[q], lane, 0.0f, 0.0f);
             }
@@ -303,12 +310,12 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
         __syncwarp();
         for (uint32_t j = 0; j < chunk; j += 2) {
             const uint32_t p = j >> 1;
-            const float4 q0 = cq[0][p], q1 = cq[1][p], q2 = cq[2][p], q3 = cq[3][p];
-            const float2 dx = __fadd2_rn(__fadd2_rn(f2(q0.x, q0.y), nhx), __fadd2_rn(f2(q2.x, q2.y), nlx));
-            const float2 dy = __fadd2_rn(__fadd2_rn(f2(q0.z, q0.w), nhy), __fadd2_rn(f2(q2.z, q2.w), nly));
-            const float2 dz = __fadd2_rn(__fadd2_rn(f2(q1.x, q1.y), nhz), __fadd2_rn(f2(q3.x, q3.y), nlz));
-            const bool in0 = (__float_as_uint(q3.z) & lane_bit) != 0u;
-            const bool in1 = (__float_as_uint(q3.w) & lane_bit) != 0u;
+            const float4 q0 = cq[0][p], q1 = cq[1][p], q2 = cq[2][p];
+            const float2 dx = __fadd2_rn(f2(q0.x, q0.y), ntx);
+            const float2 dy = __fadd2_rn(f2(q0.z, q0.w), nty);
+            const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
+            const bool in0 = (__float_as_uint(q2.x) & lane_bit) != 0u;
+            const bool in1 = (__float_as_uint(q2.y) & lane_bit) != 0u;
             cells += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
             const float2 r2e =
                 __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
@@ -316,35 +323,37 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
             const float inv1 = rsqrt_approx(r2e.y);
             const float2 inv = f2(in0 ? inv0 : 0.0f, in1 ? inv1 : 0.0f);
             const float2 inv2 = __fmul2_rn(inv, inv);
-            const float2 f = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
-            float2 tx = __fmul2_rn(dx, f), ty = __fmul2_rn(dy, f), tz = __fmul2_rn(dz, f);
+            // Monopole m d / r^3 (tree_walk.hpp:129-140).
+            float2 coef = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
             if (QUAD) {
-                const float4 q4 = cq[4][p], q5 = cq[5][p], q6 = cq[6][p];
-                const float2 xx = f2(q4.x, q4.y), xy = f2(q4.z, q4.w);
-                const float2 xz = f2(q5.x, q5.y), yy = f2(q5.z, q5.w);
-                const float2 yz = f2(q6.x, q6.y), zz = f2(q6.z, q6.w);
+                // Quadrupole -Q d / r^5 + 2.5 (d.Q d) d / r^7 (tree_walk.hpp:142-181),
+                // folded with the monopole: d (m / r^3 + 2.5 (d.Q d) / r^7) - Q d / r^5.
+                const float4 q3 = cq[3][p], q4 = cq[4][p], q5 = cq[5][p];
+                const float2 xx = f2(q3.x, q3.y), xy = f2(q3.z, q3.w);
+                const float2 xz = f2(q4.x, q4.y), yy = f2(q4.z, q4.w);
+                const float2 yz = f2(q5.x, q5.y), zz = f2(q5.z, q5.w);
                 const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
                 const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
                 const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
                 const float2 quadratic =
                     __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
                 const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
-                const float2 s = __fmul2_rn(__fmul2_rn(f2(2.5f, 2.5f), quadratic),
-                                            __fmul2_rn(inv5, inv2));
-                const float2 ninv5 = f2(-inv5.x, -inv5.y);
-                tx = __ffma2_rn(qx, ninv5, __ffma2_rn(dx, s, tx));
-                ty = __ffma2_rn(qy, ninv5, __ffma2_rn(dy, s, ty));
-                tz = __ffma2_rn(qz, ninv5, __ffma2_rn(dz, s, tz));
+                coef = __ffma2_rn(__fmul2_rn(f2(2.5f, 2.5f), quadratic),
+                                  __fmul2_rn(inv5, inv2), coef);
+                const float2 ninv5 = __fmul2_rn(inv5, f2(-1.0f, -1.0f));
+                sx = __ffma2_rn(qx, ninv5, sx);
+                sy = __ffma2_rn(qy, ninv5, sy);
+                sz = __ffma2_rn(qz, ninv5, sz);
             }
-            gx = __fadd2_rn(gx, tx);
-            gy = __fadd2_rn(gy, ty);
-            gz = __fadd2_rn(gz, tz);
+            sx = __ffma2_rn(dx, coef, sx);
+            sy = __ffma2_rn(dy, coef, sy);
+            sz = __ffma2_rn(dz, coef, sz);
         }
         __syncwarp();
     }
-    acc_x += static_cast<double>(gx.x) + static_cast<double>(gx.y);
-    acc_y += static_cast<double>(gy.x) + static_cast<double>(gy.y);
-    acc_z += static_cast<double>(gz.x) + static_cast<double>(gz.y);
+    acc_x += static_cast<double>(sx.x) + static_cast<double>(sx.y);
+    acc_y += static_cast<double>(sy.x) + static_cast<double>(sy.y);
+    acc_z += static_cast<double>(sz.x) + static_cast<double>(sz.y);
 }
 
 // Evaluates the warp's leaf list: for each opened leaf, the lanes in its mask
@@ -485,8 +494,6 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         pyl = __double2float_rn(Y - static_cast<double>(pyh));
         pzl = __double2float_rn(Z - static_cast<double>(pzh));
     }
-    const float2 nhx = f2(-pxh, -pxh), nhy = f2(-pyh, -pyh), nhz = f2(-pzh, -pzh);
-    const float2 nlx = f2(-pxl, -pxl), nly = f2(-pyl, -pyl), nlz = f2(-pzl, -pzl);
     const float2 eps2v = f2(eps2, eps2);
 
     // FP64 bounding box of the warp's targets.
@@ -501,6 +508,24 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         hiy = fmax(hiy, __shfl_xor_sync(kFull, hiy, off));
         hiz = fmax(hiz, __shfl_xor_sync(kFull, hiz, off));
     }
+
+    // The box centre G and this lane's target relative to it (FP32).
+    const double gcx = 0.5 * (lox + hix), gcy = 0.5 * (loy + hiy), gcz = 0.5 * (loz + hiz);
+    const float tgx = __double2float_rn(X - gcx), tgy = __double2float_rn(Y - gcy),
+                tgz = __double2float_rn(Z - gcz);
+    const float2 ntx = f2(-tgx, -tgx), nty = f2(-tgy, -tgy), ntz = f2(-tgz, -tgz);
+    if (lane == 0) {
+        ws.box[0] = lox;
+        ws.box[1] = loy;
+        ws.box[2] = loz;
+        ws.box[3] = hix;
+        ws.box[4] = hiy;
+        ws.box[5] = hiz;
+        ws.box[6] = gcx;
+        ws.box[7] = gcy;
+        ws.box[8] = gcz;
+    }
+    __syncwarp();
 
     double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
     uint32_t pairs = 0, cells = 0;
@@ -543,6 +568,8 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
             next = nd->next;
             const uint32_t count = nd->count;
             sibling = next < item.end;
+            const double lox = ws.box[0], loy = ws.box[1], loz = ws.box[2];
+            const double hix = ws.box[3], hiy = ws.box[4], hiz = ws.box[5];
             const double nx = fmax(fmax(__dsub_rn(lox, cx), __dsub_rn(cx, hix)), 0.0);
             const double ny = fmax(fmax(__dsub_rn(loy, cy), __dsub_rn(cy, hiy)), 0.0);
             const double nz = fmax(fmax(__dsub_rn(loz, cz), __dsub_rn(cz, hiz)), 0.0);
@@ -641,8 +668,8 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         }
         __syncwarp();
         if (ncell > kCellCap - 32u) {
-            flush_cells<QUAD>(ws, ncell, walk, nhx, nhy, nhz, nlx, nly, nlz, eps2v, lane_bit,
-                              acc_x, acc_y, acc_z, cells, node_count, status);
+            flush_cells<QUAD>(ws, ncell, nodes, walk, ntx, nty, ntz, eps2v,
+                              lane_bit, acc_x, acc_y, acc_z, cells, node_count, status);
             ncell = 0;
         }
         if (nleaf > kLeafCap - 32u) {
@@ -658,8 +685,8 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
                          pxh, pyh, pzh, pxl, pyl, pzl, ws.union_staged, acc_x, acc_y, acc_z, pairs,
                          cells);
     } else {
-        flush_cells<QUAD>(ws, ncell, walk, nhx, nhy, nhz, nlx, nly, nlz, eps2v, lane_bit, acc_x,
-                          acc_y, acc_z, cells, node_count, status);
+        flush_cells<QUAD>(ws, ncell, nodes, walk, ntx, nty, ntz, eps2v,
+                          lane_bit, acc_x, acc_y, acc_z, cells, node_count, status);
         flush_leaves(ws, nleaf, walk, first_of, leaf_rel, pxh, pyh, pzh, pxl, pyl, pzl, eps2, i,
                      lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
     }
