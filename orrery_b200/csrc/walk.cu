@@ -295,11 +295,12 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
             put(cq[1], lane, cz, m);
             put(cq[2], lane, __uint_as_float(e.y), 0.0f);
             if (QUAD) {
+                // Staged as 2.5 Q: the loop needs 2.5 (d.Q d) and Q d.
                 const float4 C = walk[e.x].c; // (xx, xy, xz, yy)
                 const float4 D = walk[e.x].d; // (yz, zz, next, count)
-                put(cq[3], lane, C.x, C.y);
-                put(cq[4], lane, C.z, C.w);
-                put(cq[5], lane, D.x, D.y);
+                put(cq[3], lane, 2.5f * C.x, 2.5f * C.y);
+                put(cq[4], lane, 2.5f * C.z, 2.5f * C.w);
+                put(cq[5], lane, 2.5f * D.x, 2.5f * D.y);
             }
         } else if (lane == chunk) {
             // The odd entry's partner: no target, zero mass, at G.
@@ -335,12 +336,12 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
                 const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
                 const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
                 const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
+                // q = 2.5 Q d, quadratic = 2.5 d.Q d.
                 const float2 quadratic =
                     __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
                 const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
-                coef = __ffma2_rn(__fmul2_rn(f2(2.5f, 2.5f), quadratic),
-                                  __fmul2_rn(inv5, inv2), coef);
-                const float2 ninv5 = __fmul2_rn(inv5, f2(-1.0f, -1.0f));
+                coef = __ffma2_rn(quadratic, __fmul2_rn(inv5, inv2), coef);
+                const float2 ninv5 = __fmul2_rn(inv5, f2(-0.4f, -0.4f));
                 sx = __ffma2_rn(qx, ninv5, sx);
                 sy = __ffma2_rn(qy, ninv5, sy);
                 sz = __ffma2_rn(qz, ninv5, sz);
