@@ -357,8 +357,9 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
     acc_z += static_cast<double>(sz.x) + static_cast<double>(sz.y);
 }
 
-// Evaluates the warp's leaf list: for each opened leaf, the lanes in its mask
-// sum its particles (staged in shared memory once per chunk of 32), two
+// Evaluates the warp's leaf list: for each opened leaf, every lane sums its
+// particles for its own target (staged in shared memory once per chunk of 32;
+// lanes outside the leaf's mask sit far away and add exactly zero), two
 // sources per FP32x2 instruction, skipping the target itself.
 __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
                                              const WalkNode *__restrict__ walk,
@@ -371,6 +372,9 @@ __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
                                              uint32_t n, unsigned *status) {
     const uint32_t lane = threadIdx.x & 31u;
     const float2 e2 = f2(eps2, eps2);
+    // FP32 sums over the batch's leaves (lanes outside a leaf's mask add
+    // exactly zero), folded into FP64 once per batch like the cell sums.
+    float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
     for (uint32_t k = 0; k < count; ++k) {
         const uint2 e = ws.leaves[k];
         if (e.x >= node_count) {
@@ -399,7 +403,6 @@ __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
         const float dy = in ? (A.y - pyh) + (B.y - pyl) : kFar;
         const float dz = in ? (A.z - pzh) + (B.z - pzl) : kFar;
         const float2 dx2 = f2(dx, dx), dy2 = f2(dy, dy), dz2 = f2(dz, dz);
-        float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
         for (uint32_t base = 0; base < size; base += 32) {
             const uint32_t chunk = min(32u, size - base);
             float4(*lq)[17] = ws.leaf_quads;
@@ -453,13 +456,11 @@ __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
             }
             __syncwarp();
         }
-        if (in) {
-            acc_x += static_cast<double>(sx.x) + static_cast<double>(sx.y);
-            acc_y += static_cast<double>(sy.x) + static_cast<double>(sy.y);
-            acc_z += static_cast<double>(sz.x) + static_cast<double>(sz.y);
-            pairs += size - (own ? 1u : 0u);
-        }
+        pairs += in ? size - (own ? 1u : 0u) : 0u;
     }
+    acc_x += static_cast<double>(sx.x) + static_cast<double>(sx.y);
+    acc_y += static_cast<double>(sy.x) + static_cast<double>(sy.y);
+    acc_z += static_cast<double>(sz.x) + static_cast<double>(sz.y);
 }
 
 template <bool QUAD>
