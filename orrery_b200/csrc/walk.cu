@@ -273,7 +273,7 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
                                             float2 nty,
                                             float2 ntz, float2 eps2, uint32_t lane_bit,
                                             double &acc_x, double &acc_y, double &acc_z,
-                                            uint32_t &cells, uint32_t node_count,
+                                            uint32_t node_count,
                                             unsigned *status) {
     const uint32_t lane = threadIdx.x & 31u;
     float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
@@ -317,7 +317,6 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
             const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
             const bool in0 = (__float_as_uint(q2.x) & lane_bit) != 0u;
             const bool in1 = (__float_as_uint(q2.y) & lane_bit) != 0u;
-            cells += (in0 ? 1u : 0u) + (in1 ? 1u : 0u);
             const float2 r2e =
                 __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
             const float inv0 = rsqrt_approx(r2e.x);
@@ -605,6 +604,7 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         const uint32_t ba = __ballot_sync(kFull, cell);
         if (cell) {
             ws.cells[ncell + __popc(ba & below)] = make_uint2(item.node, item.mask);
+            cells += __popc(item.mask); // every target of the mask takes the cell
         }
         ncell += __popc(ba);
         const uint32_t bl = __ballot_sync(kFull, leaf);
@@ -650,6 +650,7 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
             if (lane == 0) {
                 if (accepted != 0u) {
                     ws.cells[ncell] = make_uint2(v, accepted);
+                    cells += __popc(accepted);
                 }
                 if (opened != 0u) {
                     if (vcount > 0u) {
@@ -671,7 +672,7 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         __syncwarp();
         if (ncell > kCellCap - 32u) {
             flush_cells<QUAD>(ws, ncell, nodes, walk, ntx, nty, ntz, eps2v,
-                              lane_bit, acc_x, acc_y, acc_z, cells, node_count, status);
+                              lane_bit, acc_x, acc_y, acc_z, node_count, status);
             ncell = 0;
         }
         if (nleaf > kLeafCap - 32u) {
@@ -688,7 +689,7 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
                          cells);
     } else {
         flush_cells<QUAD>(ws, ncell, nodes, walk, ntx, nty, ntz, eps2v,
-                          lane_bit, acc_x, acc_y, acc_z, cells, node_count, status);
+                          lane_bit, acc_x, acc_y, acc_z, node_count, status);
         flush_leaves(ws, nleaf, walk, first_of, leaf_rel, pxh, pyh, pzh, pxl, pyl, pzl, eps2, i,
                      lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
     }
@@ -699,7 +700,8 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         ay[j] = acc_y;
         az[j] = acc_z;
     }
-    unsigned long long p = active ? pairs : 0u, c = active ? cells : 0u;
+    // pairs: per target; cells: tallied by the lanes that queued the entries.
+    unsigned long long p = active ? pairs : 0u, c = cells;
     for (int off = 16; off > 0; off >>= 1) {
         p += __shfl_down_sync(kFull, p, off);
         c += __shfl_down_sync(kFull, c, off);
