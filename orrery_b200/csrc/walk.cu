@@ -94,9 +94,10 @@ struct __align__(16) WarpSpace {
     GroupItem mixed[32];    // this round's mixed items
     uint2 cells[kCellCap];  // (node, target mask)
     uint2 leaves[kLeafCap]; // (node, target mask)
-    union {
+    union {                 // used one at a time
         float4 cell_quads[kCellQuads][17];
-        float4 union_staged[32]; // the union walk's leaf staging (after a fallback)
+        float4 leaf_pos[kLeafCap]; // queued leaves: centre - G (FP32), particle count bits
+        float4 union_staged[32];   // the union walk's leaf staging (after a fallback)
     };
     float4 leaf_quads[kLeafQuads][17];
     double box[9]; // lo xyz, hi xyz and centre G of the warp's targets (FP64)
@@ -359,48 +360,71 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
 // Evaluates the warp's leaf list: for each opened leaf, every lane sums its
 // particles for its own target (staged in shared memory once per chunk of 32;
 // lanes outside the leaf's mask sit far away and add exactly zero), two
-// sources per FP32x2 instruction, skipping the target itself.
+// sources per FP32x2 instruction, skipping the target itself. First, one
+// lane per queued leaf reads its particle range and centre of mass and stores
+// the centre relative to the warp's box centre G, and whether the leaf's range
+// can hold one of the warp's targets (the only leaves that need the
+// self-skip); each leaf then costs its offset (three subtractions) and its
+// sources.
 __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
+                                             const DeviceNode *__restrict__ nodes,
                                              const WalkNode *__restrict__ walk,
                                              const uint32_t *__restrict__ first_of,
-                                             const float4 *__restrict__ leaf_rel, float pxh,
-                                             float pyh, float pzh, float pxl, float pyl,
-                                             float pzl, float eps2, uint32_t i,
-                                             uint32_t lane_bit, double &acc_x, double &acc_y,
-                                             double &acc_z, uint32_t &pairs, uint32_t node_count,
-                                             uint32_t n, unsigned *status) {
+                                             const float4 *__restrict__ leaf_rel, float tgx,
+                                             float tgy, float tgz, float eps2, uint32_t i,
+                                             uint32_t warp_first, uint32_t lane_bit,
+                                             double &acc_x, double &acc_y, double &acc_z,
+                                             uint32_t &pairs, uint32_t node_count, uint32_t n,
+                                             unsigned *status) {
     const uint32_t lane = threadIdx.x & 31u;
     const float2 e2 = f2(eps2, eps2);
+    const uint32_t warp_end = min(warp_first + 32u, n);
+    // Per-leaf metadata, one leaf per lane: ws.leaf_pos[k] = (centre - G,
+    // count bits); ws.leaves[k].x = first particle, bit 31 set when the leaf
+    // may hold one of the warp's targets.
+    for (uint32_t base = 0; base < count; base += 32) {
+        const uint32_t k = base + lane;
+        if (k < count) {
+            const uint2 e = ws.leaves[k];
+            uint32_t size = 0u, first = 0u;
+            float4 pos = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (e.x < node_count) {
+                size = __float_as_uint(walk[e.x].d.w);
+                first = first_of[e.x];
+                if (first > n || size > n - first) {
+                    atomicOr(status, kStatusInvalid);
+                    size = 0u;
+                }
+                const DeviceNode *nd = nodes + e.x;
+                pos.x = __double2float_rn(nd->com_x - ws.box[6]);
+                pos.y = __double2float_rn(nd->com_y - ws.box[7]);
+                pos.z = __double2float_rn(nd->com_z - ws.box[8]);
+            } else {
+                atomicOr(status, kStatusInvalid);
+            }
+            pos.w = __uint_as_float(size);
+            const bool holds = first < warp_end && first + size > warp_first;
+            ws.leaf_pos[k] = pos;
+            ws.leaves[k].x = first | (holds ? 0x80000000u : 0u);
+        }
+    }
+    __syncwarp();
     // FP32 sums over the batch's leaves (lanes outside a leaf's mask add
     // exactly zero), folded into FP64 once per batch like the cell sums.
     float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
     for (uint32_t k = 0; k < count; ++k) {
+        const float4 pos = ws.leaf_pos[k];
         const uint2 e = ws.leaves[k];
-        if (e.x >= node_count) {
-            if (lane == 0) {
-                atomicOr(status, kStatusInvalid);
-            }
-            continue; // uniform: every lane reads the same entry
-        }
-        const WalkNode *w = walk + e.x;
-        const float4 A = w->a;
-        const float4 B = w->b;
-        const uint32_t size = __float_as_uint(w->d.w);
-        const uint32_t first = first_of[e.x];
-        if (first > n || size > n - first) {
-            if (lane == 0) {
-                atomicOr(status, kStatusInvalid);
-            }
-            continue;
-        }
+        const uint32_t size = __float_as_uint(pos.w);
+        const uint32_t first = e.x & 0x7fffffffu;
+        const bool masked = (e.x >> 31) != 0u; // uniform: every lane reads the same entry
         const bool in = (e.y & lane_bit) != 0u;
         const bool own = in && i >= first && i < first + size;
-        const bool masked = __any_sync(kFull, own);
         // Offset leaf centre of mass - target; source - target = source + d.
         // Lanes outside the mask sit far away: their terms are exactly zero.
-        const float dx = in ? (A.x - pxh) + (B.x - pxl) : kFar;
-        const float dy = in ? (A.y - pyh) + (B.y - pyl) : kFar;
-        const float dz = in ? (A.z - pzh) + (B.z - pzl) : kFar;
+        const float dx = in ? pos.x - tgx : kFar;
+        const float dy = in ? pos.y - tgy : kFar;
+        const float dz = in ? pos.z - tgz : kFar;
         const float2 dx2 = f2(dx, dx), dy2 = f2(dy, dy), dz2 = f2(dz, dz);
         for (uint32_t base = 0; base < size; base += 32) {
             const uint32_t chunk = min(32u, size - base);
@@ -676,8 +700,8 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
             ncell = 0;
         }
         if (nleaf > kLeafCap - 32u) {
-            flush_leaves(ws, nleaf, walk, first_of, leaf_rel, pxh, pyh, pzh, pxl, pyl, pzl, eps2,
-                         i, lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
+            flush_leaves(ws, nleaf, nodes, walk, first_of, leaf_rel, tgx, tgy, tgz, eps2, i,
+                         i - lane, lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
             nleaf = 0;
         }
     }
@@ -690,7 +714,7 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
     } else {
         flush_cells<QUAD>(ws, ncell, nodes, walk, ntx, nty, ntz, eps2v,
                           lane_bit, acc_x, acc_y, acc_z, node_count, status);
-        flush_leaves(ws, nleaf, walk, first_of, leaf_rel, pxh, pyh, pzh, pxl, pyl, pzl, eps2, i,
+        flush_leaves(ws, nleaf, nodes, walk, first_of, leaf_rel, tgx, tgy, tgz, eps2, i, i - lane,
                      lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
     }
 
