@@ -519,6 +519,8 @@ cudaError_t dispatch_direct(const DirectArgs &args, const DirectConfig &c, cudaS
 #define OB_DIRECT_CASE(T, RR)                                                                      \
     if (c.threads == T && c.targets_per_thread == RR)                                              \
         return launch_direct_t<T, RR, SPLIT>(args, c.split, stream);
+    OB_DIRECT_CASE(64, 2)
+    OB_DIRECT_CASE(64, 4)
     OB_DIRECT_CASE(128, 2)
     OB_DIRECT_CASE(128, 4)
     OB_DIRECT_CASE(256, 2)
@@ -593,11 +595,14 @@ cudaError_t launch_direct_f64(const double *x, const double *y, const double *z,
 }
 
 int direct_candidates(bool split, DirectConfig *out, int capacity) {
-    static const int split_shapes[][2] = {{128, 2}, {128, 4}, {256, 2}, {256, 4}};
-    static const int fp32_shapes[][2] = {{128, 2}, {128, 4}, {128, 8},
-                                         {256, 2}, {256, 4}, {256, 8}};
+    // 64-thread CTAs give small systems (a few thousand particles) enough
+    // CTAs to occupy the SMs.
+    static const int split_shapes[][2] = {{64, 2},  {64, 4},  {128, 2},
+                                          {128, 4}, {256, 2}, {256, 4}};
+    static const int fp32_shapes[][2] = {{64, 2},  {64, 4},  {128, 2}, {128, 4},
+                                         {128, 8}, {256, 2}, {256, 4}, {256, 8}};
     const int(*shapes)[2] = split ? split_shapes : fp32_shapes;
-    const int shape_count = split ? 4 : 6;
+    const int shape_count = split ? 6 : 8;
     static const int splits[] = {1, 2, 4, 8};
     int count = 0;
     for (int s = 0; s < shape_count; ++s) {
@@ -630,6 +635,9 @@ DirectConfig direct_default_config(uint32_t n, bool split, int sm_count) {
     }
     if (blocks() * 8u < sms) {
         c.threads = 128;
+    }
+    if (blocks() * 8u < sms) {
+        c.threads = 64;
     }
     while (c.split < 8 && blocks() * static_cast<uint32_t>(c.split) < 8u * sms &&
            static_cast<uint32_t>(c.split * 2) <= tiles) {
