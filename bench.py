@@ -1050,7 +1050,8 @@ def run_b200(args, w):
                                                   "traversal_ms")},
             "profiled_evaluations": evals,
             "autotuned_shape": None if tuned is None else
-            {"threads": tuned[0][0], "targets_per_thread": tuned[0][1], "split": tuned[0][2]},
+            {"threads": tuned[0][0], "targets_per_thread": tuned[0][1], "split": tuned[0][2],
+             "groups": tuned[0][3]},
             "roofline": roofline,
             "accuracy": accuracy,
             "e2e": {"value": e2e_value, "unit": w["unit"], "h2d_bytes_per_step": h2d,

@@ -157,15 +157,18 @@ int ob_tree_copy_order(ob_solver *solver, uint64_t *codes, uint32_t *indices, do
 int ob_morton_order_noalloc(uint64_t n, const double *x, const double *y, const double *z,
                             uint64_t *codes, uint32_t *indices, void *stream);
 
-/* Tile shape of the direct kernels: threads per CTA, targets per thread and
- * the number of CTAs (one thread-block cluster) that split the sources of a
- * target tile. No reference counterpart: the reference picks one block size
+/* Tile shape of the direct kernels: threads per CTA, targets per thread, the
+ * number of CTAs (one thread-block cluster) that split the sources of a
+ * target tile, and the number of thread groups of a CTA that split each
+ * staged tile's sources (each group serves the CTA's targets; 0 reads as 1).
+ * A CTA holds threads * targets_per_thread / groups targets. No reference
+ * counterpart: the reference picks one block size
  * (src/solvers/cuda_direct_solver.cpp:46-63). */
 typedef struct ob_direct_shape {
     int32_t threads;
     int32_t targets_per_thread;
     int32_t split;
-    int32_t reserved;
+    int32_t groups;
 } ob_direct_shape;
 
 /* Lists the shapes the library implements for a precision (FP32 or SPLIT);

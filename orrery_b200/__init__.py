@@ -68,7 +68,7 @@ class Counts(C.Structure):
 
 class DirectShape(C.Structure):
     _fields_ = [("threads", C.c_int32), ("targets_per_thread", C.c_int32),
-                ("split", C.c_int32), ("reserved", C.c_int32)]
+                ("split", C.c_int32), ("groups", C.c_int32)]
 
 
 class BatchShape(C.Structure):
@@ -317,8 +317,13 @@ class _Solver:
         _check(self._lib.ob_solver_reset_counts(self._handle))
 
     def set_shape(self, n: int, shape) -> None:
-        """Fixes the direct kernel shape (threads, targets_per_thread, split) for n."""
-        s = DirectShape(*shape, 0) if not isinstance(shape, DirectShape) else shape
+        """Fixes the direct kernel shape (threads, targets_per_thread, split[, groups])
+        for n; groups defaults to 1."""
+        if isinstance(shape, DirectShape):
+            s = shape
+        else:
+            t = tuple(shape)
+            s = DirectShape(*(t + (1,) * (4 - len(t))))
         _check(self._lib.ob_solver_set_direct_shape(self._handle, int(n), C.byref(s)))
 
     def autotune(self, n: int):
@@ -326,7 +331,7 @@ class _Solver:
         s = DirectShape()
         ms = C.c_double()
         _check(self._lib.ob_solver_autotune(self._handle, int(n), C.byref(s), C.byref(ms)))
-        return (s.threads, s.targets_per_thread, s.split), ms.value
+        return (s.threads, s.targets_per_thread, s.split, s.groups), ms.value
 
     def timings(self) -> dict:
         t = Timings()
@@ -405,13 +410,13 @@ class B200TreeSolver(_Solver):
 
 
 def direct_shapes(precision: str = "fp32"):
-    """Every (threads, targets_per_thread, split) shape of a direct kernel."""
+    """Every (threads, targets_per_thread, split, groups) shape of a direct kernel."""
     lib = load_library()
     count = C.c_int32()
     _check(lib.ob_direct_shapes(_PRECISIONS[precision], None, 0, C.byref(count)))
     arr = (DirectShape * count.value)()
     _check(lib.ob_direct_shapes(_PRECISIONS[precision], arr, count.value, C.byref(count)))
-    return [(s.threads, s.targets_per_thread, s.split) for s in arr]
+    return [(s.threads, s.targets_per_thread, s.split, s.groups) for s in arr]
 
 
 def _split_xyz(positions):
@@ -508,7 +513,7 @@ class DeviceSystem:
         s = DirectShape()
         ms = C.c_double()
         _check(self._lib.ob_system_autotune(self._handle, C.byref(s), C.byref(ms)))
-        return (s.threads, s.targets_per_thread, s.split), ms.value
+        return (s.threads, s.targets_per_thread, s.split, s.groups), ms.value
 
     def stream(self) -> int:
         """The cudaStream_t (as an integer) the system enqueues its work on."""

@@ -527,10 +527,11 @@ int ob_direct_shapes(int32_t precision, ob_direct_shape *out, int32_t capacity, 
         require(count != nullptr, "count is NULL");
         require(precision == OB_PRECISION_FP32 || precision == OB_PRECISION_SPLIT,
                 "shapes exist for the FP32 and split direct kernels");
-        ob::DirectConfig all[64];
-        const int total = ob::direct_candidates(precision == OB_PRECISION_SPLIT, all, 64);
+        ob::DirectConfig all[128];
+        const int total = ob::direct_candidates(precision == OB_PRECISION_SPLIT, all, 128);
         for (int k = 0; k < total && k < capacity && out != nullptr; ++k) {
-            out[k] = ob_direct_shape{all[k].threads, all[k].targets_per_thread, all[k].split, 0};
+            out[k] = ob_direct_shape{all[k].threads, all[k].targets_per_thread, all[k].split,
+                                     all[k].groups};
         }
         *count = total;
     });
@@ -543,18 +544,19 @@ int ob_solver_set_direct_shape(ob_solver *solver, uint64_t n, const ob_direct_sh
         const ob_solver_params &p = solver->impl->params();
         require(p.kind == OB_SOLVER_DIRECT && p.precision != OB_PRECISION_FP64,
                 "only the FP32 and split direct kernels have shapes");
-        ob::DirectConfig all[64];
-        const int total = ob::direct_candidates(p.precision == OB_PRECISION_SPLIT, all, 64);
+        const int groups = shape->groups == 0 ? 1 : shape->groups;
+        ob::DirectConfig all[128];
+        const int total = ob::direct_candidates(p.precision == OB_PRECISION_SPLIT, all, 128);
         bool known = false;
         for (int k = 0; k < total; ++k) {
             known = known || (all[k].threads == shape->threads &&
                               all[k].targets_per_thread == shape->targets_per_thread &&
-                              all[k].split == shape->split);
+                              all[k].split == shape->split && all[k].groups == groups);
         }
         require(known, "the library implements no such direct kernel shape");
         solver->impl->set_direct_config(
             static_cast<uint32_t>(n),
-            ob::DirectConfig{shape->threads, shape->targets_per_thread, shape->split});
+            ob::DirectConfig{shape->threads, shape->targets_per_thread, shape->split, groups});
     });
 }
 
@@ -565,7 +567,7 @@ int ob_solver_autotune(ob_solver *solver, uint64_t n, ob_direct_shape *chosen, d
         ob::DirectConfig c;
         const double ms = solver->impl->autotune(static_cast<uint32_t>(n), c);
         if (chosen != nullptr) {
-            *chosen = ob_direct_shape{c.threads, c.targets_per_thread, c.split, 0};
+            *chosen = ob_direct_shape{c.threads, c.targets_per_thread, c.split, c.groups};
         }
         if (best_ms != nullptr) {
             *best_ms = ms;
@@ -665,7 +667,7 @@ int ob_system_autotune(ob_system *system, ob_direct_shape *chosen, double *best_
         ob::DirectConfig c;
         const double ms = system->impl->solver().autotune(system->impl->size(), c);
         if (chosen != nullptr) {
-            *chosen = ob_direct_shape{c.threads, c.targets_per_thread, c.split, 0};
+            *chosen = ob_direct_shape{c.threads, c.targets_per_thread, c.split, c.groups};
         }
         if (best_ms != nullptr) {
             *best_ms = ms;

@@ -15,13 +15,15 @@
 //     double-buffered so the next tile lands while this one is summed;
 //   * every thread reads the same source at the same time, so each float4 read
 //     is a shared-memory broadcast amortised over the R targets of the thread;
-//   * tiles that contain no target of the CTA and no padding run a branch-free
-//     loop; the few that do select zero mass for j == i and j >= n, as the
-//     reference kernel masks (cuda_direct_kernel.cu:155-160);
+//   * tiles run a branch-free loop; with softening the target's own entry and
+//     the zero-mass padding add exactly zero (self_term_vanishes), and
+//     without it the tiles that hold them select zero mass for j == i and
+//     j >= n, as the reference kernel masks (cuda_direct_kernel.cu:155-160);
 //   * when the targets alone cannot fill 148 SMs, S CTAs of one thread-block
 //     cluster split the source range and their partial sums are reduced through
 //     distributed shared memory in a fixed rank order (deterministic).
 #include <cooperative_groups.h>
+#include <type_traits>
 
 #include "common.cuh"
 #include "internal.hpp"
@@ -68,16 +70,52 @@ __device__ __forceinline__ void stage_tile(const DirectArgs &a, float4 *tiles_hi
     }
 }
 
+// Sources per unrolled step of the tile loop: a thread with a single target
+// pair (the shapes for small systems, few warps per SM) gets more independent
+// chains to overlap.
+template <int P> constexpr int kSourceUnroll = P == 1 ? 4 : 2;
+
+// Tiles holding the CTA's own targets or padding need no masks when those
+// entries add exactly zero. A target's own entry is its packed position, so
+// d = 0 exactly and r2 = eps2, and its term is f * 0 = 0 whenever
+// f = (m y)(y y) at r2 = eps2 is finite; padded entries (zero mass, at the
+// origin) have r2 >= eps2 and give (0 y)(y y) = 0. The masked loop adds f = 0
+// for the same entries in the same order, so both loops give the same sums.
+// `f_self` is that f for one target, computed as the loop computes it.
+__device__ __forceinline__ bool self_term_vanishes(float eps2, float f_self) {
+    return eps2 >= 1.17549435e-38f && isfinite(f_self); // eps2 normal: no flush to zero
+}
+
+// Source groups. With K > 1 the threads of a CTA form K groups of TP =
+// THREADS / K: thread tid serves target lane tid % TP over the sources of
+// slice tid / TP of every tile (kDirectTile / K consecutive sources), so a
+// small system gets K times the warps. The K partial sums of a target are
+// added in slice order, so the result does not depend on scheduling.
+template <int THREADS, int K> struct SourceGroups {
+    static_assert(THREADS % K == 0 && (THREADS / K) % 32 == 0, "groups are whole warps");
+    static_assert(kDirectTile % K == 0, "a tile splits evenly");
+    static constexpr uint32_t lanes = THREADS / K;       // target lanes per group
+    static constexpr uint32_t sources = kDirectTile / K; // sources per slice of a tile
+};
+
+// Shared-memory type of the CTA's per-target sums: FP32 sums pass through
+// exactly as float when a CTA has one group; group sums are FP64.
+template <int K, typename T> using PartialType = std::conditional_t<K == 1, T, double>;
+
 // Writes the CTA's per-target sums, reducing across the cluster when split.
-// `partial` holds 3*BT values of type T laid out [component][slot].
-template <int THREADS, int R, typename T>
+// `partial` holds 3*BT values of type T laid out [component][slot] (K*3*BT
+// doubles, one block per group, when K > 1). Target slot r*TP + lane.
+template <int THREADS, int R, int K, typename T>
 __device__ __forceinline__ void finish_targets(const DirectArgs &a, uint32_t t0, T *partial,
                                                const double (&sx)[R], const double (&sy)[R],
                                                const double (&sz)[R]) {
-    constexpr uint32_t BT = THREADS * R;
+    constexpr uint32_t TP = SourceGroups<THREADS, K>::lanes;
+    constexpr uint32_t BT = TP * R;
     const uint32_t split = gridDim.x;
     const uint32_t tid = threadIdx.x;
-    if (split == 1) {
+    const uint32_t lane = tid % TP;
+    const uint32_t group = tid / TP;
+    if (K == 1 && split == 1) {
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const uint32_t i = t0 + r * THREADS + tid;
@@ -89,12 +127,50 @@ __device__ __forceinline__ void finish_targets(const DirectArgs &a, uint32_t t0,
         }
         return;
     }
+    if constexpr (K == 1) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) {
-        const uint32_t slot = r * THREADS + tid;
-        partial[slot] = static_cast<T>(sx[r]);
-        partial[BT + slot] = static_cast<T>(sy[r]);
-        partial[2 * BT + slot] = static_cast<T>(sz[r]);
+        for (int r = 0; r < R; ++r) {
+            const uint32_t slot = r * THREADS + tid;
+            partial[slot] = static_cast<T>(sx[r]);
+            partial[BT + slot] = static_cast<T>(sy[r]);
+            partial[2 * BT + slot] = static_cast<T>(sz[r]);
+        }
+    } else {
+        static_assert(sizeof(T) == sizeof(double), "group sums are FP64");
+        // Each group's sums in its own block, then added in group order into
+        // block 0 (each slot by one thread, which reads every group's value of
+        // a component before it overwrites block 0's).
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const uint32_t slot = r * TP + lane;
+            partial[(group * 3 + 0) * BT + slot] = sx[r];
+            partial[(group * 3 + 1) * BT + slot] = sy[r];
+            partial[(group * 3 + 2) * BT + slot] = sz[r];
+        }
+        __syncthreads();
+        for (uint32_t slot = tid; slot < BT; slot += THREADS) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                double s = 0.0;
+#pragma unroll
+                for (int g = 0; g < K; ++g) {
+                    s += partial[(g * 3 + c) * BT + slot];
+                }
+                partial[c * BT + slot] = s;
+            }
+        }
+        __syncthreads();
+        if (split == 1) {
+            for (uint32_t slot = tid; slot < BT; slot += THREADS) {
+                const uint32_t i = t0 + slot;
+                if (i < a.n) {
+                    a.ax[i] = partial[slot];
+                    a.ay[i] = partial[BT + slot];
+                    a.az[i] = partial[2 * BT + slot];
+                }
+            }
+            return;
+        }
     }
     cg::cluster_group cluster = cg::this_cluster();
     cluster.sync();
@@ -122,32 +198,43 @@ __device__ __forceinline__ void finish_targets(const DirectArgs &a, uint32_t t0,
 // Sources of the FP32 kernel are stored pre-duplicated, two float4 per
 // particle: (x, x, y, y) and (z, z, m, m), so that each half is already a
 // packed FP32x2 operand for a pair of targets and no register moves are needed.
-template <int THREADS, int R>
+template <int THREADS, int R, int K>
 __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a) {
     static_assert(R % 2 == 0, "targets are processed in packed pairs");
     constexpr int P = R / 2;
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr uint32_t BT = THREADS * R;
+    constexpr uint32_t TP = SourceGroups<THREADS, K>::lanes;
+    constexpr uint32_t JS = SourceGroups<THREADS, K>::sources;
+    constexpr uint32_t BT = TP * R;
+    using PT = PartialType<K, float>;
     float4 *tiles = reinterpret_cast<float4 *>(smem); // 2 buffers x 2*kDirectTile
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + 4 * kDirectTile * sizeof(float4));
-    float *partial = reinterpret_cast<float *>(bars + 2);
+    PT *partial = reinterpret_cast<PT *>(bars + 2);
 
     const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid % TP;
+    const uint32_t jb = (tid / TP) * JS; // this thread's slice of every tile
     const uint32_t t0 = blockIdx.y * BT;
     const float2 eps2 = make_float2(a.eps2, a.eps2);
 
-    // Target r = 2p + h is slot (2p + h) * THREADS + tid; pair p packs h = 0, 1.
+    // Target r = 2p + h is slot (2p + h) * TP + lane; pair p packs h = 0, 1.
     float2 nx[P], ny[P], nz[P], ax[P], ay[P], az[P];
+    const float y_self = rsqrt_approx(a.eps2);
+    bool vanish = true;
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-        const float4 u0 = a.hi[2ull * (t0 + (2 * p) * THREADS + tid)];
-        const float4 u1 = a.hi[2ull * (t0 + (2 * p) * THREADS + tid) + 1];
-        const float4 v0 = a.hi[2ull * (t0 + (2 * p + 1) * THREADS + tid)];
-        const float4 v1 = a.hi[2ull * (t0 + (2 * p + 1) * THREADS + tid) + 1];
+        const float4 u0 = a.hi[2ull * (t0 + (2 * p) * TP + lane)];
+        const float4 u1 = a.hi[2ull * (t0 + (2 * p) * TP + lane) + 1];
+        const float4 v0 = a.hi[2ull * (t0 + (2 * p + 1) * TP + lane)];
+        const float4 v1 = a.hi[2ull * (t0 + (2 * p + 1) * TP + lane) + 1];
         nx[p] = make_float2(-u0.x, -v0.x);
         ny[p] = make_float2(-u0.z, -v0.z);
         nz[p] = make_float2(-u1.x, -v1.x);
         ax[p] = ay[p] = az[p] = make_float2(0.0f, 0.0f);
+        const float2 ys = make_float2(y_self, y_self);
+        const float2 f_self = __fmul2_rn(__fmul2_rn(make_float2(u1.z, v1.z), ys), __fmul2_rn(ys, ys));
+        vanish = vanish && self_term_vanishes(a.eps2, f_self.x) &&
+                 self_term_vanishes(a.eps2, f_self.y);
     }
 
     uint32_t tb, te;
@@ -157,7 +244,7 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
         mbar_init(&bars[1], 1);
         fence_barrier_init();
     }
-    __syncthreads();
+    const bool unmasked = __syncthreads_and(vanish ? 1 : 0) != 0;
     constexpr uint32_t tile_bytes = 2 * kDirectTile * sizeof(float4);
     auto stage = [&](uint32_t k, uint32_t buf) {
         mbar_arrive_expect_tx(&bars[buf], tile_bytes);
@@ -180,10 +267,11 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
         if (ok) {
             const float4 *tile = tiles + buf * 2 * kDirectTile;
             const uint32_t j0 = k * kDirectTile;
-            const bool masked = (j0 + kDirectTile > a.n) || (j0 < t0 + BT && t0 < j0 + kDirectTile);
+            const bool masked = !unmasked && ((j0 + kDirectTile > a.n) ||
+                                              (j0 < t0 + BT && t0 < j0 + kDirectTile));
             if (!masked) {
-#pragma unroll 2
-                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+#pragma unroll(kSourceUnroll<P>)
+                for (uint32_t jj = jb; jj < jb + JS; ++jj) {
                     const float4 s0 = tile[2 * jj];     // (x, x, y, y)
                     const float4 s1 = tile[2 * jj + 1]; // (z, z, m, m)
                     const float2 sx = make_float2(s0.x, s0.y);
@@ -206,14 +294,14 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
                     }
                 }
             } else {
-                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                for (uint32_t jj = jb; jj < jb + JS; ++jj) {
                     const float4 s0 = tile[2 * jj];
                     const float4 s1 = tile[2 * jj + 1];
                     const uint32_t j = j0 + jj;
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
-                        const uint32_t i0 = t0 + (2 * p) * THREADS + tid;
-                        const uint32_t i1 = i0 + THREADS;
+                        const uint32_t i0 = t0 + (2 * p) * TP + lane;
+                        const uint32_t i1 = i0 + TP;
                         const bool skip0 = (j == i0) || (j >= a.n);
                         const bool skip1 = (j == i1) || (j >= a.n);
                         const float2 dx = __fadd2_rn(make_float2(s0.x, s0.y), nx[p]);
@@ -251,33 +339,43 @@ __global__ void __launch_bounds__(THREADS) direct_f32_kernel(const DirectArgs a)
         sz[2 * p] = az[p].x;
         sz[2 * p + 1] = az[p].y;
     }
-    finish_targets<THREADS, R, float>(a, t0, partial, sx, sy, sz);
+    finish_targets<THREADS, R, K, PT>(a, t0, partial, sx, sy, sz);
 }
 
 // Split (precision) form: targets r = 2p + h are packed in pairs p and every
 // operation is an FP32x2 instruction (split_math.cuh). Tiles carry 512 sources
 // of hi and lo parts (64 bytes per source).
-template <int THREADS, int R>
+template <int THREADS, int R, int K>
 __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs a) {
     static_assert(R % 2 == 0, "targets are processed in packed pairs");
     constexpr int P = R / 2;
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr uint32_t BT = THREADS * R;
+    constexpr uint32_t TP = SourceGroups<THREADS, K>::lanes;
+    constexpr uint32_t JS = SourceGroups<THREADS, K>::sources;
+    constexpr uint32_t BT = TP * R;
     float4 *tiles_hi = reinterpret_cast<float4 *>(smem);     // 2 buffers x 2*kDirectTile
     float4 *tiles_lo = tiles_hi + 4 * kDirectTile;           // 2 buffers x 2*kDirectTile
     uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 4 * kDirectTile);
     double *partial = reinterpret_cast<double *>(bars + 2);
 
     const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid % TP;
+    const uint32_t jb = (tid / TP) * JS; // this thread's slice of every tile
     const uint32_t t0 = blockIdx.y * BT;
     const float2 eps2 = make_float2(a.eps2, a.eps2);
 
     SplitTargets tg[P];
     double sx[R], sy[R], sz[R];
+    const float2 y_self = refined_rsqrt2(eps2);
+    bool vanish = true;
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-        const size_t i0 = t0 + (2 * p) * THREADS + tid;
-        tg[p] = load_split_targets(a.hi, a.lo, i0, i0 + THREADS);
+        const size_t i0 = t0 + (2 * p) * TP + lane;
+        tg[p] = load_split_targets(a.hi, a.lo, i0, i0 + TP);
+        const float2 m = make_float2(a.hi[2 * i0 + 1].z, a.hi[2 * (i0 + TP) + 1].z);
+        const float2 f_self = __fmul2_rn(__fmul2_rn(m, y_self), __fmul2_rn(y_self, y_self));
+        vanish = vanish && self_term_vanishes(a.eps2, f_self.x) &&
+                 self_term_vanishes(a.eps2, f_self.y);
     }
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -291,7 +389,7 @@ __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs 
         mbar_init(&bars[1], 1);
         fence_barrier_init();
     }
-    __syncthreads();
+    const bool unmasked = __syncthreads_and(vanish ? 1 : 0) != 0;
     constexpr uint32_t tile_bytes = 2 * kDirectTile * sizeof(float4);
     auto stage = [&](uint32_t k, uint32_t buf) {
         mbar_arrive_expect_tx(&bars[buf], 2 * tile_bytes);
@@ -316,15 +414,16 @@ __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs 
             const float4 *th = tiles_hi + buf * 2 * kDirectTile;
             const float4 *tl = tiles_lo + buf * 2 * kDirectTile;
             const uint32_t j0 = k * kDirectTile;
-            const bool masked = (j0 + kDirectTile > a.n) || (j0 < t0 + BT && t0 < j0 + kDirectTile);
+            const bool masked = !unmasked && ((j0 + kDirectTile > a.n) ||
+                                              (j0 < t0 + BT && t0 < j0 + kDirectTile));
             float2 kx[P], ky[P], kz[P], cx[P], cy[P], cz[P];
 #pragma unroll
             for (int p = 0; p < P; ++p) {
                 kx[p] = ky[p] = kz[p] = cx[p] = cy[p] = cz[p] = make_float2(0.0f, 0.0f);
             }
             if (!masked) {
-#pragma unroll 2
-                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+#pragma unroll(kSourceUnroll<P>)
+                for (uint32_t jj = jb; jj < jb + JS; ++jj) {
                     const float4 h0 = th[2 * jj], h1 = th[2 * jj + 1];
                     const float4 l0 = tl[2 * jj], l1 = tl[2 * jj + 1];
 #pragma unroll
@@ -341,15 +440,15 @@ __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs 
                     }
                 }
             } else {
-                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                for (uint32_t jj = jb; jj < jb + JS; ++jj) {
                     const float4 h0 = th[2 * jj], h1 = th[2 * jj + 1];
                     const float4 l0 = tl[2 * jj], l1 = tl[2 * jj + 1];
                     const uint32_t j = j0 + jj;
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
-                        const uint32_t i0 = t0 + (2 * p) * THREADS + tid;
+                        const uint32_t i0 = t0 + (2 * p) * TP + lane;
                         const bool skip0 = (j == i0) || (j >= a.n);
-                        const bool skip1 = (j == i0 + THREADS) || (j >= a.n);
+                        const bool skip1 = (j == i0 + TP) || (j >= a.n);
                         float2 dx, dy, dz;
                         split_offsets(tg[p], h0, h1, l0, l1, dx, dy, dz);
                         float2 r2 =
@@ -381,7 +480,7 @@ __global__ void __launch_bounds__(THREADS) direct_split_kernel(const DirectArgs 
             stage(k + 2, buf);
         }
     }
-    finish_targets<THREADS, R, double>(a, t0, partial, sx, sy, sz);
+    finish_targets<THREADS, R, K, double>(a, t0, partial, sx, sy, sz);
 }
 
 // FP64 direct sum in the order of accumulate_range_scalar
@@ -472,26 +571,28 @@ __global__ void pack_kernel(const double *__restrict__ x, const double *__restri
     }
 }
 
-template <int THREADS, int R, bool SPLIT> size_t direct_smem_bytes() {
+template <int THREADS, int R, int K, bool SPLIT> size_t direct_smem_bytes() {
     const size_t tiles = (SPLIT ? 8 : 4) * kDirectTile * sizeof(float4);
-    const size_t partial = 3 * THREADS * R * (SPLIT ? sizeof(double) : sizeof(float));
+    // 3 sums per target: THREADS * R / K targets, one block per group.
+    const size_t partial =
+        3 * THREADS * R * (SPLIT ? sizeof(double) : sizeof(PartialType<K, float>));
     return tiles + 2 * sizeof(uint64_t) + partial;
 }
 
-template <int THREADS, int R, bool SPLIT> auto direct_kernel_for() {
+template <int THREADS, int R, int K, bool SPLIT> auto direct_kernel_for() {
     if constexpr (SPLIT) {
-        return direct_split_kernel<THREADS, R>;
+        return direct_split_kernel<THREADS, R, K>;
     } else {
-        return direct_f32_kernel<THREADS, R>;
+        return direct_f32_kernel<THREADS, R, K>;
     }
 }
 
-template <int THREADS, int R, bool SPLIT>
+template <int THREADS, int R, int K, bool SPLIT>
 cudaError_t launch_direct_t(const DirectArgs &args, int split, cudaStream_t stream) {
-    const uint32_t bt = THREADS * R;
+    const uint32_t bt = SourceGroups<THREADS, K>::lanes * R;
     const dim3 grid(static_cast<unsigned>(split), ceil_div(args.n, bt), 1);
-    const size_t smem = direct_smem_bytes<THREADS, R, SPLIT>();
-    auto kernel = direct_kernel_for<THREADS, R, SPLIT>();
+    const size_t smem = direct_smem_bytes<THREADS, R, K, SPLIT>();
+    auto kernel = direct_kernel_for<THREADS, R, K, SPLIT>();
     // Set once per process (one process drives one device), before any graph
     // capture reaches this launch.
     static const cudaError_t configured = cudaFuncSetAttribute(
@@ -516,18 +617,24 @@ cudaError_t launch_direct_t(const DirectArgs &args, int split, cudaStream_t stre
 
 template <bool SPLIT>
 cudaError_t dispatch_direct(const DirectArgs &args, const DirectConfig &c, cudaStream_t stream) {
-#define OB_DIRECT_CASE(T, RR)                                                                      \
-    if (c.threads == T && c.targets_per_thread == RR)                                              \
-        return launch_direct_t<T, RR, SPLIT>(args, c.split, stream);
-    OB_DIRECT_CASE(64, 2)
-    OB_DIRECT_CASE(64, 4)
-    OB_DIRECT_CASE(128, 2)
-    OB_DIRECT_CASE(128, 4)
-    OB_DIRECT_CASE(256, 2)
-    OB_DIRECT_CASE(256, 4)
+#define OB_DIRECT_CASE(T, RR, KK)                                                                  \
+    if (c.threads == T && c.targets_per_thread == RR && c.groups == KK)                            \
+        return launch_direct_t<T, RR, KK, SPLIT>(args, c.split, stream);
+    OB_DIRECT_CASE(64, 2, 1)
+    OB_DIRECT_CASE(64, 4, 1)
+    OB_DIRECT_CASE(128, 2, 1)
+    OB_DIRECT_CASE(128, 4, 1)
+    OB_DIRECT_CASE(256, 2, 1)
+    OB_DIRECT_CASE(256, 4, 1)
+    OB_DIRECT_CASE(128, 2, 2)
+    OB_DIRECT_CASE(128, 2, 4)
+    OB_DIRECT_CASE(256, 2, 4)
+    OB_DIRECT_CASE(256, 2, 8)
+    OB_DIRECT_CASE(256, 4, 4)
+    OB_DIRECT_CASE(256, 4, 8)
     if constexpr (!SPLIT) {
-        OB_DIRECT_CASE(128, 8)
-        OB_DIRECT_CASE(256, 8)
+        OB_DIRECT_CASE(128, 8, 1)
+        OB_DIRECT_CASE(256, 8, 1)
     }
 #undef OB_DIRECT_CASE
     return cudaErrorInvalidValue;
@@ -538,7 +645,8 @@ bool valid_split(int split) { return split == 1 || split == 2 || split == 4 || s
 } // namespace
 
 uint32_t direct_padded_count(uint32_t n, const DirectConfig &config) {
-    const uint32_t bt = static_cast<uint32_t>(config.threads * config.targets_per_thread);
+    const uint32_t bt =
+        static_cast<uint32_t>(config.threads * config.targets_per_thread / config.groups);
     const uint32_t unit = bt > kDirectTile ? bt : kDirectTile;
     const uint32_t padded = ceil_div(n, unit) * unit;
     return padded == 0 ? unit : padded;
@@ -595,20 +703,24 @@ cudaError_t launch_direct_f64(const double *x, const double *y, const double *z,
 }
 
 int direct_candidates(bool split, DirectConfig *out, int capacity) {
-    // 64-thread CTAs give small systems (a few thousand particles) enough
-    // CTAs to occupy the SMs.
-    static const int split_shapes[][2] = {{64, 2},  {64, 4},  {128, 2},
-                                          {128, 4}, {256, 2}, {256, 4}};
-    static const int fp32_shapes[][2] = {{64, 2},  {64, 4},  {128, 2}, {128, 4},
-                                         {128, 8}, {256, 2}, {256, 4}, {256, 8}};
-    const int(*shapes)[2] = split ? split_shapes : fp32_shapes;
-    const int shape_count = split ? 6 : 8;
+    // (threads, targets per thread, source groups). 64-thread CTAs and source
+    // groups give small systems (a few thousand particles) enough warps to
+    // occupy the SMs.
+    static const int split_shapes[][3] = {{64, 2, 1},  {64, 4, 1},  {128, 2, 1}, {128, 4, 1},
+                                          {256, 2, 1}, {256, 4, 1}, {128, 2, 2}, {128, 2, 4},
+                                          {256, 2, 4}, {256, 2, 8}, {256, 4, 4}, {256, 4, 8}};
+    static const int fp32_shapes[][3] = {{64, 2, 1},  {64, 4, 1},  {128, 2, 1}, {128, 4, 1},
+                                         {128, 8, 1}, {256, 2, 1}, {256, 4, 1}, {256, 8, 1},
+                                         {128, 2, 2}, {128, 2, 4}, {256, 2, 4}, {256, 2, 8},
+                                         {256, 4, 4}, {256, 4, 8}};
+    const int(*shapes)[3] = split ? split_shapes : fp32_shapes;
+    const int shape_count = split ? 12 : 14;
     static const int splits[] = {1, 2, 4, 8};
     int count = 0;
     for (int s = 0; s < shape_count; ++s) {
         for (int k = 0; k < 4; ++k) {
             if (count < capacity) {
-                out[count] = DirectConfig{shapes[s][0], shapes[s][1], splits[k]};
+                out[count] = DirectConfig{shapes[s][0], shapes[s][1], splits[k], shapes[s][2]};
             }
             ++count;
         }

@@ -15,6 +15,7 @@ struct DirectConfig {
     int threads = 256;
     int targets_per_thread = 4;
     int split = 1;
+    int groups = 1; // thread groups of a CTA that split each tile's sources
 };
 
 // Source particles per staged shared-memory tile.

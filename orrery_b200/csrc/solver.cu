@@ -183,13 +183,13 @@ double Solver::autotune(uint32_t n, DirectConfig &chosen) {
     check(cudaMemcpyAsync(dev.data(), host.data(), sizeof(double) * 4ull * n,
                           cudaMemcpyHostToDevice, stream_),
           "uploading autotune sources");
-    DirectConfig candidates[64];
-    const int count = direct_candidates(split, candidates, 64);
+    DirectConfig candidates[128];
+    const int count = direct_candidates(split, candidates, 128);
     const auto eps2 = static_cast<float>(params_.softening_squared + 1e-6);
     double best = 1e300;
     const double *d = dev.data();
     double *out = dev.data() + 4ull * n;
-    for (int k = 0; k < count && k < 64; ++k) {
+    for (int k = 0; k < count && k < 128; ++k) {
         const DirectConfig c = candidates[k];
         if (static_cast<uint32_t>(c.split) > ceil_div(n, kDirectTile)) {
             continue;
