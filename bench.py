@@ -611,7 +611,7 @@ def run_batch(args, w):
                        "precision": "split", "integrator": "yoshida4", "dt": w["dt"],
                        "softening": "0.01 x scale radius", "work_items": items,
                        "autotuned_shape": {"threads": shape[0], "targets_per_thread": shape[1],
-                                           "chunk_tiles": shape[2]},
+                                           "chunk_tiles": shape[2], "groups": shape[3]},
                        "l2": "inputs larger than L2"},
             "roofline": {"bound": "fp32-fma-pipe", "achieved": achieved, "peak": peak,
                          "unit": "Gint/s", "frac": achieved / peak,

@@ -270,7 +270,7 @@ typedef struct ob_batch_shape {
     int32_t threads;
     int32_t targets_per_thread;
     uint32_t chunk_tiles; /* 512-source tiles per work item; 0 = a whole system */
-    int32_t reserved;
+    int32_t groups;       /* thread groups splitting each tile's sources; 0 reads as 1 */
 } ob_batch_shape;
 
 int ob_batch_create(uint32_t systems, const uint64_t *counts, const double *softening_squared,

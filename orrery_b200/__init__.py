@@ -73,7 +73,7 @@ class DirectShape(C.Structure):
 
 class BatchShape(C.Structure):
     _fields_ = [("threads", C.c_int32), ("targets_per_thread", C.c_int32),
-                ("chunk_tiles", C.c_uint32), ("reserved", C.c_int32)]
+                ("chunk_tiles", C.c_uint32), ("groups", C.c_int32)]
 
 
 class ServerConfig(C.Structure):
@@ -614,10 +614,10 @@ class DeviceBatch:
         s = BatchShape()
         ms = C.c_double()
         _check(self._lib.ob_batch_autotune(self._handle, C.byref(s), C.byref(ms)))
-        return (s.threads, s.targets_per_thread, s.chunk_tiles), ms.value
+        return (s.threads, s.targets_per_thread, s.chunk_tiles, s.groups), ms.value
 
-    def set_shape(self, threads, targets_per_thread, chunk_tiles) -> None:
-        s = BatchShape(threads, targets_per_thread, chunk_tiles, 0)
+    def set_shape(self, threads, targets_per_thread, chunk_tiles, groups=1) -> None:
+        s = BatchShape(threads, targets_per_thread, chunk_tiles, groups)
         _check(self._lib.ob_batch_set_shape(self._handle, C.byref(s)))
 
     def stats(self):

@@ -39,18 +39,30 @@ struct BatchArgs {
 };
 
 // Targets r = 2p + h of a thread are packed in pairs p; the arithmetic is
-// the split form's, in FP32x2 instructions (split_math.cuh).
-template <int THREADS, int R>
+// the split form's, in FP32x2 instructions (split_math.cuh). With K source
+// groups the CTA's threads form K groups of TP = THREADS / K: thread tid
+// serves target lane tid % TP over slice tid / TP of every tile
+// (kDirectTile / K sources), and the K partial sums of a target are added in
+// slice order before they are written.
+template <int THREADS, int R, int K>
 __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a) {
     static_assert(R % 2 == 0, "targets are processed in packed pairs");
+    static_assert(THREADS % K == 0 && (THREADS / K) % 32 == 0, "groups are whole warps");
+    static_assert(kDirectTile % K == 0, "a tile splits evenly");
     constexpr int P = R / 2;
+    constexpr uint32_t TP = THREADS / K;
+    constexpr uint32_t JS = kDirectTile / K;
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr uint32_t BT = THREADS * R;
+    constexpr uint32_t BT = TP * R;
     float4 *tiles_hi = reinterpret_cast<float4 *>(smem);   // 2 buffers x 2*kDirectTile
     float4 *tiles_lo = tiles_hi + 4 * kDirectTile;         // 2 buffers x 2*kDirectTile
     uint64_t *bars = reinterpret_cast<uint64_t *>(tiles_lo + 4 * kDirectTile);
+    double *group_sums = reinterpret_cast<double *>(bars + 2); // K x 3 x BT when K > 1
     __shared__ uint32_t s_item;
     const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid % TP;
+    const uint32_t group = tid / TP;
+    const uint32_t jb = group * JS; // this thread's slice of every tile
     if (tid == 0) {
         mbar_init(&bars[0], 1);
         mbar_init(&bars[1], 1);
@@ -83,8 +95,8 @@ __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a)
         double sx[R], sy[R], sz[R];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            const size_t i0 = item.target_begin + (2 * p) * THREADS + tid;
-            tg[p] = load_split_targets(a.hi, a.lo, i0, i0 + THREADS);
+            const size_t i0 = item.target_begin + (2 * p) * TP + lane;
+            tg[p] = load_split_targets(a.hi, a.lo, i0, i0 + TP);
         }
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -112,7 +124,7 @@ __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a)
                     kx[p] = ky[p] = kz[p] = cx[p] = cy[p] = cz[p] = make_float2(0.0f, 0.0f);
                 }
 #pragma unroll 2
-                for (uint32_t jj = 0; jj < kDirectTile; ++jj) {
+                for (uint32_t jj = jb; jj < jb + JS; ++jj) {
                     const float4 h0 = th[2 * jj], h1 = th[2 * jj + 1];
                     const float4 l0 = tl[2 * jj], l1 = tl[2 * jj + 1];
 #pragma unroll
@@ -145,22 +157,48 @@ __global__ void __launch_bounds__(THREADS) batch_split_kernel(const BatchArgs a)
             }
         }
         sequence += tiles;
-#pragma unroll
-        for (int r = 0; r < R; ++r) {
-            const uint32_t slot = r * THREADS + tid;
+        auto write = [&](uint32_t slot, double x, double y, double z) {
             if (slot < item.target_count) {
                 if (item.slot == kDirectWrite) {
                     const uint32_t i = item.target_begin + slot;
-                    a.ax[i] = sx[r];
-                    a.ay[i] = sy[r];
-                    a.az[i] = sz[r];
+                    a.ax[i] = x;
+                    a.ay[i] = y;
+                    a.az[i] = z;
                 } else {
                     double *p = a.partial + static_cast<size_t>(item.slot) * 3 * BT;
-                    p[slot] = sx[r];
-                    p[BT + slot] = sy[r];
-                    p[2 * BT + slot] = sz[r];
+                    p[slot] = x;
+                    p[BT + slot] = y;
+                    p[2 * BT + slot] = z;
                 }
             }
+        };
+        if constexpr (K == 1) {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                write(r * THREADS + tid, sx[r], sy[r], sz[r]);
+            }
+        } else {
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t slot = r * TP + lane;
+                group_sums[(group * 3 + 0) * BT + slot] = sx[r];
+                group_sums[(group * 3 + 1) * BT + slot] = sy[r];
+                group_sums[(group * 3 + 2) * BT + slot] = sz[r];
+            }
+            __syncthreads();
+            for (uint32_t slot = tid; slot < BT; slot += THREADS) {
+                double s[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+                for (int g = 0; g < K; ++g) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        s[c] += group_sums[(g * 3 + c) * BT + slot];
+                    }
+                }
+                write(slot, s[0], s[1], s[2]);
+            }
+            // The next item's group sums reuse the buffer after the barrier
+            // that follows.
         }
         if (!__syncthreads_and(ok ? 1 : 0)) {
             break;
@@ -188,10 +226,11 @@ __global__ void batch_reduce_kernel(const BatchGroup *__restrict__ groups, uint3
     }
 }
 
-template <int THREADS, int R>
+template <int THREADS, int R, int K>
 cudaError_t launch_batch_t(const BatchArgs &args, int sm_count, cudaStream_t stream) {
-    const size_t smem = 8 * kDirectTile * sizeof(float4) + 2 * sizeof(uint64_t);
-    auto kernel = batch_split_kernel<THREADS, R>;
+    const size_t smem = 8 * kDirectTile * sizeof(float4) + 2 * sizeof(uint64_t) +
+                        (K > 1 ? 3 * THREADS * R * sizeof(double) : 0);
+    auto kernel = batch_split_kernel<THREADS, R, K>;
     static const cudaError_t configured = cudaFuncSetAttribute(
         kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
     if (configured != cudaSuccess) {
@@ -221,13 +260,17 @@ cudaError_t launch_batch_forces(const float4 *hi, const float4 *lo, const float 
         return cudaSuccess;
     }
     const BatchArgs args{hi, lo, eps2, items, item_count, ax, ay, az, partial, queue, status};
-#define OB_BATCH_CASE(T, RR)                                                                       \
-    if (config.threads == T && config.targets_per_thread == RR)                                    \
-        return launch_batch_t<T, RR>(args, sm_count, stream);
-    OB_BATCH_CASE(128, 2)
-    OB_BATCH_CASE(128, 4)
-    OB_BATCH_CASE(256, 2)
-    OB_BATCH_CASE(256, 4)
+#define OB_BATCH_CASE(T, RR, KK)                                                                   \
+    if (config.threads == T && config.targets_per_thread == RR && config.groups == KK)             \
+        return launch_batch_t<T, RR, KK>(args, sm_count, stream);
+    OB_BATCH_CASE(128, 2, 1)
+    OB_BATCH_CASE(128, 4, 1)
+    OB_BATCH_CASE(256, 2, 1)
+    OB_BATCH_CASE(256, 4, 1)
+    OB_BATCH_CASE(128, 2, 4)
+    OB_BATCH_CASE(256, 2, 8)
+    OB_BATCH_CASE(256, 4, 4)
+    OB_BATCH_CASE(256, 4, 8)
 #undef OB_BATCH_CASE
     return cudaErrorInvalidValue;
 }
@@ -414,7 +457,7 @@ void Batch::remove(uint32_t id) {
 std::vector<BatchItem> Batch::make_items(const BatchConfig &config,
                                          const std::vector<uint32_t> &ids,
                                          std::vector<BatchGroup> &groups, uint32_t &slots) const {
-    const uint32_t bt = static_cast<uint32_t>(config.threads * config.targets_per_thread);
+    const uint32_t bt = config.targets_per_block();
     std::vector<BatchItem> items;
     for (const uint32_t s : ids) {
         const Member &m = members_[s];
@@ -449,7 +492,7 @@ std::vector<BatchItem> Batch::make_items(const BatchConfig &config,
 
 void Batch::upload_items(const std::vector<BatchItem> &items,
                          const std::vector<BatchGroup> &groups, uint32_t slots) {
-    const uint32_t bt = static_cast<uint32_t>(config_.threads * config_.targets_per_thread);
+    const uint32_t bt = config_.targets_per_block();
     const bool moved_items = items_.reserve(std::max<size_t>(1, items.size()));
     const bool moved_groups = groups_.reserve(std::max<size_t>(1, groups.size()));
     const bool moved_partial =
@@ -503,6 +546,16 @@ void Batch::set_state(uint32_t id, const double *x, const double *y, const doubl
         throw Error(OB_ERROR_INVALID_ARGUMENT, "positions and masses are required");
     }
     const Member &mb = members_[id];
+    // The kernel has no masks: a target's own entry enters its sum as f * 0
+    // with f = m / eps^3 in FP32, which is zero only while f is finite (the
+    // bound leaves room for the rounding of the device's 1 / eps).
+    const double inverse_cube = std::pow(mb.eps2, -1.5);
+    for (uint32_t i = 0; i < mb.count; ++i) {
+        if (!(std::fabs(m[i]) * inverse_cube < 1e37)) {
+            throw Error(OB_ERROR_INVALID_ARGUMENT,
+                        "a mass / softening^3 beyond the FP32 range of the batched kernel");
+        }
+    }
     const double *in[7] = {x, y, z, vx, vy, vz, m};
     const int arrays[7] = {kX, kY, kZ, kVx, kVy, kVz, kM};
     const size_t bytes = sizeof(double) * mb.count;
@@ -545,7 +598,7 @@ void Batch::evaluate() {
                               queue_.data(), status_.data(), sm_count_, stream_),
           "batched forces");
     check(launch_batch_reduce(groups_.data(), group_count_, partial_.data(),
-                              static_cast<uint32_t>(config_.threads * config_.targets_per_thread),
+                              config_.targets_per_block(),
                               array(kAx), array(kAy), array(kAz), stream_),
           "reducing partial sums");
 }
@@ -699,16 +752,15 @@ void Batch::energy(uint32_t id, double *kinetic, double *potential) {
 }
 
 double Batch::autotune(BatchConfig &chosen) {
-    static const int shapes[][2] = {{128, 2}, {128, 4}, {256, 2}, {256, 4}};
     static const uint32_t chunks[] = {0, 16, 8, 4};
     cudaEvent_t start, stop;
     check(cudaEventCreate(&start), "event");
     check(cudaEventCreate(&stop), "event");
     double best = 1e300;
     BatchConfig best_config = config_;
-    for (const auto &shape : shapes) {
+    for (const auto &shape : kBatchShapes) {
         for (const uint32_t chunk : chunks) {
-            set_config(BatchConfig{shape[0], shape[1], chunk});
+            set_config(BatchConfig{shape[0], shape[1], chunk, shape[2]});
             evaluate();
             check(cudaEventRecord(start, stream_), "event");
             evaluate();

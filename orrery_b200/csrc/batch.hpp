@@ -40,12 +40,31 @@ struct BatchGroup {
     uint32_t slots;
 };
 
-// Tile shape of the batched kernel.
+// Tile shape of the batched kernel. The default is the shape the autotuner
+// picks on B200 for 512 systems of 256 to 16,384 particles.
 struct BatchConfig {
-    int threads = 128;
-    int targets_per_thread = 2; // even: targets are processed in packed pairs
+    int threads = 256;
+    int targets_per_thread = 4; // even: targets are processed in packed pairs
     uint32_t chunk_tiles = 0; // source tiles per item; 0 = a whole system
+    int groups = 8;           // thread groups of a CTA that split each tile's sources
+    // Targets of one work item (one CTA).
+    [[nodiscard]] uint32_t targets_per_block() const {
+        return static_cast<uint32_t>(threads * targets_per_thread / groups);
+    }
 };
+
+// (threads, targets per thread, source groups) of the implemented batched
+// kernels.
+inline constexpr int kBatchShapes[][3] = {{128, 2, 1}, {128, 4, 1}, {256, 2, 1}, {256, 4, 1},
+                                          {128, 2, 4}, {256, 2, 8}, {256, 4, 4}, {256, 4, 8}};
+inline bool batch_shape_known(int threads, int targets_per_thread, int groups) {
+    for (const auto &s : kBatchShapes) {
+        if (s[0] == threads && s[1] == targets_per_thread && s[2] == groups) {
+            return true;
+        }
+    }
+    return false;
+}
 
 // Batched kernel launch (batch.cu).
 cudaError_t launch_batch_forces(const float4 *hi, const float4 *lo, const float *eps2,

@@ -792,7 +792,7 @@ int ob_batch_autotune(ob_batch *batch, ob_batch_shape *chosen, double *best_ms) 
         ob::BatchConfig c;
         const double ms = batch->impl->autotune(c);
         if (chosen != nullptr) {
-            *chosen = ob_batch_shape{c.threads, c.targets_per_thread, c.chunk_tiles, 0};
+            *chosen = ob_batch_shape{c.threads, c.targets_per_thread, c.chunk_tiles, c.groups};
         }
         if (best_ms != nullptr) {
             *best_ms = ms;
@@ -803,11 +803,11 @@ int ob_batch_autotune(ob_batch *batch, ob_batch_shape *chosen, double *best_ms) 
 int ob_batch_set_shape(ob_batch *batch, const ob_batch_shape *shape) {
     return guarded([&] {
         require(batch != nullptr && shape != nullptr, "NULL argument");
-        const bool known = (shape->threads == 128 || shape->threads == 256) &&
-                           (shape->targets_per_thread == 2 || shape->targets_per_thread == 4);
-        require(known, "the library implements no such batch kernel shape");
-        batch->impl->set_config(
-            ob::BatchConfig{shape->threads, shape->targets_per_thread, shape->chunk_tiles});
+        const int groups = shape->groups == 0 ? 1 : shape->groups;
+        require(ob::batch_shape_known(shape->threads, shape->targets_per_thread, groups),
+                "the library implements no such batch kernel shape");
+        batch->impl->set_config(ob::BatchConfig{shape->threads, shape->targets_per_thread,
+                                                shape->chunk_tiles, groups});
     });
 }
 

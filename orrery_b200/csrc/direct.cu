@@ -729,29 +729,20 @@ int direct_candidates(bool split, DirectConfig *out, int capacity) {
 }
 
 DirectConfig direct_default_config(uint32_t n, bool split, int sm_count) {
-    // Start from the widest register tile (most interactions per shared-memory
-    // read), then trade it for CTAs while the grid cannot fill the SMs, and
-    // split the sources across a cluster for what is still missing (the
-    // shapes the autotuner picks on B200 follow this pattern).
+    // The pattern of the shapes the autotuner picks on B200 from 1,000 to
+    // 262,144 particles: 256-thread CTAs in source groups of one warp (of two
+    // for the split form's four-target threads, whose registers allow fewer
+    // warps), two targets per thread for small systems and four from 8192 on,
+    // and the sources split across a cluster until about four CTAs per SM.
     const uint32_t sms = static_cast<uint32_t>(sm_count > 0 ? sm_count : 148);
     DirectConfig c;
     c.threads = 256;
-    c.targets_per_thread = split ? 4 : 8;
-    const int smallest = 2;
+    c.targets_per_thread = n >= 8192u ? 4 : 2;
+    c.groups = split && c.targets_per_thread == 4 ? 4 : 8;
+    const uint32_t bt = static_cast<uint32_t>(c.threads * c.targets_per_thread / c.groups);
+    const uint32_t blocks = ceil_div(n, bt);
     const uint32_t tiles = ceil_div(n, kDirectTile);
-    auto blocks = [&]() {
-        return ceil_div(n, static_cast<uint32_t>(c.threads * c.targets_per_thread));
-    };
-    while (blocks() * 8u < sms && c.targets_per_thread > smallest) {
-        c.targets_per_thread /= 2;
-    }
-    if (blocks() * 8u < sms) {
-        c.threads = 128;
-    }
-    if (blocks() * 8u < sms) {
-        c.threads = 64;
-    }
-    while (c.split < 8 && blocks() * static_cast<uint32_t>(c.split) < 8u * sms &&
+    while (c.split < 8 && blocks * static_cast<uint32_t>(c.split) < 4u * sms &&
            static_cast<uint32_t>(c.split * 2) <= tiles) {
         c.split *= 2;
     }

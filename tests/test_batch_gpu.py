@@ -53,7 +53,8 @@ def test_every_system_matches_the_fp64_oracle(b200, restatement):
 
 
 @pytest.mark.parametrize("shape", [(128, 2, 0), (128, 2, 4), (128, 4, 1), (256, 2, 0),
-                                   (256, 4, 2)])
+                                   (256, 4, 2), (128, 2, 0, 4), (256, 2, 4, 8), (256, 4, 0, 4),
+                                   (256, 4, 2, 8)])
 def test_every_shape_computes_the_same_sums(b200, restatement, shape):
     sizes, radii, systems = _systems(9, 5, hi=6000)
     batch = b200.DeviceBatch(sizes, 0.01 * radii)
@@ -104,6 +105,16 @@ def test_energy_is_conserved_per_system(b200):
     for k in range(4):
         e = sum(batch.energy(k))
         assert abs(e - e0[k]) / abs(e0[k]) < 1e-6
+
+
+def test_mass_beyond_the_fp32_range_is_refused(b200):
+    # The batched kernel adds a target's own entry as f * 0 with f = m / eps^3
+    # in FP32: a mass that makes f overflow would turn that zero into NaN.
+    batch = b200.DeviceBatch([600], [0.01])
+    x, y, z = (np.linspace(0.0, 1.0, 600) + k for k in range(3))
+    with pytest.raises(b200.OrreryError):
+        batch.set_state(0, x, y, z, None, None, None, np.full(600, 1e32))
+    batch.set_state(0, x, y, z, None, None, None, np.full(600, 1e30))
 
 
 def test_autotune_keeps_results_within_bounds(b200, restatement):
