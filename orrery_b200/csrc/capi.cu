@@ -96,12 +96,15 @@ void System::drop_graph() {
         cudaGraphExecDestroy(graph_);
         graph_ = nullptr;
     }
-    if (template_ != nullptr) {
-        cudaGraphDestroy(template_);
-        template_ = nullptr;
+    if (marked_graph_ != nullptr) {
+        cudaGraphExecDestroy(marked_graph_);
+        marked_graph_ = nullptr;
+    }
+    if (marked_template_ != nullptr) {
+        cudaGraphDestroy(marked_template_);
+        marked_template_ = nullptr;
     }
     mark_nodes_.clear();
-    marks_retargeted_ = false;
 }
 
 void System::upload(int first, int count, const double *const *host) {
@@ -182,36 +185,27 @@ void System::enqueue_substep(double timestep, const cudaEvent_t *marks) {
           "kick");
 }
 
-void System::enqueue_step(int integrator, double dt) {
-    const cudaEvent_t *m = marks_.data();
+void System::enqueue_step(int integrator, double dt, bool marked) {
+    // Without marks the solver records its own events, which a capture turns
+    // into ordering only (no graph nodes).
+    const cudaEvent_t *m = marked ? marks_.data() : nullptr;
     if (integrator == OB_INTEGRATOR_YOSHIDA4) {
         double outer = 0.0, inner = 0.0;
         yoshida_weights(outer, inner);
         enqueue_substep(outer * dt, m);
-        enqueue_substep(inner * dt, m + 4);
-        enqueue_substep(outer * dt, m + 8);
+        enqueue_substep(inner * dt, marked ? m + 4 : nullptr);
+        enqueue_substep(outer * dt, marked ? m + 8 : nullptr);
     } else {
         enqueue_substep(dt, m);
     }
 }
 
-void System::ensure_graph(int integrator, double dt) {
-    if (graph_ != nullptr && graph_integrator_ == integrator && graph_dt_ == dt &&
-        graph_generation_ == solver_->generation()) {
-        return;
-    }
-    drop_graph();
-    const size_t needed = 4u * static_cast<size_t>(evaluations_per_step(integrator));
-    while (marks_.size() < needed) {
-        cudaEvent_t e = nullptr;
-        check(cudaEventCreate(&e), "creating an event");
-        marks_.push_back(e);
-    }
+cudaGraph_t System::capture_step(int integrator, double dt, bool marked) {
     cudaGraph_t graph = nullptr;
     check(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed),
           "beginning graph capture");
     try {
-        enqueue_step(integrator, dt);
+        enqueue_step(integrator, dt, marked);
     } catch (...) {
         cudaStreamEndCapture(stream_, &graph);
         if (graph != nullptr) {
@@ -220,24 +214,61 @@ void System::ensure_graph(int integrator, double dt) {
         throw;
     }
     check(cudaStreamEndCapture(stream_, &graph), "ending graph capture");
-    template_ = graph;
-    check(cudaGraphInstantiate(&graph_, graph, 0), "instantiating the step graph");
+    return graph;
+}
+
+void System::ensure_graph(int integrator, double dt) {
+    if (graph_ != nullptr && graph_integrator_ == integrator && graph_dt_ == dt &&
+        graph_generation_ == solver_->generation()) {
+        return;
+    }
+    drop_graph();
+    cudaGraph_t graph = capture_step(integrator, dt, false);
+    size_t count = 0;
+    cudaError_t err = cudaGraphGetNodes(graph, nullptr, &count);
+    std::vector<cudaGraphNode_t> nodes(count);
+    if (err == cudaSuccess) {
+        err = cudaGraphGetNodes(graph, nodes.data(), &count);
+    }
+    graph_kernels_ = 0;
+    for (size_t k = 0; err == cudaSuccess && k < count; ++k) {
+        cudaGraphNodeType type;
+        err = cudaGraphNodeGetType(nodes[k], &type);
+        graph_kernels_ += err == cudaSuccess && type == cudaGraphNodeTypeKernel ? 1u : 0u;
+    }
+    if (err == cudaSuccess) {
+        err = cudaGraphInstantiate(&graph_, graph, 0);
+    }
+    cudaGraphDestroy(graph);
+    check(err, "instantiating the step graph");
     graph_integrator_ = integrator;
     graph_dt_ = dt;
     graph_generation_ = solver_->generation();
-    // Find the event-record node of each placeholder, and count kernels.
+}
+
+void System::ensure_marked_graph() {
+    if (marked_graph_ != nullptr) {
+        return;
+    }
+    const size_t needed = 4u * static_cast<size_t>(evaluations_per_step(graph_integrator_));
+    while (marks_.size() < needed) {
+        cudaEvent_t e = nullptr;
+        check(cudaEventCreate(&e), "creating an event");
+        marks_.push_back(e);
+    }
+    cudaGraph_t graph = capture_step(graph_integrator_, graph_dt_, true);
+    marked_template_ = graph;
+    check(cudaGraphInstantiate(&marked_graph_, graph, 0), "instantiating the profiled step graph");
+    // Find the event-record node of each placeholder.
     size_t count = 0;
     check(cudaGraphGetNodes(graph, nullptr, &count), "listing graph nodes");
     std::vector<cudaGraphNode_t> nodes(count);
     check(cudaGraphGetNodes(graph, nodes.data(), &count), "listing graph nodes");
     mark_nodes_.assign(needed, nullptr);
-    graph_kernels_ = 0;
     for (cudaGraphNode_t node : nodes) {
         cudaGraphNodeType type;
         check(cudaGraphNodeGetType(node, &type), "reading a node type");
-        if (type == cudaGraphNodeTypeKernel) {
-            ++graph_kernels_;
-        } else if (type == cudaGraphNodeTypeEventRecord) {
+        if (type == cudaGraphNodeTypeEventRecord) {
             cudaEvent_t e = nullptr;
             check(cudaGraphEventRecordNodeGetEvent(node, &e), "reading an event node");
             for (size_t k = 0; k < needed; ++k) {
@@ -252,7 +283,8 @@ void System::ensure_graph(int integrator, double dt) {
 void System::set_marks(const std::vector<cudaEvent_t> &events, size_t offset) {
     for (size_t k = 0; k < mark_nodes_.size(); ++k) {
         if (mark_nodes_[k] != nullptr) {
-            check(cudaGraphExecEventRecordNodeSetEvent(graph_, mark_nodes_[k], events[offset + k]),
+            check(cudaGraphExecEventRecordNodeSetEvent(marked_graph_, mark_nodes_[k],
+                                                       events[offset + k]),
                   "retargeting an event node");
         }
     }
@@ -318,14 +350,13 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
     ensure_graph(integrator, dt);
     for (uint64_t s = 0; s < steps; ++s) {
         if (ring_used_ < ring_steps_) {
+            ensure_marked_graph();
             set_marks(ring_, static_cast<size_t>(ring_used_) * 12);
-            marks_retargeted_ = true;
             ++ring_used_;
-        } else if (marks_retargeted_) {
-            set_marks(marks_, 0);
-            marks_retargeted_ = false;
+            check(cudaGraphLaunch(marked_graph_, stream_), "launching the profiled step graph");
+        } else {
+            check(cudaGraphLaunch(graph_, stream_), "launching the step graph");
         }
-        check(cudaGraphLaunch(graph_, stream_), "launching the step graph");
     }
     solver_->account(steps * evaluations_per_step(integrator), n_);
 }

@@ -57,9 +57,11 @@ private:
     void upload(int first, int count, const double *const *host);
     void evaluate(bool count, const cudaEvent_t *marks = nullptr);
     void enqueue_substep(double timestep, const cudaEvent_t *marks);
-    void enqueue_step(int integrator, double dt);
+    void enqueue_step(int integrator, double dt, bool marked);
+    cudaGraph_t capture_step(int integrator, double dt, bool marked);
     void drop_graph();
     void ensure_graph(int integrator, double dt);
+    void ensure_marked_graph();
     void set_marks(const std::vector<cudaEvent_t> &events, size_t offset);
 
     std::unique_ptr<Solver> solver_;
@@ -68,21 +70,25 @@ private:
     DeviceArray<double> terms_;
     cudaStream_t stream_ = nullptr;
     bool owns_stream_ = true;
-    cudaGraph_t template_ = nullptr;  // kept so its event nodes can be retargeted
+    // The step as a CUDA graph, without event nodes: what every step replays
+    // unless it is profiled.
     cudaGraphExec_t graph_ = nullptr;
     int graph_integrator_ = -1;
     double graph_dt_ = 0.0;
     uint32_t graph_kernels_ = 0;
     uint64_t graph_generation_ = 0;
 
-    // Four placeholder events per evaluation of a step, captured as event
-    // nodes; before a profiled replay they are pointed at a fresh slot of ring_.
+    // The same step with four placeholder events per evaluation captured as
+    // event nodes, built on the first profiled step; before each profiled
+    // replay its nodes are pointed at a fresh slot of ring_. The template is
+    // kept so that its event nodes can be retargeted.
+    cudaGraph_t marked_template_ = nullptr;
+    cudaGraphExec_t marked_graph_ = nullptr;
     std::vector<cudaEvent_t> marks_;
     std::vector<cudaGraphNode_t> mark_nodes_;
     std::vector<cudaEvent_t> ring_;
     uint32_t ring_steps_ = 0;     // capacity in steps
     uint32_t ring_used_ = 0;      // steps recorded
-    bool marks_retargeted_ = false;
 };
 
 } // namespace ob
