@@ -87,6 +87,13 @@ WORKLOADS = {
                                   integrator="yoshida4", precision="split",
                                   metric="direct Gint/s", unit="Gint/s", higher=True,
                                   generator="plummer"),
+    # Run output of the 2M collision: trajectory frames (positions and
+    # velocities) every `stride` steps and checkpoints, in the reference's
+    # formats.
+    "run-output-2m": dict(kind="output", n=2_000_000, eps=0.02, dt=5e-4, integrator="vv",
+                          theta=0.5, leaf=32, quadrupole=True, precision="fp32",
+                          metric="run time per trajectory frame at 2M", unit="ms/frame",
+                          higher=False, generator="collision", stride=5),
 }
 DEFAULT_WORKLOAD = "bh-collision-2m"
 
@@ -418,6 +425,25 @@ def run_reference(args, w):
         print(json.dumps(line), flush=True)
         barrier(dist)
         return
+    if w["kind"] == "output":
+        import tempfile
+
+        directory = tempfile.mkdtemp(prefix="orrery_output_ref_")
+        base = cpu_baseline_output(w, make_inputs(w), directory)
+        os.rmdir(directory)
+        line = {"impl": "reference", "metric": w["metric"], "value": base.get("value"),
+                "unit": "ms/frame", "n_gpus": args.gpus, "steps": steps,
+                "warmup": args.warmup, "ms_per_step": None, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": args.workload, "n": w["n"], "stride": w["stride"]},
+                "cpu_baseline": base,
+                "e2e": {"value": base.get("value"), "unit": "ms/frame", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        if "unavailable" in base:
+            line = {"impl": "reference", "unavailable": base["unavailable"]}
+        print(json.dumps(line), flush=True)
+        barrier(dist)
+        return
     data = make_inputs(w)
     if w["kind"] == "batch":
         base = cpu_baseline_batch(w, *data, budget_s=min(60.0, 10.0 * steps))
@@ -487,6 +513,175 @@ def load_peaks():
             p = json.load(fh)
         return p.get("hbm_gbs", 6650.0), "measured"
     return 6650.0, "fallback"
+
+
+def output_state(data):
+    """The ten arrays of a checkpoint for the collision inputs (accelerations
+    zero: the writers only move bytes)."""
+    st = {k: np.ascontiguousarray(data[k]) for k in ("m", "x", "y", "z", "vx", "vy", "vz")}
+    for k in ("ax", "ay", "az"):
+        st[k] = np.zeros(len(st["m"]))
+    return st
+
+
+def cpu_baseline_output(w, data, directory):
+    """The reference's own writers (sim::TrajectoryWriter, sim::write_checkpoint,
+    oracle/_ref) on the same 2M state: the run time a frame costs the
+    reference's run loop, which writes it synchronously."""
+    import oracle
+
+    if not oracle.Reference.available():
+        return {"unavailable": "the reference library (oracle/_ref) is not built"}
+    ref = oracle.Reference()
+    st = output_state(data)
+    frame = {k: st[k] for k in ("x", "y", "z", "vx", "vy", "vz")}
+    path = os.path.join(directory, "reference.tj")
+    frames = 3
+    t0 = time.perf_counter()
+    ref.write_trajectory(path, st["m"], w["dt"], [(k, k * w["dt"], frame)
+                                                  for k in range(frames)], True)
+    traj_s = time.perf_counter() - t0
+    os.remove(path)
+    path = os.path.join(directory, "reference.ck")
+    t0 = time.perf_counter()
+    ref.write_checkpoint(path, 1, st)
+    ck_s = time.perf_counter() - t0
+    size = os.path.getsize(path)
+    os.remove(path)
+    header = 8 + 4 + 4 + 8 + 8 * len(st["m"])
+    per_frame = traj_s / frames  # the header (masses, a sixth of a frame) included
+    return {"value": per_frame * 1e3, "unit": "ms/frame", "cores": 1, "kind": "reference",
+            "sample": f"sim::TrajectoryWriter: header ({header / 1e6:.0f} MB) and {frames} frames "
+                      "of positions and velocities of the 2M state; sim::write_checkpoint of it",
+            "checkpoint_s": ck_s, "checkpoint_bytes": size}
+
+
+def run_output(args, w):
+    """Trajectory frames and checkpoints of the 2M collision as it steps."""
+    import tempfile
+
+    import torch
+
+    import orrery_b200 as ob
+
+    world, rank, local = dist_env()
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    ob.load_library()
+    data = make_inputs(w)
+    n, dt, stride = w["n"], w["dt"], w["stride"]
+    system = ob.DeviceSystem(n, w["eps"], kind=ob.SOLVER_TREE, precision="fp32",
+                             opening_angle=w["theta"], leaf_capacity=w["leaf"],
+                             quadrupole=w["quadrupole"])
+    system.set_state(data["x"], data["y"], data["z"], data["vx"], data["vy"], data["vz"],
+                     data["m"])
+    system.step(dt, max(args.warmup, 3), w["integrator"])
+    kernels_per_step = system.step_kernels(dt, w["integrator"])
+    K = max(args.steps, 12 * stride)  # enough frames for the writers' steady state
+    directory = tempfile.mkdtemp(prefix="orrery_output_")
+    frame_bytes = 6 * 8 * n
+
+    def steps_with_frames(every, path):
+        """Wall seconds of K steps with a frame every `every` steps (none when
+        0), up to the last step's completion, and the further seconds until
+        every frame is in the file."""
+        t = ob.Trajectory(path, dt, system=system, with_velocities=True) if every else None
+        system.synchronize()
+        t0 = time.perf_counter()
+        for k in range(1, K + 1):
+            system.step_async(dt, 1, w["integrator"])
+            if every and k % every == 0:
+                t.write_frame(k, k * dt)
+        system.synchronize()
+        stepped = time.perf_counter() - t0
+        if t is not None:
+            t.close()
+        drained = time.perf_counter() - t0 - stepped
+        if every:
+            os.remove(path)
+        return stepped, drained
+
+    sampler = ClockSampler(local)
+    barrier(dist)
+    sampler.start()
+    time.sleep(0.3)
+    base, _ = steps_with_frames(0, None)
+    strided, strided_drain = steps_with_frames(stride, os.path.join(directory, f"rank{rank}_s.tj"))
+    every, every_drain = steps_with_frames(1, os.path.join(directory, f"rank{rank}_1.tj"))
+    # The snapshot on the device: two device-to-device copies of 3n doubles,
+    # timed on the system's stream.
+    stream = torch.cuda.ExternalStream(system.stream(), device=device)
+    t = ob.Trajectory(os.path.join(directory, f"rank{rank}_copy.tj"), dt, system=system,
+                      with_velocities=True)
+    reps = 4
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(reps):
+        t.write_frame(k, k * dt)
+    e1.record(stream)
+    e1.synchronize()
+    snapshot_ms = e0.elapsed_time(e1) / reps
+    t.close()
+    os.remove(os.path.join(directory, f"rank{rank}_copy.tj"))
+    # Checkpoint write and restore.
+    ck = os.path.join(directory, f"rank{rank}.ck")
+    t0 = time.perf_counter()
+    system.write_checkpoint(ck, K, "")
+    write_s = time.perf_counter() - t0
+    ck_bytes = os.path.getsize(ck)
+    t0 = time.perf_counter()
+    system.read_checkpoint(ck)
+    read_s = time.perf_counter() - t0
+    os.remove(ck)
+    clocks = sampler.stop()
+    barrier(dist)
+    per_frame_ms = (strided - base) / (K // stride) * 1e3
+    per_frame_every_ms = (every - base) / K * 1e3
+    step_ms = base / K * 1e3
+    peak, src = load_peaks()
+    copy_gbs = 2 * frame_bytes / (snapshot_ms * 1e-3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": w["metric"], "value": max(per_frame_ms, 0.0), "unit": "ms/frame",
+            "n_gpus": world, "steps": K, "warmup": max(args.warmup, 3),
+            "ms_per_step": step_ms, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "n": n, "stride": stride,
+                       "frame": "positions and velocities (ORRERYTJ v1)",
+                       "frame_bytes": frame_bytes + 24, "checkpoint": "ORRERYCK v1",
+                       "l2": "state 160 MB, larger than L2"},
+            "stepping": {"ms_per_step_without_output": step_ms,
+                         f"ms_per_step_frame_every_{stride}": strided / K * 1e3,
+                         f"drain_after_last_step_s_every_{stride}": strided_drain,
+                         "ms_per_step_frame_every_step": every / K * 1e3,
+                         "drain_after_last_step_s_every_step": every_drain,
+                         "run_time_per_frame_every_step_ms": per_frame_every_ms,
+                         "frames_per_s_written_every_step": K / (every + every_drain)},
+            "checkpoint": {"write_s": write_s, "read_s": read_s, "bytes": ck_bytes,
+                           "write_gb_s": ck_bytes / write_s / 1e9,
+                           "read_gb_s": ck_bytes / read_s / 1e9},
+            "roofline": {"bound": "hbm", "kernel": "snapshot copy (device to device)",
+                         "achieved": copy_gbs, "peak": peak, "unit": "GB/s",
+                         "frac": copy_gbs / peak, "traffic": 2 * frame_bytes,
+                         "ms_per_snapshot": snapshot_ms,
+                         "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)"},
+            "e2e": {"value": K / (every + every_drain), "unit": "frames/s",
+                    "h2d_bytes_per_step": 0, "d2h_bytes_per_step": frame_bytes,
+                    "path": "ob_trajectory_write_system_frame each step of the stepping 2M "
+                            "collision, frames in the file when the clock stops"},
+            "gpu_launches": 3 * K * kernels_per_step, "clocks": clocks,
+        }
+        base_line = cpu_baseline_output(w, data, directory)
+        line["cpu_baseline"] = base_line
+        print(json.dumps(line), flush=True)
+    try:
+        os.rmdir(directory)
+    except OSError:
+        pass
+    barrier(dist)
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def e2e_integrator_plugin(system, w, data, steps, torch):
@@ -1110,6 +1305,8 @@ def main():
         run_batch(args, w)
     elif w["kind"] == "serving":
         run_serving(args, w)
+    elif w["kind"] == "output":
+        run_output(args, w)
     else:
         run_b200(args, w)
 

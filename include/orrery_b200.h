@@ -33,6 +33,8 @@ extern "C" {
 #define OB_ERROR_TIMEOUT 5        /* a bounded device-side wait ran out */
 #define OB_ERROR_CAPACITY 6       /* a size or budget limit was exceeded */
 #define OB_ERROR_UNSUPPORTED 7
+#define OB_ERROR_IO 8             /* a file could not be opened, written or read, or fails its
+                                     format checks; the message names the file and the check */
 
 /* Solver kinds: the reference's DirectSolver and BarnesHutSolver
  * (include/orrery/solvers/direct_solver.hpp:107,
@@ -253,6 +255,73 @@ int ob_system_autotune(ob_system *system, ob_direct_shape *chosen, double *best_
 
 int ob_system_counts(ob_system *system, ob_counts *counts);
 int ob_system_size(const ob_system *system, uint64_t *n);
+
+/* ------------------------------------------------------------------------ */
+/* Run output: checkpoints and trajectories in the reference's formats       */
+/* ------------------------------------------------------------------------ */
+/* ORRERYCK v1 checkpoints (sim::write_checkpoint / sim::read_checkpoint,
+ * include/orrery/sim/checkpoint.hpp:85-94) and ORRERYTJ v1 trajectories
+ * (sim::TrajectoryWriter, include/orrery/sim/trajectory.hpp:112-146), byte for
+ * byte as the reference's double-precision build writes them, so that its
+ * `orrery resume` and `orrery show` read these files and it writes files these
+ * calls read. The configuration a checkpoint carries is the caller's text in
+ * the reference's configuration format (sim::write_configuration); it is
+ * stored and returned unparsed. A checkpoint is written to "<path>.partial"
+ * and renamed over <path>. Failures are OB_ERROR_IO. */
+
+/* A checkpoint from host arrays (n of each): masses, positions, velocities,
+ * accelerations, taken after `step` steps. */
+int ob_checkpoint_write(const char *path, uint64_t step, const char *configuration,
+                        uint64_t configuration_bytes, uint64_t n, const double *m,
+                        const double *x, const double *y, const double *z, const double *vx,
+                        const double *vy, const double *vz, const double *ax, const double *ay,
+                        const double *az);
+/* A checkpoint's header: step, particle count, configuration length. */
+int ob_checkpoint_info(const char *path, uint64_t *step, uint64_t *n,
+                       uint64_t *configuration_bytes);
+/* Reads a whole checkpoint of n particles and checks it (magic, version,
+ * flags, sizes, checksum); `configuration` (NULL to skip) receives the text. */
+int ob_checkpoint_read(const char *path, char *configuration, uint64_t configuration_capacity,
+                       uint64_t n, double *m, double *x, double *y, double *z, double *vx,
+                       double *vy, double *vz, double *ax, double *ay, double *az);
+/* A checkpoint of a device-resident system's state as it stands after the
+ * steps already enqueued (waits for them). */
+int ob_system_write_checkpoint(ob_system *system, const char *path, uint64_t step,
+                               const char *configuration, uint64_t configuration_bytes);
+/* Restores a system of the checkpoint's size to the stored state, the
+ * carried accelerations included (as sim::Simulation::restore with
+ * accelerations_are_current, include/orrery/sim/simulation.hpp:101-102), so
+ * that a resumed run continues bit for bit; returns the step and the text. */
+int ob_system_read_checkpoint(ob_system *system, const char *path, uint64_t *step,
+                              char *configuration, uint64_t configuration_capacity,
+                              uint64_t *configuration_bytes);
+
+typedef struct ob_trajectory ob_trajectory;
+
+/* A trajectory file of n particles: the header (masses, timestep, whether
+ * frames carry velocities) is written here. */
+int ob_trajectory_create(const char *path, uint64_t n, const double *masses, double timestep,
+                         int32_t with_velocities, ob_trajectory **out);
+/* The same for a device-resident system (its masses). Its frames can then
+ * be snapshots of the system taken on the device between steps and written
+ * by a background thread (ob_trajectory_write_system_frame). Close the
+ * trajectory before destroying the system. */
+int ob_trajectory_create_for_system(const char *path, ob_system *system, double timestep,
+                                    int32_t with_velocities, ob_trajectory **out);
+/* A frame from host arrays (velocities ignored when the file has none). */
+int ob_trajectory_write_frame(ob_trajectory *trajectory, uint64_t step, double time,
+                              const double *x, const double *y, const double *z,
+                              const double *vx, const double *vy, const double *vz);
+/* A frame of the bound system's state at this point of its stream: a
+ * device-to-device copy enqueued between the steps; returns without waiting
+ * for the file (at most two frames in flight; a third waits for one). */
+int ob_trajectory_write_system_frame(ob_trajectory *trajectory, uint64_t step, double time);
+/* Waits until every frame given so far is in the file and flushes it; returns
+ * the first failure of any of them. */
+int ob_trajectory_flush(ob_trajectory *trajectory);
+int ob_trajectory_frames(ob_trajectory *trajectory, uint64_t *frames);
+/* Flushes, closes and frees (returns the flush's status). */
+int ob_trajectory_close(ob_trajectory *trajectory);
 
 /* ------------------------------------------------------------------------ */
 /* Batch: many independent systems integrated together                       */

@@ -293,10 +293,101 @@ class Reference:
         lib.ref_potential_energy.restype = C.c_double
         lib.ref_kinetic_energy.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp]
         lib.ref_kinetic_energy.restype = C.c_double
+        # Run output (ref_output_shim.cpp).
+        lib.ref_last_error.restype = C.c_char_p
+        lib.ref_default_configuration.argtypes = [C.c_char_p, C.c_size_t]
+        lib.ref_default_configuration.restype = C.c_size_t
+        lib.ref_write_checkpoint.argtypes = [C.c_char_p, C.c_uint64, C.c_size_t] + [_dp] * 10
+        lib.ref_read_checkpoint.argtypes = [C.c_char_p, _u64p, _u64p, C.c_size_t] + [_dp] * 10 + [
+            C.c_char_p, C.c_size_t, C.POINTER(C.c_size_t)]
+        lib.ref_write_trajectory.argtypes = [C.c_char_p, C.c_size_t, _dp, C.c_double, C.c_int,
+                                             C.c_size_t, _u64p, _dp, _dp, _dp]
+        lib.ref_read_trajectory.argtypes = [C.c_char_p, _u64p, _dp, C.POINTER(C.c_int),
+                                            C.POINTER(C.c_size_t), C.c_size_t, C.c_size_t, _dp,
+                                            _u64p, _dp, _dp, _dp]
 
     @staticmethod
     def available(path: str = REFERENCE_PATH) -> bool:
         return os.path.exists(path)
+
+    # -- run output: the reference's own writers and readers ------------------
+
+    CHECKPOINT_ARRAYS = ("m", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+
+    def _raise(self, what):
+        raise RuntimeError(f"{what}: {self.lib.ref_last_error().decode()}")
+
+    def default_configuration(self) -> str:
+        """sim::write_configuration of a default Configuration."""
+        size = self.lib.ref_default_configuration(None, 0)
+        buf = C.create_string_buffer(size + 1)
+        self.lib.ref_default_configuration(buf, size)
+        return buf.raw[:size].decode()
+
+    def write_checkpoint(self, path, step, state):
+        """sim::write_checkpoint of {default configuration, step, state}."""
+        arrs = [np.ascontiguousarray(state[k], dtype=np.float64) for k in self.CHECKPOINT_ARRAYS]
+        if self.lib.ref_write_checkpoint(os.fsencode(path), int(step), len(arrs[0]),
+                                         *(_d(a) for a in arrs)) != 0:
+            self._raise("write_checkpoint")
+
+    def read_checkpoint(self, path, capacity=1 << 22):
+        """sim::read_checkpoint: step, state arrays and the configuration as
+        sim::write_configuration writes it back out."""
+        step, n = C.c_uint64(), C.c_uint64()
+        out = {k: np.zeros(capacity) for k in self.CHECKPOINT_ARRAYS}
+        text = C.create_string_buffer(1 << 16)
+        length = C.c_size_t()
+        if self.lib.ref_read_checkpoint(os.fsencode(path), C.byref(step), C.byref(n), capacity,
+                                        *(_d(out[k]) for k in self.CHECKPOINT_ARRAYS), text,
+                                        1 << 16, C.byref(length)) != 0:
+            self._raise("read_checkpoint")
+        res = {k: v[:n.value].copy() for k, v in out.items()}
+        res["step"] = step.value
+        res["configuration"] = text.raw[:length.value].decode()
+        return res
+
+    def write_trajectory(self, path, masses, timestep, frames, with_velocities):
+        """sim::TrajectoryWriter: `frames` is a list of (step, time, state)."""
+        m = np.ascontiguousarray(masses, dtype=np.float64)
+        n = len(m)
+        steps = np.array([f[0] for f in frames], dtype=np.uint64)
+        times = np.array([f[1] for f in frames], dtype=np.float64)
+        xyz = np.concatenate([np.concatenate([f[2][k] for k in ("x", "y", "z")])
+                              for f in frames]) if frames else np.zeros(1)
+        v = (np.concatenate([np.concatenate([f[2][k] for k in ("vx", "vy", "vz")])
+                             for f in frames]) if frames and with_velocities else np.zeros(1))
+        if self.lib.ref_write_trajectory(os.fsencode(path), n, _d(m), float(timestep),
+                                         int(with_velocities), len(frames), _u(steps),
+                                         _d(times), _d(np.ascontiguousarray(xyz)),
+                                         _d(np.ascontiguousarray(v))) != 0:
+            self._raise("TrajectoryWriter")
+
+    def read_trajectory(self, path, max_frames=64, max_n=1 << 20):
+        """sim::TrajectoryReader: header facts and the frames."""
+        n, ts, wv, nf = C.c_uint64(), C.c_double(), C.c_int(), C.c_size_t()
+        masses = np.zeros(max_n)
+        steps = np.zeros(max_frames, dtype=np.uint64)
+        times = np.zeros(max_frames)
+        xyz = np.zeros(max_frames * 3 * max_n)
+        v = np.zeros(max_frames * 3 * max_n)
+        if self.lib.ref_read_trajectory(os.fsencode(path), C.byref(n), C.byref(ts), C.byref(wv),
+                                        C.byref(nf), max_frames, max_n, _d(masses), _u(steps),
+                                        _d(times), _d(xyz), _d(v)) != 0:
+            self._raise("TrajectoryReader")
+        count, frames = n.value, min(nf.value, max_frames)
+        out = []
+        for f in range(frames):
+            p = xyz[f * 3 * count:(f + 1) * 3 * count]
+            st = {"x": p[:count].copy(), "y": p[count:2 * count].copy(),
+                  "z": p[2 * count:].copy()}
+            if wv.value:
+                q = v[f * 3 * count:(f + 1) * 3 * count]
+                st.update(vx=q[:count].copy(), vy=q[count:2 * count].copy(),
+                          vz=q[2 * count:].copy())
+            out.append((int(steps[f]), float(times[f]), st))
+        return {"n": count, "timestep": ts.value, "with_velocities": bool(wv.value),
+                "masses": masses[:count].copy(), "frames": out, "frame_count": nf.value}
 
     def worker_count(self) -> int:
         return int(self.lib.ref_default_worker_count())

@@ -33,6 +33,7 @@ ERROR_CUDA = 4
 ERROR_TIMEOUT = 5
 ERROR_CAPACITY = 6
 ERROR_UNSUPPORTED = 7
+ERROR_IO = 8
 
 SOLVER_DIRECT = 0
 SOLVER_TREE = 1
@@ -204,6 +205,21 @@ def load_library():
     lib.ob_server_cancel.argtypes = [vp, C.c_uint64]
     lib.ob_server_stats.argtypes = [vp, C.POINTER(ServerSummary)]
     lib.ob_server_drain.argtypes = [vp, C.c_double]
+    cp = C.c_char_p
+    lib.ob_checkpoint_write.argtypes = [cp, C.c_uint64, cp, C.c_uint64, C.c_uint64] + [_dp] * 10
+    lib.ob_checkpoint_info.argtypes = [cp, _u64p, _u64p, _u64p]
+    lib.ob_checkpoint_read.argtypes = [cp, C.c_char_p, C.c_uint64, C.c_uint64] + [_dp] * 10
+    lib.ob_system_write_checkpoint.argtypes = [vp, cp, C.c_uint64, cp, C.c_uint64]
+    lib.ob_system_read_checkpoint.argtypes = [vp, cp, _u64p, C.c_char_p, C.c_uint64, _u64p]
+    lib.ob_trajectory_create.argtypes = [cp, C.c_uint64, _dp, C.c_double, C.c_int32,
+                                         C.POINTER(vp)]
+    lib.ob_trajectory_create_for_system.argtypes = [cp, vp, C.c_double, C.c_int32,
+                                                    C.POINTER(vp)]
+    lib.ob_trajectory_write_frame.argtypes = [vp, C.c_uint64, C.c_double] + [_dp] * 6
+    lib.ob_trajectory_write_system_frame.argtypes = [vp, C.c_uint64, C.c_double]
+    lib.ob_trajectory_flush.argtypes = [vp]
+    lib.ob_trajectory_frames.argtypes = [vp, _u64p]
+    lib.ob_trajectory_close.argtypes = [vp]
     _lib = lib
     return lib
 
@@ -493,6 +509,27 @@ class DeviceSystem:
     def synchronize(self) -> None:
         _check(self._lib.ob_system_synchronize(self._handle))
 
+    def write_checkpoint(self, path, step: int, configuration: str = "") -> None:
+        """An ORRERYCK v1 checkpoint of the device state after `step` steps
+        (sim::write_checkpoint); `configuration` is the reference's
+        configuration text, stored as is."""
+        text = configuration.encode()
+        _check(self._lib.ob_system_write_checkpoint(self._handle, os.fsencode(path), int(step),
+                                                    text, len(text)))
+
+    def read_checkpoint(self, path):
+        """Restores the state (carried accelerations included) from an ORRERYCK
+        v1 checkpoint of this size; returns (step, configuration text)."""
+        step, n, size = (C.c_uint64() for _ in range(3))
+        _check(self._lib.ob_checkpoint_info(os.fsencode(path), C.byref(step), C.byref(n),
+                                            C.byref(size)))
+        buf = C.create_string_buffer(max(1, size.value))
+        got = C.c_uint64()
+        _check(self._lib.ob_system_read_checkpoint(self._handle, os.fsencode(path),
+                                                   C.byref(step), buf, size.value,
+                                                   C.byref(got)))
+        return step.value, buf.raw[:got.value].decode()
+
     def energy(self):
         ke, pe = C.c_double(), C.c_double()
         _check(self._lib.ob_system_energy(self._handle, C.byref(ke), C.byref(pe)))
@@ -703,6 +740,111 @@ class Server:
 
     def drain(self, timeout: float = 600.0) -> None:
         _check(self._lib.ob_server_drain(self._handle, float(timeout)))
+
+
+_CHECKPOINT_ARRAYS = ("m", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+
+
+def write_checkpoint(path, step: int, state: dict, configuration: str = "") -> None:
+    """sim::write_checkpoint (include/orrery/sim/checkpoint.hpp:85) from host
+    arrays: `state` holds m x y z vx vy vz ax ay az (FP64, equal lengths)."""
+    arrs = [_f64(state[k]) for k in _CHECKPOINT_ARRAYS]
+    n = len(arrs[0])
+    if any(len(a) != n for a in arrs):
+        raise OrreryError(ERROR_INVALID_ARGUMENT, "every state array needs the same length")
+    text = configuration.encode()
+    lib = load_library()
+    _check(lib.ob_checkpoint_write(os.fsencode(path), int(step), text, len(text), n,
+                                   *(_ptr(a) for a in arrs)))
+
+
+def checkpoint_info(path) -> dict:
+    """The header of an ORRERYCK checkpoint: step, particle count, configuration length."""
+    lib = load_library()
+    step, n, size = (C.c_uint64() for _ in range(3))
+    _check(lib.ob_checkpoint_info(os.fsencode(path), C.byref(step), C.byref(n), C.byref(size)))
+    return {"step": step.value, "n": n.value, "configuration_bytes": size.value}
+
+
+def read_checkpoint(path) -> dict:
+    """sim::read_checkpoint (include/orrery/sim/checkpoint.hpp:94): the step,
+    the configuration text and the ten state arrays, checked against the
+    file's checksum."""
+    info = checkpoint_info(path)
+    n = info["n"]
+    out = {k: np.empty(n) for k in _CHECKPOINT_ARRAYS}
+    buf = C.create_string_buffer(max(1, info["configuration_bytes"]))
+    lib = load_library()
+    _check(lib.ob_checkpoint_read(os.fsencode(path), buf, info["configuration_bytes"], n,
+                                  *(_ptr(out[k]) for k in _CHECKPOINT_ARRAYS)))
+    out["step"] = info["step"]
+    out["configuration"] = buf.raw[:info["configuration_bytes"]].decode()
+    return out
+
+
+class Trajectory:
+    """sim::TrajectoryWriter (include/orrery/sim/trajectory.hpp:112-146): an
+    ORRERYTJ v1 file. Over host arrays (``masses`` given), or bound to a
+    DeviceSystem (``system`` given), whose frames are snapshots taken on the
+    device between steps and written by a background thread."""
+
+    def __init__(self, path, timestep: float, masses=None, system=None,
+                 with_velocities: bool = False):
+        lib = load_library()
+        handle = C.c_void_p()
+        if system is not None:
+            _check(lib.ob_trajectory_create_for_system(os.fsencode(path), system._handle,
+                                                       float(timestep), int(with_velocities),
+                                                       C.byref(handle)))
+            self.n = system.n
+        else:
+            m = _f64(masses)
+            _check(lib.ob_trajectory_create(os.fsencode(path), len(m), _ptr(m), float(timestep),
+                                            int(with_velocities), C.byref(handle)))
+            self.n = len(m)
+        self._lib = lib
+        self._handle = handle
+        self._system = system  # kept alive while the trajectory is open
+        self.with_velocities = bool(with_velocities)
+
+    def write_frame(self, step: int, time: float, state: dict = None) -> None:
+        """A frame from host arrays (x y z, and vx vy vz when the file carries
+        them), or, with no `state`, a snapshot of the bound system."""
+        if state is None:
+            _check(self._lib.ob_trajectory_write_system_frame(self._handle, int(step),
+                                                              float(time)))
+            return
+        keys = ("x", "y", "z", "vx", "vy", "vz") if self.with_velocities else ("x", "y", "z")
+        arrs = [_f64(state[k]) for k in keys] + [None] * (6 - len(keys))
+        _check(self._lib.ob_trajectory_write_frame(self._handle, int(step), float(time),
+                                                   *(_ptr(a) for a in arrs)))
+
+    def flush(self) -> None:
+        _check(self._lib.ob_trajectory_flush(self._handle))
+
+    @property
+    def frames(self) -> int:
+        f = C.c_uint64()
+        _check(self._lib.ob_trajectory_frames(self._handle, C.byref(f)))
+        return f.value
+
+    def close(self) -> None:
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            self._handle = None
+            _check(self._lib.ob_trajectory_close(h))
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            self._lib.ob_trajectory_close(h)
+            self._handle = None
 
 
 def compute_accelerations(positions, masses, softening: float = 0.0, solver: str = "direct",

@@ -11,6 +11,7 @@
 #include "orrery_b200.h"
 #include "solver.hpp"
 #include "batch.hpp"
+#include "output.hpp"
 #include "system.hpp"
 #include "tree.hpp"
 
@@ -149,6 +150,32 @@ void System::refresh() {
 void System::evaluate(bool count, const cudaEvent_t *marks) {
     solver_->evaluate_device(n_, array(kX), array(kY), array(kZ), array(kM), array(kAx),
                              array(kAy), array(kAz), stream_, count, marks);
+}
+
+namespace {
+// Checkpoint order (m x y z vx vy vz ax ay az) as System arrays.
+constexpr int kCheckpointOrder[10] = {System::kM,  System::kX,  System::kY,  System::kZ,
+                                      System::kVx, System::kVy, System::kVz, System::kAx,
+                                      System::kAy, System::kAz};
+} // namespace
+
+void System::snapshot(double *const *arrays) {
+    check(cudaStreamSynchronize(stream_), "finishing the steps before a snapshot");
+    for (int k = 0; k < 10 && n_ > 0; ++k) {
+        check(cudaMemcpyAsync(arrays[k], array(kCheckpointOrder[k]), sizeof(double) * n_,
+                              cudaMemcpyDeviceToHost, stream_),
+              "downloading state");
+    }
+    check(cudaStreamSynchronize(stream_), "downloading state");
+}
+
+void System::restore(const double *const *arrays) {
+    for (int k = 0; k < 10 && n_ > 0; ++k) {
+        check(cudaMemcpyAsync(array(kCheckpointOrder[k]), arrays[k], sizeof(double) * n_,
+                              cudaMemcpyHostToDevice, stream_),
+              "uploading state");
+    }
+    check(cudaStreamSynchronize(stream_), "uploading state");
 }
 
 void System::get_state(double *const *out) {
@@ -857,6 +884,186 @@ int ob_batch_stream(ob_batch *batch, void **stream) {
         require(batch != nullptr && stream != nullptr, "NULL argument");
         *stream = batch->impl->stream();
     });
+}
+
+// --------------------------------------------------------------------------
+// Run output: ORRERYCK checkpoints and ORRERYTJ trajectories (output.hpp)
+// --------------------------------------------------------------------------
+
+int ob_checkpoint_write(const char *path, uint64_t step, const char *configuration,
+                        uint64_t configuration_bytes, uint64_t n, const double *m,
+                        const double *x, const double *y, const double *z, const double *vx,
+                        const double *vy, const double *vz, const double *ax, const double *ay,
+                        const double *az) {
+    return guarded([&] {
+        require(path != nullptr, "path is NULL");
+        require(configuration != nullptr || configuration_bytes == 0, "configuration is NULL");
+        const double *arrays[ob::kCheckpointArrays] = {m, x, y, z, vx, vy, vz, ax, ay, az};
+        ob::write_checkpoint_file(path, step, std::string(configuration ? configuration : "",
+                                                          configuration_bytes),
+                                  n, arrays);
+    });
+}
+
+int ob_checkpoint_info(const char *path, uint64_t *step, uint64_t *n,
+                       uint64_t *configuration_bytes) {
+    return guarded([&] {
+        require(path != nullptr, "path is NULL");
+        const ob::CheckpointHeader h = ob::read_checkpoint_file(path, nullptr, 0);
+        if (step != nullptr) *step = h.step;
+        if (n != nullptr) *n = h.n;
+        if (configuration_bytes != nullptr) *configuration_bytes = h.configuration.size();
+    });
+}
+
+int ob_checkpoint_read(const char *path, char *configuration, uint64_t configuration_capacity,
+                       uint64_t n, double *m, double *x, double *y, double *z, double *vx,
+                       double *vy, double *vz, double *ax, double *ay, double *az) {
+    return guarded([&] {
+        require(path != nullptr, "path is NULL");
+        double *const arrays[ob::kCheckpointArrays] = {m, x, y, z, vx, vy, vz, ax, ay, az};
+        for (double *a : arrays) {
+            require(n == 0 || a != nullptr, "every state array is required");
+        }
+        const ob::CheckpointHeader h = ob::read_checkpoint_file(path, arrays, n);
+        if (configuration != nullptr) {
+            require(h.configuration.size() <= configuration_capacity,
+                    "the configuration buffer is too small (see ob_checkpoint_info)");
+            std::memcpy(configuration, h.configuration.data(), h.configuration.size());
+        }
+    });
+}
+
+int ob_system_write_checkpoint(ob_system *system, const char *path, uint64_t step,
+                               const char *configuration, uint64_t configuration_bytes) {
+    return guarded([&] {
+        require(system != nullptr && path != nullptr, "NULL argument");
+        require(configuration != nullptr || configuration_bytes == 0, "configuration is NULL");
+        const uint64_t n = system->impl->size();
+        std::vector<double> host(10 * n);
+        double *arrays[ob::kCheckpointArrays];
+        for (int k = 0; k < ob::kCheckpointArrays; ++k) {
+            arrays[k] = host.data() + k * n;
+        }
+        system->impl->snapshot(arrays);
+        const double *const *in = arrays;
+        ob::write_checkpoint_file(path, step, std::string(configuration ? configuration : "",
+                                                          configuration_bytes),
+                                  n, in);
+    });
+}
+
+int ob_system_read_checkpoint(ob_system *system, const char *path, uint64_t *step,
+                              char *configuration, uint64_t configuration_capacity,
+                              uint64_t *configuration_bytes) {
+    return guarded([&] {
+        require(system != nullptr && path != nullptr, "NULL argument");
+        const uint64_t n = system->impl->size();
+        std::vector<double> host(10 * n);
+        double *arrays[ob::kCheckpointArrays];
+        for (int k = 0; k < ob::kCheckpointArrays; ++k) {
+            arrays[k] = host.data() + k * n;
+        }
+        const ob::CheckpointHeader h = ob::read_checkpoint_file(path, arrays, n);
+        if (configuration != nullptr) {
+            require(h.configuration.size() <= configuration_capacity,
+                    "the configuration buffer is too small (see ob_checkpoint_info)");
+            std::memcpy(configuration, h.configuration.data(), h.configuration.size());
+        }
+        const double *const *in = arrays;
+        system->impl->restore(in);
+        if (step != nullptr) *step = h.step;
+        if (configuration_bytes != nullptr) *configuration_bytes = h.configuration.size();
+    });
+}
+
+} // extern "C"
+
+struct ob_trajectory {
+    std::unique_ptr<ob::TrajectoryFile> host;     // host-array frames only
+    std::unique_ptr<ob::DeviceTrajectory> device; // bound to a system
+};
+
+extern "C" {
+
+int ob_trajectory_create(const char *path, uint64_t n, const double *masses, double timestep,
+                         int32_t with_velocities, ob_trajectory **out) {
+    return guarded([&] {
+        require(path != nullptr && out != nullptr, "NULL argument");
+        *out = nullptr;
+        auto t = std::make_unique<ob_trajectory>();
+        t->host = std::make_unique<ob::TrajectoryFile>(path, n, masses, timestep,
+                                                       with_velocities != 0);
+        *out = t.release();
+    });
+}
+
+int ob_trajectory_create_for_system(const char *path, ob_system *system, double timestep,
+                                    int32_t with_velocities, ob_trajectory **out) {
+    return guarded([&] {
+        require(path != nullptr && system != nullptr && out != nullptr, "NULL argument");
+        *out = nullptr;
+        auto t = std::make_unique<ob_trajectory>();
+        t->device = std::make_unique<ob::DeviceTrajectory>(path, *system->impl, timestep,
+                                                           with_velocities != 0);
+        *out = t.release();
+    });
+}
+
+int ob_trajectory_write_frame(ob_trajectory *trajectory, uint64_t step, double time,
+                              const double *x, const double *y, const double *z,
+                              const double *vx, const double *vy, const double *vz) {
+    return guarded([&] {
+        require(trajectory != nullptr, "trajectory is NULL");
+        const double *xyz[3] = {x, y, z};
+        const double *v[3] = {vx, vy, vz};
+        if (trajectory->device) {
+            trajectory->device->write_host_frame(step, time, xyz, v);
+            return;
+        }
+        ob::TrajectoryFile &f = *trajectory->host;
+        for (int c = 0; c < 3; ++c) {
+            require(f.size() == 0 || (xyz[c] != nullptr &&
+                                      (!f.with_velocities() || v[c] != nullptr)),
+                    "a frame needs every array the file carries");
+        }
+        f.write_frame(step, time, xyz, v);
+    });
+}
+
+int ob_trajectory_write_system_frame(ob_trajectory *trajectory, uint64_t step, double time) {
+    return guarded([&] {
+        require(trajectory != nullptr, "trajectory is NULL");
+        require(trajectory->device != nullptr, "the trajectory is not bound to a system");
+        trajectory->device->write_frame(step, time);
+    });
+}
+
+int ob_trajectory_flush(ob_trajectory *trajectory) {
+    return guarded([&] {
+        require(trajectory != nullptr, "trajectory is NULL");
+        if (trajectory->device) {
+            trajectory->device->flush();
+        } else {
+            trajectory->host->flush();
+        }
+    });
+}
+
+int ob_trajectory_frames(ob_trajectory *trajectory, uint64_t *frames) {
+    return guarded([&] {
+        require(trajectory != nullptr && frames != nullptr, "NULL argument");
+        *frames = trajectory->device ? trajectory->device->frames() : trajectory->host->frames();
+    });
+}
+
+int ob_trajectory_close(ob_trajectory *trajectory) {
+    if (trajectory == nullptr) {
+        return OB_OK;
+    }
+    const int rc = ob_trajectory_flush(trajectory);
+    delete trajectory;
+    return rc;
 }
 
 } // extern "C"

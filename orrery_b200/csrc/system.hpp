@@ -32,6 +32,12 @@ public:
                    const double *vy, const double *vz, const double *m);
     void set_accelerations(const double *ax, const double *ay, const double *az);
     void get_state(double *const *out); // x y z vx vy vz ax ay az, NULL entries skipped
+    // The ten state arrays in a checkpoint's order: m x y z vx vy vz ax ay az.
+    void snapshot(double *const *arrays);
+    // Installs a checkpoint's ten arrays as they are; the accelerations are the
+    // ones the run carried, not re-evaluated (sim::Simulation::restore with
+    // accelerations_are_current, include/orrery/sim/simulation.hpp:101-102).
+    void restore(const double *const *arrays);
     void refresh();
     void step_async(int integrator, double dt, uint64_t steps);
     // Uploads x y z vx vy vz ax ay az (io) and m, steps, downloads io.
