@@ -53,9 +53,12 @@ extern "C" {
 #define OB_PRECISION_FP64 2
 
 /* Integrators (src/integrators/velocity_verlet.cpp:59-72,
- * src/integrators/yoshida4.cpp:45-59). */
+ * src/integrators/yoshida4.cpp:45-59, src/integrators/runge_kutta4.cpp:64-139).
+ * RK4 takes four force evaluations a step; batches and the server run VV and
+ * Yoshida-4. */
 #define OB_INTEGRATOR_VV 0
 #define OB_INTEGRATOR_YOSHIDA4 1
+#define OB_INTEGRATOR_RK4 2
 
 /* Solver parameters. Mirrors core::Softening (softening.hpp:50-60), which
  * stores the square of the softening length -- pass Softening::squared() so

@@ -112,7 +112,7 @@ class Restatement:
         lib.oc_barnes_hut_targets.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double,
                                               C.c_double, C.c_uint64, C.c_int, C.c_size_t,
                                               _u64p, _dp, _u64p, _u64p]
-        for name in ("oc_vv_step_direct", "oc_yoshida_step_direct"):
+        for name in ("oc_vv_step_direct", "oc_yoshida_step_direct", "oc_rk4_step_direct"):
             getattr(lib, name).argtypes = [C.c_size_t] + [_dp] * 10 + [C.c_double, C.c_double,
                                                                        C.POINTER(Counts)]
         lib.oc_yoshida_weights.argtypes = [_dp, _dp]
@@ -232,8 +232,8 @@ class Restatement:
     def integrate_direct(self, state, m, softening, dt, steps, integrator="vv"):
         """Advance ``state`` (dict of x y z vx vy vz ax ay az arrays, copied) in place."""
         s = {k: np.ascontiguousarray(v, dtype=np.float64).copy() for k, v in state.items()}
-        fn = self.lib.oc_yoshida_step_direct if integrator == "yoshida4" else \
-            self.lib.oc_vv_step_direct
+        fn = {"yoshida4": self.lib.oc_yoshida_step_direct, "rk4": self.lib.oc_rk4_step_direct,
+              "vv": self.lib.oc_vv_step_direct}[integrator]
         counts = Counts()
         for _ in range(steps):
             fn(len(m), *(_d(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")),
@@ -465,7 +465,7 @@ class Reference:
         s = {k: np.ascontiguousarray(v, dtype=np.float64).copy() for k, v in state.items()}
         self.lib.ref_integrate_direct(
             len(m), *(_d(s[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")),
-            _d(m), softening, dt, steps, 1 if integrator == "yoshida4" else 0,
+            _d(m), softening, dt, steps, {"vv": 0, "yoshida4": 1, "rk4": 2}[integrator],
             1 if kernel == "avx2" else 0)
         return s
 

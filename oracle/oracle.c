@@ -688,6 +688,55 @@ void oc_yoshida_step_direct(size_t n, double *x, double *y, double *z, double *v
     oc_vv_step_direct(n, x, y, z, vx, vy, vz, ax, ay, az, m, softening, outer * dt, counts);
 }
 
+/* RungeKutta4::step (runge_kutta4.cpp:64-139) with the direct field: stages at
+ * h/2, h/2 and h from the step's start (x0, v0), each moving the state to
+ * x0 + s v and v0 + s a with the previous stage's v and a, derivative sums
+ * weighted 1, 2, 2, 1, the state set to x0 + (h/6) S, and a last evaluation
+ * so that the carried accelerations belong to the final positions. */
+void oc_rk4_step_direct(size_t n, double *x, double *y, double *z, double *vx, double *vy,
+                        double *vz, double *ax, double *ay, double *az, const double *m,
+                        double softening, double dt, oc_counts *counts) {
+    double *p[3] = {x, y, z}, *v[3] = {vx, vy, vz}, *a[3] = {ax, ay, az};
+    double *start = malloc(sizeof(double) * 12 * (n ? n : 1));
+    double *x0 = start, *v0 = start + 3 * n, *sx = start + 6 * n, *sv = start + 9 * n;
+    for (int c = 0; c < 3; ++c) {
+        for (size_t i = 0; i < n; ++i) {
+            x0[c * n + i] = p[c][i];
+            v0[c * n + i] = v[c][i];
+            sx[c * n + i] = v[c][i];
+            sv[c * n + i] = a[c][i];
+        }
+    }
+    const double scales[3] = {dt / 2.0, dt / 2.0, dt};
+    const double weights[3] = {2.0, 2.0, 1.0};
+    for (int stage = 0; stage < 3; ++stage) {
+        const double s = scales[stage];
+        for (int c = 0; c < 3; ++c) {
+            for (size_t i = 0; i < n; ++i) {
+                const double stage_v = v[c][i];
+                p[c][i] = x0[c * n + i] + (s * stage_v);
+                v[c][i] = v0[c * n + i] + (s * a[c][i]);
+            }
+        }
+        oc_direct(n, x, y, z, m, softening, ax, ay, az, counts);
+        for (int c = 0; c < 3; ++c) {
+            for (size_t i = 0; i < n; ++i) {
+                sx[c * n + i] += weights[stage] * v[c][i];
+                sv[c * n + i] += weights[stage] * a[c][i];
+            }
+        }
+    }
+    const double sixth = dt / 6.0;
+    for (int c = 0; c < 3; ++c) {
+        for (size_t i = 0; i < n; ++i) {
+            p[c][i] = x0[c * n + i] + (sixth * sx[c * n + i]);
+            v[c][i] = v0[c * n + i] + (sixth * sv[c * n + i]);
+        }
+    }
+    oc_direct(n, x, y, z, m, softening, ax, ay, az, counts);
+    free(start);
+}
+
 /* ------------------------------------------------------------------------- */
 /* Energies (diagnostics.cpp:36-158)                                           */
 /* ------------------------------------------------------------------------- */

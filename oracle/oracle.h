@@ -125,6 +125,11 @@ void oc_yoshida_step_direct(size_t n, double *x, double *y, double *z, double *v
                             double *vz, double *ax, double *ay, double *az, const double *m,
                             double softening, double dt, oc_counts *counts);
 
+/* RungeKutta4::step (runge_kutta4.cpp:64-139) with the direct field. */
+void oc_rk4_step_direct(size_t n, double *x, double *y, double *z, double *vx, double *vy,
+                        double *vz, double *ax, double *ay, double *az, const double *m,
+                        double softening, double dt, oc_counts *counts);
+
 /* Yoshida-4 substep weights (yoshida4.cpp:24-30). */
 void oc_yoshida_weights(double *outer, double *inner);
 

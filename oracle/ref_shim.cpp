@@ -20,6 +20,7 @@
 #include "orrery/core/random.hpp"
 #include "orrery/core/softening.hpp"
 #include "orrery/initial_conditions/plummer.hpp"
+#include "orrery/integrators/runge_kutta4.hpp"
 #include "orrery/integrators/velocity_verlet.hpp"
 #include "orrery/integrators/yoshida4.hpp"
 #include "orrery/solvers/barnes_hut_solver.hpp"
@@ -296,8 +297,11 @@ int ref_integrate_direct(std::size_t n, double* x, double* y, double* z, double*
     solver.select_kernel(kernel_for(kernel));
     orrery::integrators::VelocityVerlet vv;
     orrery::integrators::Yoshida4 y4;
+    orrery::integrators::RungeKutta4 rk4;
     orrery::integrators::Integrator& chosen =
-        integrator == 1 ? static_cast<orrery::integrators::Integrator&>(y4) : vv;
+        integrator == 1   ? static_cast<orrery::integrators::Integrator&>(y4)
+        : integrator == 2 ? static_cast<orrery::integrators::Integrator&>(rk4)
+                          : vv;
     for (std::uint64_t s = 0; s < steps; ++s) {
         chosen.step(data, dt, solver);
     }

@@ -42,10 +42,12 @@ PRECISION_SPLIT = 1
 PRECISION_FP64 = 2
 INTEGRATOR_VV = 0
 INTEGRATOR_YOSHIDA4 = 1
+INTEGRATOR_RK4 = 2
 
 _PRECISIONS = {"fp32": PRECISION_FP32, "split": PRECISION_SPLIT, "fp64": PRECISION_FP64}
 _INTEGRATORS = {"vv": INTEGRATOR_VV, "velocity-verlet": INTEGRATOR_VV,
-                "yoshida4": INTEGRATOR_YOSHIDA4}
+                "yoshida4": INTEGRATOR_YOSHIDA4, "rk4": INTEGRATOR_RK4,
+                "runge-kutta4": INTEGRATOR_RK4}
 
 
 class OrreryError(RuntimeError):

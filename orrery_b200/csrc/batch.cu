@@ -668,6 +668,9 @@ void Batch::enqueue_step(int integrator, double dt) {
 }
 
 void Batch::step_async(int integrator, double dt, uint64_t steps) {
+    if (integrator == OB_INTEGRATOR_RK4) {
+        throw Error(OB_ERROR_UNSUPPORTED, "batches step with VV or Yoshida-4 (RK4: ob_system_*)");
+    }
     if (integrator != OB_INTEGRATOR_VV && integrator != OB_INTEGRATOR_YOSHIDA4) {
         throw Error(OB_ERROR_INVALID_ARGUMENT, "unknown integrator");
     }

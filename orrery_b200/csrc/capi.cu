@@ -197,7 +197,29 @@ static void yoshida_weights(double &outer, double &inner) {
 }
 
 int System::evaluations_per_step(int integrator) {
-    return integrator == OB_INTEGRATOR_YOSHIDA4 ? 3 : 1;
+    return integrator == OB_INTEGRATOR_YOSHIDA4 ? 3 : integrator == OB_INTEGRATOR_RK4 ? 4 : 1;
+}
+
+void System::enqueue_rk4_step(double dt, const cudaEvent_t *marks) {
+    // RungeKutta4::step (src/integrators/runge_kutta4.cpp:64-139): stages at
+    // h/2, h/2 and h weighted 2, 2, 1 after the first, the h/6 combination, and
+    // the evaluation that leaves the carried accelerations at the final state.
+    double *state[9];
+    for (int k = 0; k < 9; ++k) {
+        state[k] = array(kX + k);
+    }
+    double *save = rk4_.data();
+    const double half = dt / 2.0;
+    const double sixth = dt / 6.0;
+    auto mark = [&](int e) { return marks != nullptr ? marks + 4 * e : nullptr; };
+    check(launch_rk4_stage(0, state, save, n_, 0.0, half, stream_), "RK4 first stage");
+    evaluate(false, mark(0));
+    check(launch_rk4_stage(1, state, save, n_, 2.0, half, stream_), "RK4 second stage");
+    evaluate(false, mark(1));
+    check(launch_rk4_stage(1, state, save, n_, 2.0, dt, stream_), "RK4 third stage");
+    evaluate(false, mark(2));
+    check(launch_rk4_stage(2, state, save, n_, 1.0, sixth, stream_), "RK4 combination");
+    evaluate(false, mark(3));
 }
 
 void System::enqueue_substep(double timestep, const cudaEvent_t *marks) {
@@ -222,6 +244,8 @@ void System::enqueue_step(int integrator, double dt, bool marked) {
         enqueue_substep(outer * dt, m);
         enqueue_substep(inner * dt, marked ? m + 4 : nullptr);
         enqueue_substep(outer * dt, marked ? m + 8 : nullptr);
+    } else if (integrator == OB_INTEGRATOR_RK4) {
+        enqueue_rk4_step(dt, m);
     } else {
         enqueue_substep(dt, m);
     }
@@ -250,6 +274,9 @@ void System::ensure_graph(int integrator, double dt) {
         return;
     }
     drop_graph();
+    if (integrator == OB_INTEGRATOR_RK4) {
+        rk4_.reserve(12ull * (n_ == 0 ? 1 : n_)); // before the capture: no allocation inside it
+    }
     cudaGraph_t graph = capture_step(integrator, dt, false);
     size_t count = 0;
     cudaError_t err = cudaGraphGetNodes(graph, nullptr, &count);
@@ -325,7 +352,7 @@ void System::profile(uint32_t steps) {
     ring_.clear();
     ring_steps_ = steps;
     ring_used_ = 0;
-    const size_t per_step = 12; // enough for the largest step (Yoshida-4: 3 x 4)
+    const size_t per_step = kMarksPerStep;
     ring_.resize(per_step * steps, nullptr);
     for (auto &e : ring_) {
         check(cudaEventCreate(&e), "creating an event");
@@ -340,7 +367,7 @@ ob_timings System::phase_times(uint32_t &evaluations) {
     const size_t evals = mark_nodes_.size() / per_eval_marks;
     for (uint32_t s = 0; s < ring_used_; ++s) {
         for (size_t e = 0; e < evals; ++e) {
-            const cudaEvent_t *m = &ring_[s * 12 + e * 4];
+            const cudaEvent_t *m = &ring_[s * kMarksPerStep + e * 4];
             float a = 0, b = 0, c = 0;
             check(cudaEventElapsedTime(&a, m[0], m[1]), "phase timing");
             check(cudaEventElapsedTime(&b, m[1], m[2]), "phase timing");
@@ -360,14 +387,16 @@ ob_timings System::phase_times(uint32_t &evaluations) {
 }
 
 uint32_t System::step_kernels(int integrator, double dt) {
-    require(integrator == OB_INTEGRATOR_VV || integrator == OB_INTEGRATOR_YOSHIDA4,
+    require(integrator == OB_INTEGRATOR_VV || integrator == OB_INTEGRATOR_YOSHIDA4 ||
+                integrator == OB_INTEGRATOR_RK4,
             "unknown integrator");
     ensure_graph(integrator, dt);
     return graph_kernels_;
 }
 
 void System::step_async(int integrator, double dt, uint64_t steps) {
-    require(integrator == OB_INTEGRATOR_VV || integrator == OB_INTEGRATOR_YOSHIDA4,
+    require(integrator == OB_INTEGRATOR_VV || integrator == OB_INTEGRATOR_YOSHIDA4 ||
+                integrator == OB_INTEGRATOR_RK4,
             "unknown integrator");
     require(std::isfinite(dt), "the timestep must be finite");
     if (steps == 0 || n_ == 0) {
@@ -378,7 +407,7 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
     for (uint64_t s = 0; s < steps; ++s) {
         if (ring_used_ < ring_steps_) {
             ensure_marked_graph();
-            set_marks(ring_, static_cast<size_t>(ring_used_) * 12);
+            set_marks(ring_, static_cast<size_t>(ring_used_) * kMarksPerStep);
             ++ring_used_;
             check(cudaGraphLaunch(marked_graph_, stream_), "launching the profiled step graph");
         } else {

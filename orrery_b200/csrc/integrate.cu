@@ -47,6 +47,69 @@ __global__ void kick_kernel(double *__restrict__ vx, double *__restrict__ vy,
     }
 }
 
+// Classical Runge-Kutta 4 (src/integrators/runge_kutta4.cpp:64-139) as three
+// update kernels between the four force evaluations of a step. `save` holds
+// 12n doubles: the step's start x0 (x y z), v0 (vx vy vz) and the weighted
+// derivative sums Sx, Sv. Each moves the state to a stage as
+// advance_to_stage does (runge_kutta4.cpp:31-40): x = x0 + s v, v = v0 + s a,
+// with v and a those of the stage before.
+struct Rk4State {
+    double *p[3];
+    double *v[3];
+    const double *a[3];
+    double *save;
+    uint32_t n;
+};
+
+// The first stage: remember x0 and v0, seed the sums with v0 and a0 (the
+// first stage's derivatives, :101-102), move to the first midpoint.
+__global__ void rk4_begin_kernel(Rk4State s, double scale) {
+    const uint32_t n = s.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double x = s.p[c][i], v = s.v[c][i], a = s.a[c][i];
+            s.save[c * n + i] = x;
+            s.save[(3 + c) * n + i] = v;
+            s.save[(6 + c) * n + i] = v;
+            s.save[(9 + c) * n + i] = a;
+            s.p[c][i] = __dadd_rn(x, __dmul_rn(scale, v));
+            s.v[c][i] = __dadd_rn(v, __dmul_rn(scale, a));
+        }
+    }
+}
+
+// Adds the stage just evaluated to the sums with `weight` (accumulate_component,
+// :42-46), then moves to the next stage.
+__global__ void rk4_next_kernel(Rk4State s, double weight, double scale) {
+    const uint32_t n = s.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double v = s.v[c][i], a = s.a[c][i];
+            s.save[(6 + c) * n + i] = __dadd_rn(s.save[(6 + c) * n + i], __dmul_rn(weight, v));
+            s.save[(9 + c) * n + i] = __dadd_rn(s.save[(9 + c) * n + i], __dmul_rn(weight, a));
+            s.p[c][i] = __dadd_rn(s.save[c * n + i], __dmul_rn(scale, v));
+            s.v[c][i] = __dadd_rn(s.save[(3 + c) * n + i], __dmul_rn(scale, a));
+        }
+    }
+}
+
+// Adds the last stage, then sets x = x0 + scale Sx, v = v0 + scale Sv
+// (combine_component, :48-53, with scale h/6).
+__global__ void rk4_finish_kernel(Rk4State s, double weight, double scale) {
+    const uint32_t n = s.n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double sx = __dadd_rn(s.save[(6 + c) * n + i], __dmul_rn(weight, s.v[c][i]));
+            const double sv = __dadd_rn(s.save[(9 + c) * n + i], __dmul_rn(weight, s.a[c][i]));
+            s.p[c][i] = __dadd_rn(s.save[c * n + i], __dmul_rn(scale, sx));
+            s.v[c][i] = __dadd_rn(s.save[(3 + c) * n + i], __dmul_rn(scale, sv));
+        }
+    }
+}
+
 // Per-particle kinetic terms m |v|^2 (src/core/diagnostics.cpp:118-127); the
 // host sums them in index order with the reference's Neumaier summation.
 __global__ void kinetic_terms_kernel(const double *__restrict__ vx, const double *__restrict__ vy,
@@ -122,6 +185,26 @@ cudaError_t launch_kick(double *vx, double *vy, double *vz, const double *ax, co
         return cudaSuccess;
     }
     kick_kernel<<<blocks_for(n), kThreads, 0, stream>>>(vx, vy, vz, ax, ay, az, n, h);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_rk4_stage(int phase, double *const *state, double *save, uint32_t n,
+                             double weight, double scale, cudaStream_t stream) {
+    if (n == 0) {
+        return cudaSuccess;
+    }
+    const Rk4State s{{state[0], state[1], state[2]},
+                     {state[3], state[4], state[5]},
+                     {state[6], state[7], state[8]},
+                     save,
+                     n};
+    if (phase == 0) {
+        rk4_begin_kernel<<<blocks_for(n), kThreads, 0, stream>>>(s, scale);
+    } else if (phase == 1) {
+        rk4_next_kernel<<<blocks_for(n), kThreads, 0, stream>>>(s, weight, scale);
+    } else {
+        rk4_finish_kernel<<<blocks_for(n), kThreads, 0, stream>>>(s, weight, scale);
+    }
     return cudaGetLastError();
 }
 

@@ -61,6 +61,12 @@ cudaError_t launch_kick_drift(double *x, double *y, double *z, double *vx, doubl
                               uint32_t n, double h, double dt, cudaStream_t stream);
 cudaError_t launch_kick(double *vx, double *vy, double *vz, const double *ax, const double *ay,
                         const double *az, uint32_t n, double h, cudaStream_t stream);
+// One of the three RK4 update kernels between force evaluations: phase 0
+// starts the step and moves to the first stage, 1 accumulates a stage and moves
+// to the next, 2 accumulates the last and combines. `state` = x y z vx vy vz
+// ax ay az; `save` holds 12n doubles.
+cudaError_t launch_rk4_stage(int phase, double *const *state, double *save, uint32_t n,
+                             double weight, double scale, cudaStream_t stream);
 
 // Energies: per-block partial sums written to `partials` (length returned by
 // energy_partials_needed); the host folds them with Neumaier summation.

@@ -239,6 +239,9 @@ private:
         if (spec.kind != OB_SOLVER_DIRECT && spec.kind != OB_SOLVER_TREE) {
             throw Error(OB_ERROR_INVALID_ARGUMENT, "unknown job kind");
         }
+        if (spec.integrator == OB_INTEGRATOR_RK4) {
+            throw Error(OB_ERROR_UNSUPPORTED, "served jobs step with VV or Yoshida-4");
+        }
         if (spec.integrator != OB_INTEGRATOR_VV && spec.integrator != OB_INTEGRATOR_YOSHIDA4) {
             throw Error(OB_ERROR_INVALID_ARGUMENT, "unknown integrator");
         }

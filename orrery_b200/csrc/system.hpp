@@ -64,6 +64,7 @@ private:
     void evaluate(bool count, const cudaEvent_t *marks = nullptr);
     void enqueue_substep(double timestep, const cudaEvent_t *marks);
     void enqueue_step(int integrator, double dt, bool marked);
+    void enqueue_rk4_step(double dt, const cudaEvent_t *marks);
     cudaGraph_t capture_step(int integrator, double dt, bool marked);
     void drop_graph();
     void ensure_graph(int integrator, double dt);
@@ -74,6 +75,7 @@ private:
     uint32_t n_;
     DeviceArray<double> state_;
     DeviceArray<double> terms_;
+    DeviceArray<double> rk4_; // RK4: x0, v0 and the derivative sums (12n), reserved on first use
     cudaStream_t stream_ = nullptr;
     bool owns_stream_ = true;
     // The step as a CUDA graph, without event nodes: what every step replays
@@ -92,6 +94,7 @@ private:
     cudaGraphExec_t marked_graph_ = nullptr;
     std::vector<cudaEvent_t> marks_;
     std::vector<cudaGraphNode_t> mark_nodes_;
+    static constexpr size_t kMarksPerStep = 16; // four per evaluation, RK4's four at most
     std::vector<cudaEvent_t> ring_;
     uint32_t ring_steps_ = 0;     // capacity in steps
     uint32_t ring_used_ = 0;      // steps recorded

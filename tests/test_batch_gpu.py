@@ -107,6 +107,13 @@ def test_energy_is_conserved_per_system(b200):
         assert abs(e - e0[k]) / abs(e0[k]) < 1e-6
 
 
+def test_batches_refuse_rk4(b200):
+    batch = b200.DeviceBatch([600], [0.01])
+    with pytest.raises(b200.OrreryError) as err:
+        batch.step(1e-3, 1, "rk4")
+    assert err.value.code == b200.ERROR_UNSUPPORTED
+
+
 def test_mass_beyond_the_fp32_range_is_refused(b200):
     # The batched kernel adds a target's own entry as f * 0 with f = m / eps^3
     # in FP32: a mass that makes f overflow would turn that zero into NaN.

@@ -13,9 +13,12 @@ Three kinds of check:
 from __future__ import annotations
 
 import math
+import os
 
 import numpy as np
 import pytest
+
+from conftest import GOLDEN
 
 
 # --------------------------------------------------------------------------
@@ -253,6 +256,29 @@ def test_integrators_match_reference_bitwise(restatement, golden_trajectory, int
     for k in keys:
         assert np.array_equal(out[k], g[f"{tag}_{k}"]), k
     assert counts.evaluations == steps * (3 if integrator == "yoshida4" else 1)
+
+
+def test_rk4_matches_reference_bitwise(restatement, golden_trajectory):
+    # tests/golden/trajectory_rk4_512.npz: the reference's RungeKutta4
+    # (runge_kutta4.cpp:64-139), 10 steps from the same start.
+    g = golden_trajectory
+    rk4 = dict(np.load(os.path.join(GOLDEN, "trajectory_rk4_512.npz")))
+    keys = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+    state = {k: g[f"start_{k}"] for k in keys}
+    out, counts = restatement.integrate_direct(state, g["m"], 0.01, 1e-3, 10, "rk4")
+    for k in keys:
+        assert np.array_equal(out[k], rk4[f"rk4_10_{k}"]), k
+    assert counts.evaluations == 10 * 4
+
+
+def test_rk4_matches_live_reference(restatement, reference):
+    d = reference.plummer(257, 1.0, 1.0, 77)
+    a0, _ = reference.direct(d["x"], d["y"], d["z"], d["m"], 0.02, kernel="scalar")
+    state = dict(x=d["x"], y=d["y"], z=d["z"], vx=d["vx"], vy=d["vy"], vz=d["vz"],
+                 ax=a0[:, 0].copy(), ay=a0[:, 1].copy(), az=a0[:, 2].copy())
+    mine, _ = restatement.integrate_direct(state, d["m"], 0.02, 2e-3, 4, "rk4")
+    theirs = reference.integrate_direct(state, d["m"], 0.02, 2e-3, 4, "rk4")
+    assert all(np.array_equal(mine[k], theirs[k]) for k in state)
 
 
 def test_energies_match_reference_bitwise(restatement, golden_plummer):

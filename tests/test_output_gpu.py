@@ -57,7 +57,8 @@ def test_system_checkpoint_is_the_host_checkpoint_of_its_state(b200, tmp_path):
 
 
 @pytest.mark.parametrize("kind,integrator,n", [("fp64", "vv", 400), ("fp32", "yoshida4", 1000),
-                                                ("split", "yoshida4", 700), ("tree", "vv", 5000)])
+                                                ("split", "yoshida4", 700), ("tree", "vv", 5000),
+                                                ("fp64", "rk4", 300), ("tree", "rk4", 3000)])
 def test_resumed_run_continues_bit_for_bit(b200, tmp_path, kind, integrator, n):
     a, d = make_system(b200, kind, n)
     a.step(1e-3, 6, integrator)

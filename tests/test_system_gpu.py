@@ -55,7 +55,39 @@ def test_steps_split_across_calls_equal_one_call(b200, golden_trajectory):
     assert all(np.array_equal(sa[k], sb[k]) for k in KEYS)
 
 
-@pytest.mark.parametrize("integrator", ["vv", "yoshida4"])
+def test_fp64_rk4_trajectory_is_bit_identical(b200, golden_trajectory):
+    # tests/golden/trajectory_rk4_512.npz: the reference's RungeKutta4 over its
+    # scalar DirectSolver, 10 steps of dt 1e-3 from the same start.
+    import os
+    from conftest import GOLDEN
+    rk4 = dict(np.load(os.path.join(GOLDEN, "trajectory_rk4_512.npz")))
+    s = _system(b200, golden_trajectory, "fp64")
+    s.step(1e-3, 10, "rk4")
+    st = s.state()
+    for k in KEYS:
+        assert np.array_equal(st[k], rk4[f"rk4_10_{k}"]), k
+    c = s.interaction_count()
+    assert c.evaluations == 1 + 10 * 4
+
+
+def test_rk4_over_the_tree_follows_the_exact_field(b200, golden_trajectory):
+    # Barnes-Hut forces (theta 0.5, quadrupoles) carry ~1e-3 relative errors;
+    # over five RK4 steps of 1e-3 they move positions by far less than 1e-6.
+    g = golden_trajectory
+    n = len(g["m"])
+    t = b200.DeviceSystem(n, 0.01, b200.SOLVER_TREE, "fp32", 0.5, 32, True)
+    t.set_state(g["start_x"], g["start_y"], g["start_z"], g["start_vx"], g["start_vy"],
+                g["start_vz"], g["m"])
+    e = _system(b200, g, "fp64")
+    t.step(1e-3, 5, "rk4")
+    e.step(1e-3, 5, "rk4")
+    st, se = t.state(), e.state()
+    for k in ("x", "y", "z"):
+        assert np.max(np.abs(st[k] - se[k])) < 1e-6, k
+    assert t.interaction_count().evaluations == 1 + 5 * 4
+
+
+@pytest.mark.parametrize("integrator", ["vv", "yoshida4", "rk4"])
 def test_host_state_steps_equal_resident_steps(b200, golden_trajectory, integrator):
     # Integrator::step over host arrays (upload, device step, download) is the
     # resident step: the carried accelerations make each call independent.
