@@ -65,6 +65,12 @@ WORKLOADS = {
                             theta=0.5, leaf=32, quadrupole=True, precision="fp32",
                             metric="BH ms/step at 2M", unit="ms/step", higher=False,
                             generator="collision"),
+    # The parity mode: forces bit-identical to the reference's FP64
+    # BarnesHutSolver (scalar leaf kernel).
+    "bh-collision-2m-fp64": dict(kind="tree", n=2_000_000, eps=0.02, dt=5e-4, integrator="vv",
+                                 theta=0.5, leaf=32, quadrupole=True, precision="fp64",
+                                 metric="BH ms/step at 2M (FP64 parity)", unit="ms/step",
+                                 higher=False, generator="collision"),
     # The same scenario at a quarter of the size, for profiler captures.
     "bh-collision-500k": dict(kind="tree", n=500_000, eps=0.02, dt=5e-4, integrator="vv",
                               theta=0.5, leaf=32, quadrupole=True, precision="fp32",
@@ -712,7 +718,8 @@ def e2e_drop_in(ob, w, data, steps, torch):
     if w["kind"] == "direct":
         solver = ob.B200DirectSolver(w["eps"], w["precision"])
     else:
-        solver = ob.B200TreeSolver(w["eps"], w["theta"], w["leaf"], w["quadrupole"])
+        solver = ob.B200TreeSolver(w["eps"], w["theta"], w["leaf"], w["quadrupole"],
+                                   w["precision"])
     solver.evaluate((x, y, z), m, (ax, ay, az))
     weights = [w["dt"]]
     if w["integrator"] == "yoshida4":
@@ -1202,16 +1209,29 @@ def run_b200(args, w):
         # term and 16 (monopole) or 39 (with quadrupole) per particle-cell
         # term, against the measured FFMA lane rate. Its HBM figures are
         # reported beside it.
-        ffma, _ = ob.probe_fp32()
         hbm, src = load_peaks()
         evals_done = max(1, K * evaluations_per_step(w))
-        ops = (12 * pair_count + (39 if w["quadrupole"] else 16) * cell_count) / evals_done
+        if w["precision"] == "fp64":
+            # The parity walk's FP64 operations by the reference's arithmetic
+            # (square root and divide counted as one each): 20 per pair term,
+            # 20 per monopole and 41 more per quadrupole cell term, against
+            # the measured DFMA lane rate.
+            peak = ob.probe_fp64()
+            ops = (20 * pair_count + (61 if w["quadrupole"] else 20) * cell_count) / evals_done
+            bound, unit, src_peak = ("fp64-pipe", "T FP64 op/s",
+                                     "measured DFMA lane rate on this GPU (ob_probe_fp64)")
+        else:
+            peak, _ = ob.probe_fp32()
+            ops = (12 * pair_count + (39 if w["quadrupole"] else 16) * cell_count) / evals_done
+            bound, unit, src_peak = ("fp32-fma-pipe", "T FP32 op/s",
+                                     "measured FFMA lane rate on this GPU (ob_probe_fp32)")
         achieved_t = ops / (kernel_ms * 1e-3) / 1e12
-        roofline = {"bound": "fp32-fma-pipe", "achieved": achieved_t, "peak": ffma / 1e12,
-                    "unit": "T FP32 op/s", "frac": achieved_t / (ffma / 1e12),
-                    "peak_source": "measured FFMA lane rate on this GPU (ob_probe_fp32)",
-                    "algorithmic_fp32_ops": ops, "kernel_ms": kernel_ms,
-                    "traffic": TRAFFIC_BYTES[("walk", "fp32")](n),
+        roofline = {"bound": bound, "achieved": achieved_t, "peak": peak / 1e12,
+                    "unit": unit, "frac": achieved_t / (peak / 1e12),
+                    "peak_source": src_peak,
+                    "algorithmic_ops": ops, "kernel_ms": kernel_ms,
+                    "traffic": TRAFFIC_BYTES[("walk", "fp32")](n) if w["precision"] == "fp32"
+                    else None,
                     "hbm": {"peak": hbm, "unit": "GB/s",
                             "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs, a copy "
                                            "kernel)"}}

@@ -459,6 +459,10 @@ int ob_probe_fp32(double *ffma_lane_per_s, double *rsqrt_lane_per_s);
  * counts as two), for comparison with the scalar FFMA rate. */
 int ob_probe_fp32x2(double *ffma2_flop_lanes_per_s);
 
+/* Measured FP64 FMA lane operations per second on the current device: the
+ * denominator of the FP64 (parity-mode) tree walk's roofline. */
+int ob_probe_fp64(double *dfma_lane_per_s);
+
 #ifdef __cplusplus
 }
 #endif

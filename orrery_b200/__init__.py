@@ -174,6 +174,7 @@ def load_library():
     lib.ob_system_size.argtypes = [vp, C.POINTER(C.c_uint64)]
     lib.ob_probe_fp32.argtypes = [_dp, _dp]
     lib.ob_probe_fp32x2.argtypes = [_dp]
+    lib.ob_probe_fp64.argtypes = [_dp]
     _u64p = C.POINTER(C.c_uint64)
     lib.ob_tree_stats.argtypes = [vp, _u64p, _u64p, C.POINTER(C.c_uint32)]
     lib.ob_tree_copy.argtypes = [vp, _dp, _u64p, _dp]
@@ -376,13 +377,17 @@ class B200DirectSolver(_Solver):
 
 
 class B200TreeSolver(_Solver):
-    """Barnes-Hut solver (the reference's BarnesHutSolver / CudaTreeSolver)."""
+    """Barnes-Hut solver (the reference's BarnesHutSolver / CudaTreeSolver).
+
+    ``precision="fp32"`` computes FP32 forces on FP64 state; ``"fp64"`` is the
+    parity mode, whose forces equal BarnesHutSolver's (scalar leaf kernel) bit
+    for bit."""
 
     _name = "b200-tree"
 
     def __init__(self, softening: float = 0.0, opening_angle: float = 0.5,
-                 leaf_capacity: int = 32, quadrupole: bool = False):
-        super().__init__(make_params(SOLVER_TREE, "fp32", softening, opening_angle,
+                 leaf_capacity: int = 32, quadrupole: bool = False, precision: str = "fp32"):
+        super().__init__(make_params(SOLVER_TREE, precision, softening, opening_angle,
                                      leaf_capacity, quadrupole))
 
     def tree_stats(self):
@@ -418,9 +423,9 @@ class B200TreeSolver(_Solver):
 
     @classmethod
     def try_create(cls, softening: float = 0.0, opening_angle: float = 0.5,
-                   leaf_capacity: int = 32, quadrupole: bool = False):
+                   leaf_capacity: int = 32, quadrupole: bool = False, precision: str = "fp32"):
         try:
-            return cls(softening, opening_angle, leaf_capacity, quadrupole)
+            return cls(softening, opening_angle, leaf_capacity, quadrupole, precision)
         except OrreryError as e:
             if e.code == ERROR_NO_DEVICE:
                 return None
@@ -584,6 +589,13 @@ def probe_fp32():
     a, b = C.c_double(), C.c_double()
     _check(load_library().ob_probe_fp32(C.byref(a), C.byref(b)))
     return a.value, b.value
+
+
+def probe_fp64() -> float:
+    """Measured FP64 FMA lane operations per second of the current device."""
+    r = C.c_double()
+    _check(load_library().ob_probe_fp64(C.byref(r)))
+    return r.value
 
 
 def probe_fp32x2() -> float:
@@ -857,7 +869,7 @@ def compute_accelerations(positions, masses, softening: float = 0.0, solver: str
     if solver == "direct":
         s = B200DirectSolver(softening, precision)
     elif solver in ("tree", "barnes-hut"):
-        s = B200TreeSolver(softening, opening_angle, leaf_capacity, quadrupole)
+        s = B200TreeSolver(softening, opening_angle, leaf_capacity, quadrupole, precision)
     else:
         raise ValueError(f"unknown solver {solver!r}")
     return s.evaluate(positions, masses)

@@ -32,6 +32,7 @@ EXTRA = {
     "integrate.cu": ["--fmad=false"],
     "tree.cu": ["--fmad=false"],
     "walk.cu": ["-ftz=true"],
+    "walk_f64.cu": ["--fmad=false"],
 }
 
 

@@ -86,6 +86,31 @@ __global__ void __launch_bounds__(kProbeThreads) rsqrt_probe(float *out, int ite
     }
 }
 
+// FP64 FMA (DFMA) lane operations: the FP64 pipe's rate, the denominator of
+// the parity-mode tree walk's roofline.
+__global__ void __launch_bounds__(kProbeThreads) dfma_probe(double *out, int iterations,
+                                                            double a, double b) {
+    double v[kChains];
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        v[k] = threadIdx.x * 1e-3 + k;
+    }
+    for (int it = 0; it < iterations; ++it) {
+#pragma unroll
+        for (int k = 0; k < kChains; ++k) {
+            v[k] = fma(v[k], a, b);
+        }
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < kChains; ++k) {
+        s += v[k];
+    }
+    if (s == 12345.678) {
+        out[threadIdx.x] = s;
+    }
+}
+
 template <typename Launch> double lane_ops_per_second(Launch launch, double ops) {
     cudaEvent_t a, b;
     check(cudaEventCreate(&a), "probe event");
@@ -152,6 +177,26 @@ extern "C" int ob_probe_fp32(double *ffma_lane_per_s, double *rsqrt_lane_per_s) 
                 [&] { ob::rsqrt_probe<<<blocks, ob::kProbeThreads>>>(sink, rsq_iterations); },
                 threads * rsq_iterations * ob::kChains);
         }
+        cudaFree(sink);
+        return OB_OK;
+    } catch (const ob::Error &e) {
+        return ob::set_error(e.code(), e.what());
+    }
+}
+
+extern "C" int ob_probe_fp64(double *dfma_lane_per_s) {
+    try {
+        int device = 0, sms = 0;
+        ob::check(cudaGetDevice(&device), "cudaGetDevice");
+        ob::check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "SMs");
+        double *sink = nullptr;
+        ob::check(cudaMalloc(&sink, ob::kProbeThreads * sizeof(double)), "probe buffer");
+        const int blocks = sms * 8;
+        const double threads = static_cast<double>(blocks) * ob::kProbeThreads;
+        const int iterations = 1 << 14;
+        *dfma_lane_per_s = ob::lane_ops_per_second(
+            [&] { ob::dfma_probe<<<blocks, ob::kProbeThreads>>>(sink, iterations, 0.999, 1e-3); },
+            threads * iterations * ob::kChains);
         cudaFree(sink);
         return OB_OK;
     } catch (const ob::Error &e) {

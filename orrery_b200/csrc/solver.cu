@@ -28,9 +28,10 @@ ob_solver_params corrected(const ob_solver_params &in) {
         p.precision != OB_PRECISION_FP64) {
         throw Error(OB_ERROR_INVALID_ARGUMENT, "unknown precision");
     }
-    if (p.kind == OB_SOLVER_TREE && p.precision != OB_PRECISION_FP32) {
+    if (p.kind == OB_SOLVER_TREE && p.precision == OB_PRECISION_SPLIT) {
         throw Error(OB_ERROR_UNSUPPORTED,
-                    "the tree solver computes FP32 forces on FP64 state (precision FP32)");
+                    "the tree solver computes FP32 forces (precision FP32) or the reference's "
+                    "FP64 forces (precision FP64)");
     }
     if (!(p.softening_squared >= 0.0) || !std::isfinite(p.softening_squared)) {
         throw Error(OB_ERROR_INVALID_ARGUMENT, "softening squared must be finite and >= 0");

@@ -603,7 +603,14 @@ void TreePipeline::evaluate(uint32_t n, const double *x, const double *y, const 
           "moments");
     record(built, stream, external);
 
-    // Traversal.
+    // Traversal: FP32 forces, or the FP64 parity walk.
+    if (params_.precision == OB_PRECISION_FP64) {
+        check(launch_walk_f64(nodes_.data(), params_.quadrupole ? quads_.data() : nullptr,
+                              sorted_.data(), perm, n, params_.softening_squared, ax, ay, az,
+                              meta_.data(), counters_.data(), status, stream),
+              "FP64 tree walk");
+        return;
+    }
     check(launch_walk(nodes_.data(), walk_nodes_.data(), first_of_.data(), leaf_rel_.data(),
                       sorted_.data(), perm, n, params_.softening_squared,
                       params_.quadrupole != 0, ax, ay, az, meta_.data(), counters_.data(),

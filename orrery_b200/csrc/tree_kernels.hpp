@@ -89,4 +89,11 @@ cudaError_t launch_walk(const DeviceNode *nodes, const WalkNode *walk_nodes,
                         double *ax, double *ay, double *az, TreeMeta *meta,
                         unsigned long long *counters, unsigned *status, cudaStream_t stream);
 
+// The FP64 walk of the parity mode (walk_f64.cu); `quads` NULL without
+// quadrupoles; `sorted` = x, y, z, m in Morton order.
+cudaError_t launch_walk_f64(const DeviceNode *nodes, const DeviceQuadrupole *quads,
+                            const double *sorted, const uint32_t *perm, uint32_t n, double eps2,
+                            double *ax, double *ay, double *az, const TreeMeta *meta,
+                            unsigned long long *counters, unsigned *status, cudaStream_t stream);
+
 } // namespace ob

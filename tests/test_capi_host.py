@@ -57,7 +57,7 @@ def test_invalid_parameters_are_rejected_before_the_device(lib):
     assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
     bad.softening_squared = float("nan")
     assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
-    bad = ob.make_params(kind=ob.SOLVER_TREE, precision="fp64")
+    bad = ob.make_params(kind=ob.SOLVER_TREE, precision="split")
     assert lib.ob_solver_create(C.byref(bad), C.byref(handle)) == ob.ERROR_UNSUPPORTED
     assert lib.ob_solver_create(None, C.byref(handle)) == ob.ERROR_INVALID_ARGUMENT
 

@@ -92,6 +92,70 @@ def test_ragged_sizes_and_parameters_against_oracle(b200, restatement, n, leaf, 
         assert a.tolist() == [[0.0, 0.0, 0.0]]
 
 
+# --------------------------------------------------------------------------
+# The FP64 parity mode: forces equal to BarnesHutSolver's bit for bit
+# --------------------------------------------------------------------------
+
+@pytest.mark.parametrize("theta,quad,tag", [(0.5, False, "mono"), (0.5, True, "quad"),
+                                            (0.0, False, "theta0")])
+def test_fp64_walk_equals_the_reference_bitwise(b200, golden_plummer, theta, quad, tag):
+    # tests/golden/plummer_2048.npz: the reference's BarnesHutSolver (scalar
+    # leaf kernel), eps 0.05, leaf 32.
+    g = golden_plummer
+    s = b200.B200TreeSolver(0.05, theta, 32, quad, precision="fp64")
+    a = s.evaluate((g["x"], g["y"], g["z"]), g["m"])
+    assert np.array_equal(a, g[f"bh_{tag}_acc"])
+    c = s.interaction_count()
+    assert [c.evaluations, c.particle_particle, c.particle_cell] == \
+        g[f"bh_{tag}_counts"].tolist()
+
+
+@pytest.mark.parametrize("n,leaf,theta,quad", [(1, 32, 0.5, False), (2, 1, 0.5, True),
+                                               (33, 4, 0.7, True), (1000, 8, 0.5, False),
+                                               (20000, 32, 0.5, True)])
+def test_fp64_walk_equals_the_oracle_on_ragged_inputs(b200, restatement, n, leaf, theta, quad):
+    from orrery_b200 import initial_conditions as ic
+    d = ic.plummer_sphere(n, seed=17 + n)
+    x, y, z, m = _xyzm(d)
+    a_ref, counts = restatement.barnes_hut(x, y, z, m, 0.02, theta, leaf, quad)
+    s = b200.B200TreeSolver(0.02, theta, leaf, quad, precision="fp64")
+    a = s.evaluate((x, y, z), m)
+    assert np.array_equal(a, a_ref)
+    c = s.interaction_count()
+    assert (c.particle_particle, c.particle_cell) == (counts.particle_particle,
+                                                      counts.particle_cell)
+
+
+def test_fp64_walk_at_two_million_equals_the_oracle_on_sampled_targets(b200, restatement):
+    from orrery_b200 import initial_conditions as ic
+    d = ic.galaxy_collision(2_000_000, softening=0.02, seed=20260811)
+    x, y, z, m = _xyzm(d)
+    s = b200.B200TreeSolver(0.02, 0.5, 32, True, precision="fp64")
+    a = s.evaluate((x, y, z), m)
+    targets = np.random.default_rng(6).choice(len(m), 4096, replace=False)
+    a_ref, pairs, cells = restatement.barnes_hut_targets(x, y, z, m, 0.02, 0.5, 32, True,
+                                                         targets)
+    assert np.array_equal(a[targets], a_ref)
+
+
+def test_fp64_tree_system_steps_equal_the_oracle(b200, restatement):
+    # A device-resident system over the parity-mode field: its carried
+    # accelerations, before and after two VV steps, equal the oracle's FP64
+    # walk at the same positions.
+    from orrery_b200 import initial_conditions as ic
+    n = 3000
+    d = ic.plummer_sphere(n, seed=41)
+    s = b200.DeviceSystem(n, 0.02, b200.SOLVER_TREE, "fp64", 0.5, 16, True)
+    s.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+    a0, _ = restatement.barnes_hut(d["x"], d["y"], d["z"], d["m"], 0.02, 0.5, 16, True)
+    st = s.state()
+    assert np.array_equal(np.stack([st["ax"], st["ay"], st["az"]], axis=1), a0)
+    s.step(1e-3, 2, "vv")
+    st = s.state()
+    a1, _ = restatement.barnes_hut(st["x"], st["y"], st["z"], d["m"], 0.02, 0.5, 16, True)
+    assert np.array_equal(np.stack([st["ax"], st["ay"], st["az"]], axis=1), a1)
+
+
 def test_coincident_particles_hit_the_depth_limit(b200, restatement):
     # octree_test.cpp:407-432: identical codes cannot be separated, so the
     # subdivision stops at level 21 with one over-full leaf.
