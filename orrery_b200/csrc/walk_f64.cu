@@ -14,9 +14,13 @@
 // acceleration is bit-identical to BarnesHutSolver's with its scalar leaf
 // kernel. Counts are the reference's per-target pair and cell counts.
 //
-// Index checks: a node index past the node count, an escape index that does
-// not move forward, or a leaf range past n (none of which a valid tree
-// produces) sets kStatusInvalid and ends that target's walk.
+// The warp walks the union of its targets' walks in node order (each lane's
+// cursor is its own next node), so lanes at the same node read it, and the
+// same leaf sources, together.
+//
+// Index checks: an escape index that does not move forward or a leaf range
+// past n (neither of which a valid tree produces) sets kStatusInvalid and ends
+// that target's walk.
 #include "common.cuh"
 #include "tree_kernels.hpp"
 
@@ -80,11 +84,21 @@ __global__ void __launch_bounds__(kWalk64Threads)
     const double *sm = sorted + 3ull * n;
     unsigned long long pairs = 0, cells = 0;
     double acc_x = 0.0, acc_y = 0.0, acc_z = 0.0;
-    if (active) {
-        const double px = sx[i], py = sy[i], pz = sz[i];
-        uint32_t node = 0;
-        while (node < node_count) {
-            const DeviceNode cell = nodes[node];
+    const double px = active ? sx[i] : 0.0, py = active ? sy[i] : 0.0, pz = active ? sz[i] : 0.0;
+    // Each lane's cursor is the next node of its own pre-order walk; the warp
+    // visits the union of its lanes' walks in node order, taking the smallest
+    // cursor each time, and the lanes standing at that node handle it
+    // together (their node and source reads are broadcasts). A lane still
+    // performs exactly its own operations in its own order.
+    constexpr uint32_t kDone = 0xffffffffu;
+    uint32_t node = active ? 0u : kDone;
+    while (true) {
+        const uint32_t cur = __reduce_min_sync(kFull, node < node_count ? node : kDone);
+        if (cur == kDone) {
+            break;
+        }
+        if (node == cur) {
+            const DeviceNode cell = nodes[cur];
             const double ox = __dsub_rn(cell.com_x, px);
             const double oy = __dsub_rn(cell.com_y, py);
             const double oz = __dsub_rn(cell.com_z, pz);
@@ -97,7 +111,7 @@ __global__ void __launch_bounds__(kWalk64Threads)
                 acc_y = __dadd_rn(acc_y, __dmul_rn(oy, factor));
                 acc_z = __dadd_rn(acc_z, __dmul_rn(oz, factor));
                 if (quads != nullptr) {
-                    const DeviceQuadrupole q = quads[node];
+                    const DeviceQuadrupole q = quads[cur];
                     const double inverse = inverse_distance(d2, eps2);
                     const double inv2 = __dmul_rn(inverse, inverse);
                     const double inv5 = __dmul_rn(__dmul_rn(inv2, inv2), inverse);
@@ -119,34 +133,38 @@ __global__ void __launch_bounds__(kWalk64Threads)
                 const uint32_t begin = cell.first;
                 if (begin > n || cell.count > n - begin) {
                     atomicOr(status, kStatusInvalid);
-                    break;
-                }
-                const uint32_t end = begin + cell.count;
-                double rx, ry, rz;
-                if (i >= begin && i < end) {
-                    range_sum(sx, sy, sz, sm, begin, i, px, py, pz, eps2, rx, ry, rz);
+                    following = kDone;
+                } else {
+                    const uint32_t end = begin + cell.count;
+                    double rx, ry, rz;
+                    if (i >= begin && i < end) {
+                        range_sum(sx, sy, sz, sm, begin, i, px, py, pz, eps2, rx, ry, rz);
+                        acc_x = __dadd_rn(acc_x, rx);
+                        acc_y = __dadd_rn(acc_y, ry);
+                        acc_z = __dadd_rn(acc_z, rz);
+                        range_sum(sx, sy, sz, sm, i + 1, end, px, py, pz, eps2, rx, ry, rz);
+                        pairs += cell.count - 1;
+                    } else {
+                        range_sum(sx, sy, sz, sm, begin, end, px, py, pz, eps2, rx, ry, rz);
+                        pairs += cell.count;
+                    }
                     acc_x = __dadd_rn(acc_x, rx);
                     acc_y = __dadd_rn(acc_y, ry);
                     acc_z = __dadd_rn(acc_z, rz);
-                    range_sum(sx, sy, sz, sm, i + 1, end, px, py, pz, eps2, rx, ry, rz);
-                    pairs += cell.count - 1;
-                } else {
-                    range_sum(sx, sy, sz, sm, begin, end, px, py, pz, eps2, rx, ry, rz);
-                    pairs += cell.count;
+                    following = cell.next;
                 }
-                acc_x = __dadd_rn(acc_x, rx);
-                acc_y = __dadd_rn(acc_y, ry);
-                acc_z = __dadd_rn(acc_z, rz);
-                following = cell.next;
             } else {
-                following = node + 1;
+                following = cur + 1;
             }
-            if (following <= node) { // a pre-order walk only moves forward
+            if (following <= cur) { // a pre-order walk only moves forward
                 atomicOr(status, kStatusInvalid);
-                break;
+                following = kDone;
             }
             node = following;
         }
+        __syncwarp();
+    }
+    if (active) {
         const uint32_t j = perm[i];
         ax[j] = acc_x;
         ay[j] = acc_y;
