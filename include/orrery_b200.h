@@ -236,6 +236,40 @@ int ob_system_synchronize(ob_system *system);
  * softening. Either pointer may be NULL. */
 int ob_system_energy(ob_system *system, double *kinetic, double *potential);
 
+/* core::Diagnostics (include/orrery/core/diagnostics.hpp:52-82). */
+typedef struct ob_diagnostics {
+    double kinetic_energy;
+    double potential_energy;
+    double linear_momentum[3];
+    double angular_momentum[3];
+} ob_diagnostics;
+
+/* core::measure_diagnostics (src/core/diagnostics.cpp:179-200) of the
+ * system's current state: the energies as ob_system_energy computes them, and
+ * the momenta as compensated sums in index order, bit-identical to the
+ * reference's. Waits for the enqueued steps. */
+int ob_system_diagnostics(ob_system *system, ob_diagnostics *out);
+
+/* The device addresses of the system's ten FP64 state arrays, each of n
+ * doubles: x y z vx vy vz ax ay az m (NULL when n is 0), for zero-copy views
+ * (e.g. DLPack or __cuda_array_interface__). They stay valid until the
+ * system is destroyed. Work on them from another stream is ordered against the
+ * system's steps by the caller (ob_system_synchronize, or events on
+ * ob_system_stream). */
+int ob_system_device_arrays(ob_system *system, void **arrays);
+
+/* The whole state, masses included, in a checkpoint's order (after the
+ * enqueued steps; waits for them). */
+int ob_system_snapshot(ob_system *system, double *m, double *x, double *y, double *z,
+                       double *vx, double *vy, double *vz, double *ax, double *ay, double *az);
+
+/* Installs a state whose accelerations already belong to its positions, as
+ * sim::Simulation::restore with accelerations_are_current
+ * (include/orrery/sim/simulation.hpp:101-102): no force evaluation. */
+int ob_system_restore(ob_system *system, const double *m, const double *x, const double *y,
+                      const double *z, const double *vx, const double *vy, const double *vz,
+                      const double *ax, const double *ay, const double *az);
+
 /* The stream the system's work is enqueued on (a cudaStream_t), for callers
  * that order their own work or events after it. */
 int ob_system_stream(ob_system *system, void **stream);

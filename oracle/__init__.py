@@ -293,6 +293,7 @@ class Reference:
         lib.ref_potential_energy.restype = C.c_double
         lib.ref_kinetic_energy.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp]
         lib.ref_kinetic_energy.restype = C.c_double
+        lib.ref_diagnostics.argtypes = [C.c_size_t] + [_dp] * 7 + [C.c_double, _dp]
         # Run output (ref_output_shim.cpp).
         lib.ref_last_error.restype = C.c_char_p
         lib.ref_default_configuration.argtypes = [C.c_char_p, C.c_size_t]
@@ -363,7 +364,7 @@ class Reference:
                                          _d(np.ascontiguousarray(v))) != 0:
             self._raise("TrajectoryWriter")
 
-    def read_trajectory(self, path, max_frames=64, max_n=1 << 20):
+    def read_trajectory(self, path, max_frames=16, max_n=4096):
         """sim::TrajectoryReader: header facts and the frames."""
         n, ts, wv, nf = C.c_uint64(), C.c_double(), C.c_int(), C.c_size_t()
         masses = np.zeros(max_n)
@@ -474,6 +475,15 @@ class Reference:
 
     def kinetic_energy(self, vx, vy, vz, m):
         return self.lib.ref_kinetic_energy(len(m), _d(vx), _d(vy), _d(vz), _d(m))
+
+    def diagnostics(self, x, y, z, vx, vy, vz, m, softening):
+        """core::measure_diagnostics: kinetic and potential energy, linear and
+        angular momentum."""
+        out = np.zeros(8)
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (x, y, z, vx, vy, vz, m)]
+        self.lib.ref_diagnostics(len(arrs[-1]), *(_d(a) for a in arrs), softening, _d(out))
+        return {"kinetic_energy": out[0], "potential_energy": out[1],
+                "linear_momentum": out[2:5].copy(), "angular_momentum": out[5:8].copy()}
 
 
 class ReferenceCuda:

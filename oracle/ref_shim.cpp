@@ -316,6 +316,25 @@ double ref_potential_energy(std::size_t n, const double* x, const double* y, con
                                           orrery::core::Softening{softening});
 }
 
+// core::measure_diagnostics: kinetic, potential, linear momentum (3), angular
+// momentum (3) into out[8].
+int ref_diagnostics(std::size_t n, const double* x, const double* y, const double* z,
+                    const double* vx, const double* vy, const double* vz, const double* m,
+                    double softening, double* out) {
+    ParticleData data = make_data(n, x, y, z, vx, vy, vz, m);
+    const orrery::core::Diagnostics d =
+        orrery::core::measure_diagnostics(data, orrery::core::Softening{softening});
+    out[0] = d.kinetic_energy;
+    out[1] = d.potential_energy;
+    out[2] = d.linear_momentum.x;
+    out[3] = d.linear_momentum.y;
+    out[4] = d.linear_momentum.z;
+    out[5] = d.angular_momentum.x;
+    out[6] = d.angular_momentum.y;
+    out[7] = d.angular_momentum.z;
+    return 0;
+}
+
 double ref_kinetic_energy(std::size_t n, const double* vx, const double* vy, const double* vz,
                           const double* m) {
     ParticleData data = make_data(n, vx, vy, vz, nullptr, nullptr, nullptr, m);

@@ -109,6 +109,11 @@ class ServerSummary(C.Structure):
                 ("hbm_peak", C.c_uint64)]
 
 
+class Diagnostics(C.Structure):
+    _fields_ = [("kinetic_energy", C.c_double), ("potential_energy", C.c_double),
+                ("linear_momentum", C.c_double * 3), ("angular_momentum", C.c_double * 3)]
+
+
 class Timings(C.Structure):
     _fields_ = [("transfer_in_ms", C.c_double), ("ordering_ms", C.c_double),
                 ("construction_ms", C.c_double), ("traversal_ms", C.c_double),
@@ -175,6 +180,10 @@ def load_library():
     lib.ob_probe_fp32.argtypes = [_dp, _dp]
     lib.ob_probe_fp32x2.argtypes = [_dp]
     lib.ob_probe_fp64.argtypes = [_dp]
+    lib.ob_system_diagnostics.argtypes = [vp, C.POINTER(Diagnostics)]
+    lib.ob_system_device_arrays.argtypes = [vp, C.POINTER(vp)]
+    lib.ob_system_snapshot.argtypes = [vp] + [_dp] * 10
+    lib.ob_system_restore.argtypes = [vp] + [_dp] * 10
     _u64p = C.POINTER(C.c_uint64)
     lib.ob_tree_stats.argtypes = [vp, _u64p, _u64p, C.POINTER(C.c_uint32)]
     lib.ob_tree_copy.argtypes = [vp, _dp, _u64p, _dp]
@@ -542,6 +551,22 @@ class DeviceSystem:
         _check(self._lib.ob_system_energy(self._handle, C.byref(ke), C.byref(pe)))
         return ke.value, pe.value
 
+    def diagnostics(self) -> dict:
+        """core::measure_diagnostics of the state: kinetic_energy,
+        potential_energy, linear_momentum (3), angular_momentum (3)."""
+        d = Diagnostics()
+        _check(self._lib.ob_system_diagnostics(self._handle, C.byref(d)))
+        return {"kinetic_energy": d.kinetic_energy, "potential_energy": d.potential_energy,
+                "linear_momentum": np.array(d.linear_momentum[:]),
+                "angular_momentum": np.array(d.angular_momentum[:])}
+
+    def snapshot(self) -> dict:
+        """The whole state on the host: x y z vx vy vz ax ay az and m."""
+        keys = ("m", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+        out = {k: np.empty(self.n) for k in keys}
+        _check(self._lib.ob_system_snapshot(self._handle, *(_ptr(out[k]) for k in keys)))
+        return out
+
     def kinetic_energy(self) -> float:
         ke = C.c_double()
         _check(self._lib.ob_system_energy(self._handle, C.byref(ke), None))
@@ -873,3 +898,6 @@ def compute_accelerations(positions, masses, softening: float = 0.0, solver: str
     else:
         raise ValueError(f"unknown solver {solver!r}")
     return s.evaluate(positions, masses)
+
+
+from .simulation import DeviceArrayView, FileOutput, Simulation, device_arrays  # noqa: E402,F401

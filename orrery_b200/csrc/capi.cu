@@ -452,6 +452,45 @@ static double compensated_sum(const std::vector<double> &terms) {
     return total + correction;
 }
 
+// core::measure_diagnostics (src/core/diagnostics.cpp:179-200): the energies
+// as System::energy computes them (device terms, compensated host sums), and
+// the linear and angular momentum as compensated sums of v m and (x cross v) m
+// in index order, one Neumaier sum per component, over the downloaded state.
+ob_diagnostics System::diagnostics() {
+    ob_diagnostics d{};
+    energy(&d.kinetic_energy, &d.potential_energy);
+    if (n_ == 0) {
+        return d;
+    }
+    std::vector<double> host(7ull * n_);
+    const int arrays[7] = {kX, kY, kZ, kVx, kVy, kVz, kM};
+    for (int k = 0; k < 7; ++k) {
+        check(cudaMemcpyAsync(host.data() + k * n_, array(arrays[k]), sizeof(double) * n_,
+                              cudaMemcpyDeviceToHost, stream_),
+              "downloading state");
+    }
+    check(cudaStreamSynchronize(stream_), "downloading state");
+    const double *x = host.data(), *y = x + n_, *z = y + n_;
+    const double *vx = z + n_, *vy = vx + n_, *vz = vy + n_, *m = vz + n_;
+    std::vector<double> terms[6];
+    for (auto &t : terms) {
+        t.resize(n_);
+    }
+    for (uint32_t i = 0; i < n_; ++i) {
+        terms[0][i] = vx[i] * m[i];
+        terms[1][i] = vy[i] * m[i];
+        terms[2][i] = vz[i] * m[i];
+        terms[3][i] = ((y[i] * vz[i]) - (z[i] * vy[i])) * m[i];
+        terms[4][i] = ((z[i] * vx[i]) - (x[i] * vz[i])) * m[i];
+        terms[5][i] = ((x[i] * vy[i]) - (y[i] * vx[i])) * m[i];
+    }
+    for (int c = 0; c < 3; ++c) {
+        d.linear_momentum[c] = compensated_sum(terms[c]);
+        d.angular_momentum[c] = compensated_sum(terms[3 + c]);
+    }
+    return d;
+}
+
 void System::energy(double *kinetic, double *potential) {
     if (n_ == 0) {
         if (kinetic) *kinetic = 0.0;
@@ -738,6 +777,47 @@ int ob_system_energy(ob_system *system, double *kinetic, double *potential) {
     return guarded([&] {
         require(system != nullptr, "system is NULL");
         system->impl->energy(kinetic, potential);
+    });
+}
+
+int ob_system_diagnostics(ob_system *system, ob_diagnostics *out) {
+    return guarded([&] {
+        require(system != nullptr && out != nullptr, "NULL argument");
+        *out = system->impl->diagnostics();
+    });
+}
+
+int ob_system_restore(ob_system *system, const double *m, const double *x, const double *y,
+                      const double *z, const double *vx, const double *vy, const double *vz,
+                      const double *ax, const double *ay, const double *az) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        const double *arrays[10] = {m, x, y, z, vx, vy, vz, ax, ay, az};
+        for (const double *a : arrays) {
+            require(system->impl->size() == 0 || a != nullptr, "every state array is required");
+        }
+        system->impl->restore(arrays);
+    });
+}
+
+int ob_system_snapshot(ob_system *system, double *m, double *x, double *y, double *z,
+                       double *vx, double *vy, double *vz, double *ax, double *ay, double *az) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        double *const arrays[10] = {m, x, y, z, vx, vy, vz, ax, ay, az};
+        for (double *a : arrays) {
+            require(system->impl->size() == 0 || a != nullptr, "every state array is required");
+        }
+        system->impl->snapshot(arrays);
+    });
+}
+
+int ob_system_device_arrays(ob_system *system, void **arrays) {
+    return guarded([&] {
+        require(system != nullptr && arrays != nullptr, "NULL argument");
+        for (int k = 0; k < 10; ++k) {
+            arrays[k] = system->impl->size() == 0 ? nullptr : system->impl->array(k);
+        }
     });
 }
 

@@ -44,6 +44,7 @@ public:
     void step_host(int integrator, double dt, uint64_t steps, double *const *io, const double *m);
     void synchronize();
     void energy(double *kinetic, double *potential);
+    ob_diagnostics diagnostics();
 
     [[nodiscard]] Solver &solver() noexcept { return *solver_; }
     [[nodiscard]] uint32_t size() const noexcept { return n_; }

@@ -1,0 +1,226 @@
+"""A run on the device: the counterpart of the reference's sim::Simulation and
+its run output, over the C ABI.
+
+``Simulation`` mirrors the reference's Python ``orrery.Simulation``
+(python/src/sim_bindings.cpp:274-343, src/sim/simulation.cpp:16-70): it holds
+the state, the solver, the integrator and the step counter; the simulated time
+is ``step_index * timestep``, computed rather than accumulated; ``run`` records
+through an attached output at the start, every stride and the last step, as
+sim::FileOutput::record does (src/sim/run_output.cpp). The state stays in HBM:
+``particles`` copies it to the host, ``device_particles`` gives zero-copy views
+of it (``__cuda_array_interface__``, readable by torch, CuPy or Numba).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import (DeviceSystem, OrreryError, Trajectory, SOLVER_DIRECT, SOLVER_TREE,
+               ERROR_INVALID_ARGUMENT, _check, _f64, _ptr, load_library)
+
+_STATE = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
+
+
+class DeviceArrayView:
+    """One FP64 state array of a DeviceSystem, exposed without a copy through
+    ``__cuda_array_interface__`` (version 3). Valid while the system lives;
+    reads and writes from another stream must be ordered against the
+    system's steps by the caller (``DeviceSystem.synchronize``)."""
+
+    def __init__(self, address: int, n: int, owner):
+        self._owner = owner  # keeps the system alive
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8",
+                                         "data": (address, False), "version": 3,
+                                         "strides": None, "stream": None}
+
+    def __len__(self):
+        return self.__cuda_array_interface__["shape"][0]
+
+
+def device_arrays(system: DeviceSystem) -> dict:
+    """Zero-copy views of a system's ten state arrays, keyed x y z vx vy vz ax
+    ay az m (ob_system_device_arrays)."""
+    lib = load_library()
+    ptrs = (C.c_void_p * 10)()
+    _check(lib.ob_system_device_arrays(system._handle, ptrs))
+    return {k: DeviceArrayView(ptrs[i] or 0, system.n, system) for i, k in enumerate(_STATE)}
+
+
+class FileOutput:
+    """sim::FileOutput (src/sim/run_output.cpp): a trajectory frame every
+    ``trajectory_stride`` steps and a checkpoint every ``checkpoint_stride``,
+    each also at the first record and the last step of a run (a stride of 0:
+    only those). Frames are device snapshots written in the background; the
+    trajectory is flushed with each checkpoint, so a run killed after a
+    checkpoint leaves frames that reach at least that far."""
+
+    def __init__(self, trajectory_path=None, trajectory_stride: int = 0,
+                 trajectory_velocities: bool = False, checkpoint_path=None,
+                 checkpoint_stride: int = 0, configuration: str = ""):
+        self.trajectory_path = trajectory_path
+        self.trajectory_stride = int(trajectory_stride)
+        self.trajectory_velocities = bool(trajectory_velocities)
+        self.checkpoint_path = checkpoint_path
+        self.checkpoint_stride = int(checkpoint_stride)
+        self.configuration = configuration
+        self._trajectory = None
+        self._first = True
+        self.checkpoints = 0
+
+    def _due(self, step, stride, is_final):
+        return self._first or is_final or (stride != 0 and step % stride == 0)
+
+    def next_due(self, step: int, last: int) -> int:
+        """The first step after `step`, up to `last`, at which something is due."""
+        due = last
+        for stride, on in ((self.trajectory_stride, self.trajectory_path),
+                           (self.checkpoint_stride, self.checkpoint_path)):
+            if on and stride > 0:
+                due = min(due, (step // stride + 1) * stride)
+        return due
+
+    def record(self, simulation: "Simulation", is_final: bool) -> None:
+        step = simulation.step_index
+        if self.trajectory_path is not None:
+            if self._trajectory is None:
+                self._trajectory = Trajectory(self.trajectory_path, simulation.timestep,
+                                              system=simulation.system,
+                                              with_velocities=self.trajectory_velocities)
+            if self._due(step, self.trajectory_stride, is_final):
+                self._trajectory.write_frame(step, simulation.time)
+        if self.checkpoint_path is not None and \
+                self._due(step, self.checkpoint_stride, is_final):
+            if self._trajectory is not None:
+                self._trajectory.flush()
+            simulation.write_checkpoint(self.checkpoint_path, self.configuration)
+            self.checkpoints += 1
+        self._first = False
+
+    @property
+    def frames_written(self) -> int:
+        return self._trajectory.frames if self._trajectory is not None else 0
+
+    def close(self) -> None:
+        if self._trajectory is not None:
+            self._trajectory.close()
+            self._trajectory = None
+
+
+class Simulation:
+    """sim::Simulation with its state resident on the device.
+
+    ``state`` holds x y z vx vy vz m (FP64 arrays of one length). Building it
+    costs one force evaluation, which establishes the carried accelerations
+    (the reference's constructor does the same, src/sim/simulation.cpp:23)."""
+
+    def __init__(self, state: dict, timestep: float, integrator: str = "vv",
+                 solver: str = "direct", precision: str = "fp32", softening: float = 0.0,
+                 opening_angle: float = 0.5, leaf_capacity: int = 32,
+                 quadrupole: bool = False, output: FileOutput = None):
+        kind = SOLVER_TREE if solver in ("tree", "barnes-hut") else SOLVER_DIRECT
+        if solver not in ("direct", "tree", "barnes-hut"):
+            raise OrreryError(ERROR_INVALID_ARGUMENT, f"unknown solver {solver!r}")
+        arrs = {k: _f64(state[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
+        self.n = len(arrs["m"])
+        self.system = DeviceSystem(self.n, softening, kind, precision, opening_angle,
+                                   leaf_capacity, quadrupole)
+        self.system.set_state(arrs["x"], arrs["y"], arrs["z"], arrs["vx"], arrs["vy"],
+                              arrs["vz"], arrs["m"])
+        self.timestep = float(timestep)
+        self.integrator_name = integrator
+        self.solver_name = "b200-tree" if kind == SOLVER_TREE else "b200-direct"
+        self.output = output
+        self._step = 0
+
+    # -- the clock ----------------------------------------------------------
+
+    @property
+    def step_index(self) -> int:
+        return self._step
+
+    @property
+    def time(self) -> float:
+        """The simulated time, step_index * timestep (computed, not accumulated)."""
+        return float(self._step) * self.timestep
+
+    # -- stepping -----------------------------------------------------------
+
+    def step(self) -> None:
+        """Advance by one step. Records nothing."""
+        self.system.step(self.timestep, 1, self.integrator_name)
+        self._step += 1
+
+    def run(self, steps: int) -> None:
+        """Advance by `steps` steps, recording through the output (if any) at
+        the start, wherever a stride falls and at the last step."""
+        steps = int(steps)
+        out = self.output
+        if out is None:
+            self.system.step(self.timestep, steps, self.integrator_name)
+            self._step += steps
+            return
+        out.record(self, steps == 0)
+        end = self._step + steps
+        while self._step < end:
+            target = out.next_due(self._step, end)
+            self.system.step_async(self.timestep, target - self._step, self.integrator_name)
+            self._step = target
+            out.record(self, self._step == end)
+        self.system.synchronize()
+
+    # -- state --------------------------------------------------------------
+
+    @property
+    def particles(self) -> dict:
+        """A host copy of the state: x y z vx vy vz ax ay az and m."""
+        return self.system.snapshot()
+
+    def device_particles(self) -> dict:
+        """Zero-copy views of the device state (see DeviceArrayView)."""
+        self.system.synchronize()
+        return device_arrays(self.system)
+
+    def restore(self, state: dict, step: int = 0, accelerations_are_current: bool = False):
+        """Replace the state and the step counter. Re-establishes the carried
+        accelerations with one evaluation unless they are given as current."""
+        keys = ("x", "y", "z", "vx", "vy", "vz", "m")
+        arrs = {k: _f64(state[k]) for k in keys}
+        if len(arrs["m"]) != self.n:
+            raise OrreryError(ERROR_INVALID_ARGUMENT, "a restored state keeps the particle count")
+        if accelerations_are_current:
+            acc = {k: _f64(state[k]) for k in ("ax", "ay", "az")}
+            lib = load_library()
+            _check(lib.ob_system_restore(self.system._handle, _ptr(arrs["m"]),
+                                         *(_ptr(arrs[k]) for k in keys[:6]),
+                                         *(_ptr(acc[k]) for k in ("ax", "ay", "az"))))
+        else:
+            self.system.set_state(*(arrs[k] for k in keys))
+        self._step = int(step)
+
+    def measure(self) -> dict:
+        """core::measure_diagnostics of the current state: kinetic, potential
+        and total energy, linear and angular momentum, virial ratio."""
+        d = self.system.diagnostics()
+        d["total_energy"] = d["kinetic_energy"] + d["potential_energy"]
+        pe = d["potential_energy"]
+        d["virial_ratio"] = 2 * d["kinetic_energy"] / (-pe if pe < 0 else pe) if pe else \
+            float("inf")
+        return d
+
+    @property
+    def interaction_count(self):
+        return self.system.interaction_count()
+
+    # -- checkpoints --------------------------------------------------------
+
+    def write_checkpoint(self, path, configuration: str = "") -> None:
+        self.system.write_checkpoint(path, self._step, configuration)
+
+    def resume(self, path) -> str:
+        """Restore from an ORRERYCK checkpoint of this size (state, carried
+        accelerations and step); returns its configuration text."""
+        step, text = self.system.read_checkpoint(path)
+        self._step = step
+        return text
+
+    def __repr__(self):
+        return f"<Simulation of {self.n} particles at step {self._step}>"
