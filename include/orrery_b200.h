@@ -423,6 +423,10 @@ typedef struct ob_server_config {
     int32_t fake_device;             /* nonzero: no GPU; steps take modelled time */
     double fake_direct_gint_s;       /* fake mode: direct interactions per second / 1e9 */
     double fake_tree_ns_per_particle;/* fake mode: tree step time per particle */
+    double max_job_work;             /* per-job ceiling in ob_work_units (0: none); above it a
+                                        job is refused (OB_ERROR_CAPACITY) */
+    double max_running_work;         /* max ob_work_units of the running jobs together (0:
+                                        none); a job alone always runs */
 } ob_server_config;
 
 typedef struct ob_job_spec {
@@ -466,6 +470,11 @@ typedef struct ob_server_summary {
 } ob_server_summary;
 
 int ob_server_create(const ob_server_config *config, ob_server **out);
+/* The reference service's cost of a run (work_units,
+ * service/orrery_service/limits.py:82-111): count^2 * steps for the direct
+ * solver (kind OB_SOLVER_DIRECT), count * log2(count) * steps for the tree; 0
+ * below two particles. */
+double ob_work_units(uint64_t count, uint64_t steps, int32_t kind);
 /* Stops the loop (running jobs are cancelled) and frees everything. */
 void ob_server_destroy(ob_server *server);
 /* Copies the initial state (vx..vz may be NULL = zero); returns the job id. A

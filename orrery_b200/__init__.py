@@ -83,7 +83,8 @@ class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_uint64), ("direct_pairs_cap", C.c_uint64),
                 ("direct_arena_particles", C.c_uint64), ("max_tree_jobs", C.c_uint32),
                 ("fake_device", C.c_int32), ("fake_direct_gint_s", C.c_double),
-                ("fake_tree_ns_per_particle", C.c_double)]
+                ("fake_tree_ns_per_particle", C.c_double), ("max_job_work", C.c_double),
+                ("max_running_work", C.c_double)]
 
 
 class JobSpec(C.Structure):
@@ -217,6 +218,8 @@ def load_library():
     lib.ob_server_cancel.argtypes = [vp, C.c_uint64]
     lib.ob_server_stats.argtypes = [vp, C.POINTER(ServerSummary)]
     lib.ob_server_drain.argtypes = [vp, C.c_double]
+    lib.ob_work_units.argtypes = [C.c_uint64, C.c_uint64, C.c_int32]
+    lib.ob_work_units.restype = C.c_double
     cp = C.c_char_p
     lib.ob_checkpoint_write.argtypes = [cp, C.c_uint64, cp, C.c_uint64, C.c_uint64] + [_dp] * 10
     lib.ob_checkpoint_info.argtypes = [cp, _u64p, _u64p, _u64p]
@@ -720,11 +723,13 @@ class Server:
 
     def __init__(self, hbm_budget_bytes: int, direct_pairs_cap: int = 0,
                  direct_arena_particles: int = 0, max_tree_jobs: int = 1, fake: bool = False,
-                 fake_direct_gint_s: float = 800.0, fake_tree_ns_per_particle: float = 12.0):
+                 fake_direct_gint_s: float = 800.0, fake_tree_ns_per_particle: float = 12.0,
+                 max_job_work: float = 0.0, max_running_work: float = 0.0):
         lib = load_library()
         cfg = ServerConfig(int(hbm_budget_bytes), int(direct_pairs_cap),
                            int(direct_arena_particles), int(max_tree_jobs), 1 if fake else 0,
-                           float(fake_direct_gint_s), float(fake_tree_ns_per_particle))
+                           float(fake_direct_gint_s), float(fake_tree_ns_per_particle),
+                           float(max_job_work), float(max_running_work))
         handle = C.c_void_p()
         _check(lib.ob_server_create(C.byref(cfg), C.byref(handle)))
         self._lib = lib
@@ -884,6 +889,14 @@ class Trajectory:
         if h is not None and h.value:
             self._lib.ob_trajectory_close(h)
             self._handle = None
+
+
+def work_units(count: int, steps: int, solver: str) -> float:
+    """The reference service's cost of a run (service/orrery_service/limits.py:82-111),
+    as the server's admission counts it: count^2 * steps for "direct",
+    count * log2(count) * steps for the tree ("barnes-hut" or "tree")."""
+    kind = SOLVER_DIRECT if solver == "direct" else SOLVER_TREE
+    return load_library().ob_work_units(int(count), int(steps), kind)
 
 
 def compute_accelerations(positions, masses, softening: float = 0.0, solver: str = "direct",

@@ -69,6 +69,7 @@ struct Job {
     double submitted = 0, admitted = 0, finished = 0;
     uint64_t steps_done = 0;
     uint64_t bytes = 0;
+    double work = 0;             // work units (work_units below)
     std::vector<double> input;   // x y z vx vy vz m (7n)
     std::vector<double> output;  // x y z vx vy vz ax ay az (9n)
     bool cancel_requested = false;
@@ -124,6 +125,12 @@ public:
         job->spec = spec;
         job->bytes = spec.kind == OB_SOLVER_DIRECT ? direct_job_bytes(spec.n)
                                                    : tree_job_bytes(spec.n);
+        job->work = ob_work_units(spec.n, spec.steps, spec.kind);
+        if (config_.max_job_work > 0 && job->work > config_.max_job_work) {
+            std::lock_guard<std::mutex> lock(mutex_);
+            ++rejected_;
+            throw Error(OB_ERROR_CAPACITY, "the job's work exceeds the server's per-job ceiling");
+        }
         if (job->bytes > config_.hbm_budget_bytes ||
             (spec.kind == OB_SOLVER_DIRECT &&
              (Batch::footprint(static_cast<uint32_t>(spec.n)) > config_.direct_arena_particles ||
@@ -303,7 +310,8 @@ private:
             drop_cancelled_queued(direct_queue_);
             drop_cancelled_queued(tree_queue_);
             while (!tree_queue_.empty() && running_trees_ < config_.max_tree_jobs &&
-                   hbm_in_use_ + tree_queue_.front()->bytes <= config_.hbm_budget_bytes) {
+                   hbm_in_use_ + tree_queue_.front()->bytes <= config_.hbm_budget_bytes &&
+                   work_allows(tree_queue_.front())) {
                 Job *job = tree_queue_.front();
                 tree_queue_.pop_front();
                 start_job_locked(job);
@@ -318,6 +326,9 @@ private:
                 }
                 if (config_.direct_pairs_cap > 0 && direct_pairs_ > 0 &&
                     direct_pairs_ + pairs > config_.direct_pairs_cap) {
+                    break;
+                }
+                if (!work_allows(job)) {
                     break;
                 }
                 direct_queue_.pop_front();
@@ -355,9 +366,17 @@ private:
         }
     }
 
+    // The running jobs' work units leave room for this one (a job alone
+    // always runs: the per-job ceiling is checked at submission).
+    bool work_allows(const Job *job) const {
+        return config_.max_running_work <= 0 || running_ == 0 ||
+               running_work_ + job->work <= config_.max_running_work;
+    }
+
     void start_job_locked(Job *job) {
         job->status = OB_JOB_RUNNING;
         job->admitted = now();
+        running_work_ += job->work;
         hbm_in_use_ += job->bytes;
         hbm_peak_ = std::max(hbm_peak_, hbm_in_use_);
         ++admitted_;
@@ -582,6 +601,7 @@ private:
         job->in_flight = false;
         hbm_in_use_ -= job->bytes;
         --running_;
+        running_work_ = running_ == 0 ? 0.0 : running_work_ - job->work;
         if (status == OB_JOB_DONE) {
             ++completed_;
             job_latency_.push_back(job->finished - job->submitted);
@@ -682,6 +702,7 @@ private:
              rejected_ = 0, running_ = 0;
     uint32_t running_trees_ = 0;
     uint64_t direct_pairs_ = 0;
+    double running_work_ = 0; // work units of the running jobs
     uint64_t hbm_in_use_ = 0, hbm_peak_ = 0;
     std::vector<double> job_latency_, step_latency_;
 };
@@ -709,6 +730,17 @@ void need(bool condition, const char *message) {
     }
 }
 } // namespace
+
+extern "C" double ob_work_units(uint64_t count, uint64_t steps, int32_t kind) {
+    // The reference service's cost model (service/orrery_service/limits.py:82-111):
+    // count^2 per step for the direct sum, count log2(count) for the tree.
+    if (count < 2) {
+        return 0.0;
+    }
+    const double c = static_cast<double>(count);
+    const double per_step = kind == OB_SOLVER_DIRECT ? c * c : c * std::log2(c);
+    return per_step * static_cast<double>(steps);
+}
 
 extern "C" {
 

@@ -103,6 +103,50 @@ def test_direct_work_cap_is_respected():
         s.close()
 
 
+def test_work_units_are_the_reference_cost_model():
+    # tests/golden/work_units.json: service/orrery_service/limits.py's own
+    # work_units, written by tests/golden/make_golden_work_units.py.
+    import json
+    import os
+    from conftest import GOLDEN
+    with open(os.path.join(GOLDEN, "work_units.json")) as fh:
+        g = json.load(fh)
+    for case in g["cases"]:
+        assert ob.work_units(case["count"], case["steps"], case["solver"]) == case["work"], case
+    assert ob.work_units(g["MAX_PARTICLES"], 6000, "barnes-hut") == g["MAX_WORK"]
+
+
+def test_a_job_above_the_work_ceiling_is_refused():
+    ceiling = ob.work_units(1000, 20, "direct")
+    s = ob.Server(hbm_budget_bytes=1 << 34, fake=True, max_job_work=ceiling)
+    try:
+        ok = s.submit(_state(1000), steps=20, dt=1e-3, softening=0.01)
+        with pytest.raises(ob.OrreryError) as err:
+            s.submit(_state(1000), steps=21, dt=1e-3, softening=0.01)
+        assert err.value.code == ob.ERROR_CAPACITY
+        assert s.wait(ok, timeout=60, outputs=False)[0]["status"] == ob.JOB_DONE
+        assert s.stats()["rejected"] == 1
+    finally:
+        s.close()
+
+
+def test_running_work_holds_jobs_back():
+    # Three equal direct jobs under a cap of one and a half jobs' work: they run
+    # one after another (a job alone always runs).
+    w = ob.work_units(3000, 5, "direct")
+    s = ob.Server(hbm_budget_bytes=1 << 34, fake=True, fake_direct_gint_s=1.0,
+                  max_running_work=1.5 * w)
+    try:
+        ids = [s.submit(_state(3000, k), steps=5, dt=1e-3, softening=0.01) for k in range(3)]
+        r = [s.wait(i, timeout=60, outputs=False)[0] for i in ids]
+        assert r[1]["admitted_s"] >= r[0]["finished_s"] - 1e-3
+        assert r[2]["admitted_s"] >= r[1]["finished_s"] - 1e-3
+        big = s.submit(_state(6000), steps=5, dt=1e-3, softening=0.01)  # above the cap alone
+        assert s.wait(big, timeout=60, outputs=False)[0]["status"] == ob.JOB_DONE
+    finally:
+        s.close()
+
+
 def test_cancelled_jobs_stop(server):
     slow = ob.Server(hbm_budget_bytes=1 << 34, max_tree_jobs=1, fake=True,
                      fake_tree_ns_per_particle=1000.0)
