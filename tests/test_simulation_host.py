@@ -1,0 +1,89 @@
+"""The run loop's record points on the CPU (no GPU): sim::FileOutput::record
+(src/sim/run_output.cpp) records at the first call, wherever a stride falls
+and at the last step of a run; Simulation.run steps the device from one such
+point to the next. A stub system stands in for the device."""
+from __future__ import annotations
+
+import orrery_b200 as ob
+from orrery_b200.simulation import FileOutput, Simulation
+
+
+class StubSystem:
+    def __init__(self):
+        self.enqueued = []
+
+    def step_async(self, dt, steps, integrator):
+        self.enqueued.append(steps)
+
+    def step(self, dt, steps, integrator):
+        self.enqueued.append(steps)
+
+    def synchronize(self):
+        pass
+
+    def write_checkpoint(self, path, step, configuration=""):
+        self.last_checkpoint = (path, step, configuration)
+
+
+def stub_simulation(output):
+    sim = Simulation.__new__(Simulation)  # no device: only the loop is exercised
+    sim.system = StubSystem()
+    sim.timestep = 1e-3
+    sim.integrator_name = "vv"
+    sim.output = output
+    sim._step = 0
+    sim.n = 0
+    return sim
+
+
+class Recorder(FileOutput):
+    def __init__(self, **kw):
+        super().__init__(**kw)
+        self.points = []
+
+    def record(self, simulation, is_final):
+        self.points.append((simulation.step_index, is_final))
+        super().record(simulation, is_final)
+
+
+def test_checkpoints_fall_at_start_strides_and_end():
+    out = Recorder(checkpoint_path="run.ck", checkpoint_stride=8, configuration="text")
+    sim = stub_simulation(out)
+    sim.run(23)
+    assert [p for p, _ in out.points] == [0, 8, 16, 23]
+    assert out.points[-1] == (23, True)
+    assert out.checkpoints == 4
+    assert sim.system.last_checkpoint == ("run.ck", 23, "text")
+    assert sum(sim.system.enqueued) == 23 and sim.step_index == 23
+    assert sim.time == 23 * 1e-3
+
+
+def test_a_second_run_continues_the_strides():
+    out = Recorder(checkpoint_path="run.ck", checkpoint_stride=10)
+    sim = stub_simulation(out)
+    sim.run(12)
+    sim.run(15)
+    # The first call records step 0; the second run starts at 12 and records
+    # 20, then its last step 27 (src/sim/simulation.cpp:52-64).
+    assert [p for p, _ in out.points] == [0, 10, 12, 12, 20, 27]
+    assert sim.step_index == 27
+
+
+def test_next_due_takes_the_nearest_stride():
+    out = FileOutput(trajectory_path="t", trajectory_stride=5, checkpoint_path="c",
+                     checkpoint_stride=8)
+    assert out.next_due(0, 100) == 5
+    assert out.next_due(5, 100) == 8
+    assert out.next_due(8, 100) == 10
+    assert out.next_due(39, 40) == 40
+    assert FileOutput().next_due(3, 50) == 50
+
+
+def test_a_run_without_output_is_one_enqueue():
+    sim = stub_simulation(None)
+    sim.run(17)
+    assert sim.system.enqueued == [17] and sim.step_index == 17
+
+
+def test_the_package_exports_the_run_surface():
+    assert ob.Simulation is Simulation and ob.FileOutput is FileOutput
