@@ -84,6 +84,10 @@ System::~System() {
     for (auto e : marks_) {
         cudaEventDestroy(e);
     }
+    if (copy_stream_ != nullptr) {
+        cudaStreamDestroy(copy_stream_);
+        cudaEventDestroy(drifted_);
+    }
     for (auto e : ring_) {
         cudaEventDestroy(e);
     }
@@ -200,7 +204,7 @@ int System::evaluations_per_step(int integrator) {
     return integrator == OB_INTEGRATOR_YOSHIDA4 ? 3 : integrator == OB_INTEGRATOR_RK4 ? 4 : 1;
 }
 
-void System::enqueue_rk4_step(double dt, const cudaEvent_t *marks) {
+void System::enqueue_rk4_step(double dt, const cudaEvent_t *marks, cudaEvent_t drifted) {
     // RungeKutta4::step (src/integrators/runge_kutta4.cpp:64-139): stages at
     // h/2, h/2 and h weighted 2, 2, 1 after the first, the h/6 combination, and
     // the evaluation that leaves the carried accelerations at the final state.
@@ -219,22 +223,28 @@ void System::enqueue_rk4_step(double dt, const cudaEvent_t *marks) {
     check(launch_rk4_stage(1, state, save, n_, 2.0, dt, stream_), "RK4 third stage");
     evaluate(false, mark(2));
     check(launch_rk4_stage(2, state, save, n_, 1.0, sixth, stream_), "RK4 combination");
+    if (drifted != nullptr) {
+        check(cudaEventRecord(drifted, stream_), "recording the final positions");
+    }
     evaluate(false, mark(3));
 }
 
-void System::enqueue_substep(double timestep, const cudaEvent_t *marks) {
+void System::enqueue_substep(double timestep, const cudaEvent_t *marks, cudaEvent_t drifted) {
     // velocity_verlet_step (src/integrators/velocity_verlet.cpp:59-72).
     const double half = timestep / 2.0;
     check(launch_kick_drift(array(kX), array(kY), array(kZ), array(kVx), array(kVy), array(kVz),
                             array(kAx), array(kAy), array(kAz), n_, half, timestep, stream_),
           "kick and drift");
+    if (drifted != nullptr) {
+        check(cudaEventRecord(drifted, stream_), "recording the final positions");
+    }
     evaluate(false, marks);
     check(launch_kick(array(kVx), array(kVy), array(kVz), array(kAx), array(kAy), array(kAz), n_,
                       half, stream_),
           "kick");
 }
 
-void System::enqueue_step(int integrator, double dt, bool marked) {
+void System::enqueue_step(int integrator, double dt, bool marked, cudaEvent_t drifted) {
     // Without marks the solver records its own events, which a capture turns
     // into ordering only (no graph nodes).
     const cudaEvent_t *m = marked ? marks_.data() : nullptr;
@@ -243,11 +253,11 @@ void System::enqueue_step(int integrator, double dt, bool marked) {
         yoshida_weights(outer, inner);
         enqueue_substep(outer * dt, m);
         enqueue_substep(inner * dt, marked ? m + 4 : nullptr);
-        enqueue_substep(outer * dt, marked ? m + 8 : nullptr);
+        enqueue_substep(outer * dt, marked ? m + 8 : nullptr, drifted);
     } else if (integrator == OB_INTEGRATOR_RK4) {
-        enqueue_rk4_step(dt, m);
+        enqueue_rk4_step(dt, m, drifted);
     } else {
-        enqueue_substep(dt, m);
+        enqueue_substep(dt, m, drifted);
     }
 }
 
@@ -426,8 +436,35 @@ void System::step_host(int integrator, double dt, uint64_t steps, double *const 
     const double *in[9] = {io[0], io[1], io[2], io[3], io[4], io[5], io[6], io[7], io[8]};
     upload(kX, 9, in);
     upload(kM, 1, &m);
-    step_async(integrator, dt, steps);
-    get_state(io);
+    if (steps == 0 || n_ == 0) {
+        step_async(integrator, dt, steps);
+        get_state(io);
+        synchronize();
+        return;
+    }
+    // All but the last step replay the step graph; the last is enqueued
+    // directly with an event once its positions are final, so that their
+    // download overlaps its force evaluation (same kernels, same order).
+    step_async(integrator, dt, steps - 1);
+    ensure_graph(integrator, dt); // checks the integrator, reserves RK4's area
+    if (copy_stream_ == nullptr) {
+        check(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking), "a copy stream");
+        check(cudaEventCreateWithFlags(&drifted_, cudaEventDisableTiming), "an event");
+    }
+    enqueue_step(integrator, dt, false, drifted_);
+    solver_->account(evaluations_per_step(integrator), n_);
+    check(cudaStreamWaitEvent(copy_stream_, drifted_, 0), "ordering the position download");
+    for (int k = 0; k < 3; ++k) {
+        check(cudaMemcpyAsync(io[k], array(kX + k), sizeof(double) * n_, cudaMemcpyDeviceToHost,
+                              copy_stream_),
+              "downloading positions");
+    }
+    for (int k = 3; k < 9; ++k) {
+        check(cudaMemcpyAsync(io[k], array(kX + k), sizeof(double) * n_, cudaMemcpyDeviceToHost,
+                              stream_),
+              "downloading state");
+    }
+    check(cudaStreamSynchronize(copy_stream_), "downloading positions");
     synchronize();
 }
 

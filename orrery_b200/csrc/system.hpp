@@ -63,9 +63,10 @@ public:
 private:
     void upload(int first, int count, const double *const *host);
     void evaluate(bool count, const cudaEvent_t *marks = nullptr);
-    void enqueue_substep(double timestep, const cudaEvent_t *marks);
-    void enqueue_step(int integrator, double dt, bool marked);
-    void enqueue_rk4_step(double dt, const cudaEvent_t *marks);
+    // `drifted` (optional) is recorded once the step's positions are final.
+    void enqueue_substep(double timestep, const cudaEvent_t *marks, cudaEvent_t drifted = nullptr);
+    void enqueue_step(int integrator, double dt, bool marked, cudaEvent_t drifted = nullptr);
+    void enqueue_rk4_step(double dt, const cudaEvent_t *marks, cudaEvent_t drifted = nullptr);
     cudaGraph_t capture_step(int integrator, double dt, bool marked);
     void drop_graph();
     void ensure_graph(int integrator, double dt);
@@ -78,6 +79,10 @@ private:
     DeviceArray<double> terms_;
     DeviceArray<double> rk4_; // RK4: x0, v0 and the derivative sums (12n), reserved on first use
     cudaStream_t stream_ = nullptr;
+    // step_host: downloads the positions on this stream while the last step's
+    // force evaluation runs (created on first use).
+    cudaStream_t copy_stream_ = nullptr;
+    cudaEvent_t drifted_ = nullptr;
     bool owns_stream_ = true;
     // The step as a CUDA graph, without event nodes: what every step replays
     // unless it is profiled.
