@@ -55,21 +55,6 @@ __device__ __forceinline__ void source_tiles(uint32_t n, uint32_t split, uint32_
     te = min(tb + per, tiles);
 }
 
-// Issues the bulk copies of tile `k` into buffer `buf` (thread 0 only).
-template <bool SPLIT>
-__device__ __forceinline__ void stage_tile(const DirectArgs &a, float4 *tiles_hi,
-                                           float4 *tiles_lo, uint64_t *bars, uint32_t k,
-                                           uint32_t buf) {
-    constexpr uint32_t bytes = kDirectTile * sizeof(float4);
-    mbar_arrive_expect_tx(&bars[buf], SPLIT ? 2 * bytes : bytes);
-    bulk_copy_g2s(tiles_hi + buf * kDirectTile, a.hi + static_cast<size_t>(k) * kDirectTile,
-                  bytes, &bars[buf]);
-    if (SPLIT) {
-        bulk_copy_g2s(tiles_lo + buf * kDirectTile, a.lo + static_cast<size_t>(k) * kDirectTile,
-                      bytes, &bars[buf]);
-    }
-}
-
 // Sources per unrolled step of the tile loop: a thread with a single target
 // pair (the shapes for small systems, few warps per SM) gets more independent
 // chains to overlap.
