@@ -1,0 +1,40 @@
+"""The C++ in INTEGRATION.md compiles against the reference's headers.
+
+The listings there (the ForceSolver adapter, the Integrator wrapper, the run
+with output) are what a maintainer would paste into the reference; each is
+compiled here with g++ -fsyntax-only against the reference's include tree and
+this library's C header, so that a change on either side that breaks them
+shows up. Skipped where the reference's sources or g++ are absent.
+"""
+from __future__ import annotations
+
+import os
+import re
+import shutil
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REFERENCE_INCLUDE = os.environ.get("ORRERY_REFERENCE_INCLUDE", "/root/reference/include")
+
+
+def listings():
+    with open(os.path.join(ROOT, "INTEGRATION.md")) as fh:
+        return re.findall(r"```cpp\n(.*?)```", fh.read(), re.S)
+
+
+def test_there_are_listings():
+    assert len(listings()) >= 3
+
+
+@pytest.mark.parametrize("index", range(len(listings())))
+def test_listing_compiles_against_the_reference(tmp_path, index):
+    if shutil.which("g++") is None or not os.path.isdir(REFERENCE_INCLUDE):
+        pytest.skip("g++ or the reference's headers are not available here")
+    source = tmp_path / f"listing{index}.cpp"
+    source.write_text(listings()[index])
+    out = subprocess.run(["g++", "-std=c++20", "-fsyntax-only", f"-I{REFERENCE_INCLUDE}",
+                          f"-I{os.path.join(ROOT, 'include')}", str(source)],
+                         capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr[-3000:]
