@@ -306,6 +306,7 @@ class Reference:
         lib.ref_read_trajectory.argtypes = [C.c_char_p, _u64p, _dp, C.POINTER(C.c_int),
                                             C.POINTER(C.c_size_t), C.c_size_t, C.c_size_t, _dp,
                                             _u64p, _dp, _dp, _dp]
+        lib.ref_write_diagnostics_log.argtypes = [C.c_char_p, C.c_size_t, _u64p] + [_dp] * 5
 
     @staticmethod
     def available(path: str = REFERENCE_PATH) -> bool:
@@ -363,6 +364,23 @@ class Reference:
                                          _d(times), _d(np.ascontiguousarray(xyz)),
                                          _d(np.ascontiguousarray(v))) != 0:
             self._raise("TrajectoryWriter")
+
+    def write_diagnostics_log(self, path, rows):
+        """sim::DiagnosticsLog: `rows` is a list of (step, time, diagnostics),
+        each diagnostics a dict as `diagnostics` returns."""
+        steps = np.array([r[0] for r in rows] or [0], dtype=np.uint64)
+        cols = {k: np.array([r[2][k] for r in rows] or [0.0], dtype=np.float64)
+                for k in ("kinetic_energy", "potential_energy")}
+        vecs = {k: np.ascontiguousarray(np.concatenate([np.asarray(r[2][k], dtype=np.float64)
+                                                        for r in rows]) if rows else np.zeros(3))
+                for k in ("linear_momentum", "angular_momentum")}
+        times = np.array([r[1] for r in rows] or [0.0], dtype=np.float64)
+        if self.lib.ref_write_diagnostics_log(os.fsencode(path), len(rows), _u(steps), _d(times),
+                                              _d(cols["kinetic_energy"]),
+                                              _d(cols["potential_energy"]),
+                                              _d(vecs["linear_momentum"]),
+                                              _d(vecs["angular_momentum"])) != 0:
+            self._raise("DiagnosticsLog")
 
     def read_trajectory(self, path, max_frames=16, max_n=4096):
         """sim::TrajectoryReader: header facts and the frames."""

@@ -1,5 +1,6 @@
-// C entry points over the reference's own checkpoint and trajectory code
-// (src/sim/checkpoint.cpp, src/sim/trajectory.cpp, src/sim/config_file.cpp),
+// C entry points over the reference's own checkpoint, trajectory and
+// diagnostics-log code (src/sim/checkpoint.cpp, src/sim/trajectory.cpp,
+// src/sim/diagnostics_log.cpp, src/sim/config_file.cpp),
 // so that the tests can compare this backend's files with the reference's
 // byte for byte and read each side's files with the other's reader.
 //
@@ -17,6 +18,7 @@
 #include "orrery/sim/checkpoint.hpp"
 #include "orrery/sim/config_file.hpp"
 #include "orrery/sim/configuration.hpp"
+#include "orrery/sim/diagnostics_log.hpp"
 #include "orrery/sim/trajectory.hpp"
 
 namespace {
@@ -204,6 +206,30 @@ int ref_read_trajectory(const char* path, std::uint64_t* n, double* timestep,
             ++f;
         }
         *frames = f;
+    });
+}
+
+// sim::DiagnosticsLog: the header row, then one row per measurement; row r is
+// step[r], time[r] and the core::Diagnostics of kinetic[r], potential[r],
+// linear[3r..3r+2], angular[3r..3r+2].
+int ref_write_diagnostics_log(const char* path, std::size_t rows, const std::uint64_t* steps,
+                              const double* times, const double* kinetic,
+                              const double* potential, const double* linear,
+                              const double* angular) {
+    return guarded([&] {
+        orrery::sim::DiagnosticsLog log(path);
+        for (std::size_t r = 0; r < rows; ++r) {
+            orrery::core::Diagnostics d;
+            d.kinetic_energy = kinetic[r];
+            d.potential_energy = potential[r];
+            d.linear_momentum = {linear[3 * r], linear[3 * r + 1], linear[3 * r + 2]};
+            d.angular_momentum = {angular[3 * r], angular[3 * r + 1], angular[3 * r + 2]};
+            log.record(steps[r], times[r], d);
+        }
+        log.flush();
+        if (!log.ok()) {
+            throw std::runtime_error("the diagnostics log could not be written");
+        }
     });
 }
 

@@ -913,4 +913,5 @@ def compute_accelerations(positions, masses, softening: float = 0.0, solver: str
     return s.evaluate(positions, masses)
 
 
-from .simulation import DeviceArrayView, FileOutput, Simulation, device_arrays  # noqa: E402,F401
+from .simulation import (DeviceArrayView, DiagnosticsLog, FileOutput, Simulation,  # noqa: E402,F401
+                         device_arrays)

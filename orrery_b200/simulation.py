@@ -13,6 +13,9 @@ of it (``__cuda_array_interface__``, readable by torch, CuPy or Numba).
 from __future__ import annotations
 
 import ctypes as C
+import math
+
+import numpy as np
 
 from . import (DeviceSystem, OrreryError, Trajectory, SOLVER_DIRECT, SOLVER_TREE,
                ERROR_INVALID_ARGUMENT, _check, _f64, _ptr, load_library)
@@ -45,24 +48,85 @@ def device_arrays(system: DeviceSystem) -> dict:
     return {k: DeviceArrayView(ptrs[i] or 0, system.n, system) for i, k in enumerate(_STATE)}
 
 
+_DIAGNOSTICS_HEADER = ("step,time,kinetic_energy,potential_energy,total_energy,"
+                       "relative_energy_error,virial_ratio,momentum_x,momentum_y,momentum_z,"
+                       "angular_momentum_x,angular_momentum_y,angular_momentum_z\n")
+
+
+def _real(value: float) -> str:
+    """A double as the reference's log writes it: an ostream in the classic
+    locale at max_digits10 = 17 significant digits, i.e. C's "%.17g", whose
+    NaN carries its sign ("-nan" for the x86 default NaN of 0/0)."""
+    if value != value:
+        return "-nan" if math.copysign(1.0, value) < 0 else "nan"
+    return "%.17g" % value
+
+
+def _virial_ratio(kinetic: float, potential: float) -> float:
+    """2T/|U| with IEEE division (core/diagnostics.hpp:79-82): no potential
+    energy gives an infinity, or a NaN when nothing moves either."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return float(np.float64(2 * kinetic) /
+                     np.float64(-potential if potential < 0 else potential))
+
+
+class DiagnosticsLog:
+    """sim::DiagnosticsLog (src/sim/diagnostics_log.cpp): a CSV of the
+    conserved quantities, one row per measurement, every number at full
+    precision. The first row fixes the energy the error column is relative to
+    (core::relative_energy_error, src/core/diagnostics.cpp:85-89: the absolute
+    difference when that energy is zero)."""
+
+    def __init__(self, path):
+        self._file = open(path, "w", encoding="ascii", newline="\n")
+        self._file.write(_DIAGNOSTICS_HEADER)
+        self.reference_energy = None
+
+    def record(self, step: int, time: float, diagnostics: dict) -> None:
+        kinetic = float(diagnostics["kinetic_energy"])
+        potential = float(diagnostics["potential_energy"])
+        energy = kinetic + potential
+        if self.reference_energy is None:
+            self.reference_energy = energy
+        scale = abs(self.reference_energy)
+        difference = energy - self.reference_energy
+        error = difference / scale if scale > 0 else difference
+        row = [kinetic, potential, energy, error, _virial_ratio(kinetic, potential),
+               *(float(v) for v in diagnostics["linear_momentum"]),
+               *(float(v) for v in diagnostics["angular_momentum"])]
+        self._file.write(f"{int(step)},{_real(float(time))}," +
+                         ",".join(_real(v) for v in row) + "\n")
+
+    def flush(self) -> None:
+        self._file.flush()
+
+    def close(self) -> None:
+        self._file.close()
+
+
 class FileOutput:
     """sim::FileOutput (src/sim/run_output.cpp): a trajectory frame every
-    ``trajectory_stride`` steps and a checkpoint every ``checkpoint_stride``,
-    each also at the first record and the last step of a run (a stride of 0:
-    only those). Frames are device snapshots written in the background; the
-    trajectory is flushed with each checkpoint, so a run killed after a
-    checkpoint leaves frames that reach at least that far."""
+    ``trajectory_stride`` steps, a diagnostics row every ``diagnostics_stride``
+    and a checkpoint every ``checkpoint_stride``, each also at the first record
+    and the last step of a run (a stride of 0: only those). Frames are device
+    snapshots written in the background. The trajectory and the diagnostics
+    log are flushed with each checkpoint, after it is written, as the
+    reference does."""
 
     def __init__(self, trajectory_path=None, trajectory_stride: int = 0,
                  trajectory_velocities: bool = False, checkpoint_path=None,
-                 checkpoint_stride: int = 0, configuration: str = ""):
+                 checkpoint_stride: int = 0, configuration: str = "",
+                 diagnostics_path=None, diagnostics_stride: int = 0):
         self.trajectory_path = trajectory_path
         self.trajectory_stride = int(trajectory_stride)
         self.trajectory_velocities = bool(trajectory_velocities)
         self.checkpoint_path = checkpoint_path
         self.checkpoint_stride = int(checkpoint_stride)
+        self.diagnostics_path = diagnostics_path
+        self.diagnostics_stride = int(diagnostics_stride)
         self.configuration = configuration
         self._trajectory = None
+        self._diagnostics = None
         self._first = True
         self.checkpoints = 0
 
@@ -73,6 +137,7 @@ class FileOutput:
         """The first step after `step`, up to `last`, at which something is due."""
         due = last
         for stride, on in ((self.trajectory_stride, self.trajectory_path),
+                           (self.diagnostics_stride, self.diagnostics_path),
                            (self.checkpoint_stride, self.checkpoint_path)):
             if on and stride > 0:
                 due = min(due, (step // stride + 1) * stride)
@@ -87,12 +152,19 @@ class FileOutput:
                                               with_velocities=self.trajectory_velocities)
             if self._due(step, self.trajectory_stride, is_final):
                 self._trajectory.write_frame(step, simulation.time)
+        if self.diagnostics_path is not None:
+            if self._diagnostics is None:
+                self._diagnostics = DiagnosticsLog(self.diagnostics_path)
+            if self._due(step, self.diagnostics_stride, is_final):
+                self._diagnostics.record(step, simulation.time, simulation.measure())
         if self.checkpoint_path is not None and \
                 self._due(step, self.checkpoint_stride, is_final):
-            if self._trajectory is not None:
-                self._trajectory.flush()
             simulation.write_checkpoint(self.checkpoint_path, self.configuration)
             self.checkpoints += 1
+            if self._trajectory is not None:
+                self._trajectory.flush()
+            if self._diagnostics is not None:
+                self._diagnostics.flush()
         self._first = False
 
     @property
@@ -103,6 +175,9 @@ class FileOutput:
         if self._trajectory is not None:
             self._trajectory.close()
             self._trajectory = None
+        if self._diagnostics is not None:
+            self._diagnostics.close()
+            self._diagnostics = None
 
 
 class Simulation:
@@ -201,9 +276,7 @@ class Simulation:
         and total energy, linear and angular momentum, virial ratio."""
         d = self.system.diagnostics()
         d["total_energy"] = d["kinetic_energy"] + d["potential_energy"]
-        pe = d["potential_energy"]
-        d["virial_ratio"] = 2 * d["kinetic_energy"] / (-pe if pe < 0 else pe) if pe else \
-            float("inf")
+        d["virial_ratio"] = _virial_ratio(d["kinetic_energy"], d["potential_energy"])
         return d
 
     @property

@@ -79,7 +79,8 @@ def test_run_output_records_where_the_reference_does(b200, reference, tmp_path):
     # the end.
     out = b200.FileOutput(trajectory_path=tmp_path / "run.tj", trajectory_stride=5,
                           trajectory_velocities=True, checkpoint_path=tmp_path / "run.ck",
-                          checkpoint_stride=8, configuration="[run]\ntimestep = 0.001\n")
+                          checkpoint_stride=8, configuration="[run]\ntimestep = 0.001\n",
+                          diagnostics_path=tmp_path / "run.csv", diagnostics_stride=5)
     sim = b200.Simulation(plummer(500), timestep=1e-3, softening=0.01, output=out)
     sim.run(23)
     out.close()
@@ -92,6 +93,14 @@ def test_run_output_records_where_the_reference_does(b200, reference, tmp_path):
     assert out.checkpoints == 4  # steps 0, 8, 16, 23
     ck = reference.read_checkpoint(tmp_path / "run.ck")
     assert ck["step"] == 23
+    # The diagnostics rows fall on the frames' steps: the reference's
+    # DiagnosticsLog over core::measure_diagnostics of each frame writes the
+    # same file, byte for byte.
+    rows = [(step, time, reference.diagnostics(st["x"], st["y"], st["z"], st["vx"], st["vy"],
+                                               st["vz"], got["masses"], 0.01))
+            for step, time, st in got["frames"]]
+    reference.write_diagnostics_log(tmp_path / "ref.csv", rows)
+    assert (tmp_path / "run.csv").read_bytes() == (tmp_path / "ref.csv").read_bytes()
 
 
 @pytest.mark.parametrize("solver,precision,integrator", [("direct", "fp32", "vv"),

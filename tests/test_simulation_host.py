@@ -24,6 +24,10 @@ class StubSystem:
     def write_checkpoint(self, path, step, configuration=""):
         self.last_checkpoint = (path, step, configuration)
 
+    def diagnostics(self):
+        return {"kinetic_energy": 0.25, "potential_energy": -0.5,
+                "linear_momentum": [0.0, 0.0, 0.0], "angular_momentum": [0.0, 0.0, 1.0]}
+
 
 def stub_simulation(output):
     sim = Simulation.__new__(Simulation)  # no device: only the loop is exercised
@@ -69,6 +73,20 @@ def test_a_second_run_continues_the_strides():
     assert sim.step_index == 27
 
 
+def test_diagnostics_rows_fall_at_start_strides_and_end(tmp_path):
+    path = tmp_path / "run.csv"
+    out = Recorder(diagnostics_path=path, diagnostics_stride=4)
+    sim = stub_simulation(out)
+    sim.run(10)
+    out.close()
+    lines = path.read_text().splitlines()
+    assert lines[0].startswith("step,time,kinetic_energy,")
+    assert [int(r.split(",")[0]) for r in lines[1:]] == [0, 4, 8, 10]
+    assert [float(r.split(",")[1]) for r in lines[1:]] == [0.0, 4e-3, 8e-3, 10 * 1e-3]
+    # The device was stepped only to the record points.
+    assert sim.system.enqueued == [4, 4, 2]
+
+
 def test_next_due_takes_the_nearest_stride():
     out = FileOutput(trajectory_path="t", trajectory_stride=5, checkpoint_path="c",
                      checkpoint_stride=8)
@@ -77,12 +95,31 @@ def test_next_due_takes_the_nearest_stride():
     assert out.next_due(8, 100) == 10
     assert out.next_due(39, 40) == 40
     assert FileOutput().next_due(3, 50) == 50
+    assert FileOutput(diagnostics_path="d", diagnostics_stride=3).next_due(3, 50) == 6
 
 
 def test_a_run_without_output_is_one_enqueue():
     sim = stub_simulation(None)
     sim.run(17)
     assert sim.system.enqueued == [17] and sim.step_index == 17
+
+
+def test_virial_ratio_follows_the_reference_division():
+    # 2T/|U| (core/diagnostics.hpp:79-82): a bound state gives a number, no
+    # potential energy an infinity, and nothing at all a NaN.
+    import math
+
+    sim = stub_simulation(None)
+    for kinetic, potential, expected in ((0.25, -0.5, 1.0), (0.5, 0.0, math.inf),
+                                         (0.0, 0.0, math.nan), (0.125, 0.5, 0.5)):
+        sim.system.diagnostics = lambda k=kinetic, p=potential: {
+            "kinetic_energy": k, "potential_energy": p}
+        d = sim.measure()
+        assert d["total_energy"] == kinetic + potential
+        if math.isnan(expected):
+            assert math.isnan(d["virial_ratio"])
+        else:
+            assert d["virial_ratio"] == expected
 
 
 def test_the_package_exports_the_run_surface():
