@@ -18,9 +18,15 @@ import math
 import numpy as np
 
 from . import (DeviceSystem, OrreryError, Trajectory, SOLVER_DIRECT, SOLVER_TREE,
-               ERROR_INVALID_ARGUMENT, _check, _f64, _ptr, load_library)
+               ERROR_INVALID_ARGUMENT, INTEGRATOR_RK4, INTEGRATOR_VV, INTEGRATOR_YOSHIDA4,
+               _INTEGRATORS, _check, _f64, _ptr, load_library)
 
 _STATE = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
+
+# Integrator::name of the reference's three integrators
+# (include/orrery/integrators/{velocity_verlet,yoshida4,runge_kutta4}.hpp).
+_INTEGRATOR_NAMES = {INTEGRATOR_VV: "velocity Verlet", INTEGRATOR_YOSHIDA4: "Yoshida 4",
+                     INTEGRATOR_RK4: "RK4"}
 
 
 class DeviceArrayView:
@@ -151,7 +157,14 @@ class FileOutput:
                                               system=simulation.system,
                                               with_velocities=self.trajectory_velocities)
             if self._due(step, self.trajectory_stride, is_final):
-                self._trajectory.write_frame(step, simulation.time)
+                if self._trajectory._system is simulation.system:
+                    self._trajectory.write_frame(step, simulation.time)
+                elif simulation.n == self._trajectory.n:
+                    # The system was replaced by a restore: a frame of its state
+                    # from the host.
+                    self._trajectory.write_frame(step, simulation.time, simulation.particles)
+                # A state of another particle count is not written: the format
+                # has no per-frame length (src/sim/trajectory.cpp:73-79).
         if self.diagnostics_path is not None:
             if self._diagnostics is None:
                 self._diagnostics = DiagnosticsLog(self.diagnostics_path)
@@ -194,17 +207,25 @@ class Simulation:
         kind = SOLVER_TREE if solver in ("tree", "barnes-hut") else SOLVER_DIRECT
         if solver not in ("direct", "tree", "barnes-hut"):
             raise OrreryError(ERROR_INVALID_ARGUMENT, f"unknown solver {solver!r}")
+        if integrator not in _INTEGRATORS:
+            raise OrreryError(ERROR_INVALID_ARGUMENT, f"unknown integrator {integrator!r}")
         arrs = {k: _f64(state[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
         self.n = len(arrs["m"])
-        self.system = DeviceSystem(self.n, softening, kind, precision, opening_angle,
-                                   leaf_capacity, quadrupole)
+        self._solver = (softening, kind, precision, opening_angle, leaf_capacity, quadrupole)
+        self.system = DeviceSystem(self.n, *self._solver)
         self.system.set_state(arrs["x"], arrs["y"], arrs["z"], arrs["vx"], arrs["vy"],
                               arrs["vz"], arrs["m"])
         self.timestep = float(timestep)
-        self.integrator_name = integrator
+        self._integrator = integrator
         self.solver_name = "b200-tree" if kind == SOLVER_TREE else "b200-direct"
         self.output = output
         self._step = 0
+
+    @property
+    def integrator_name(self) -> str:
+        """The integrator's name as the reference's integrators give it
+        (Integrator::name: "velocity Verlet", "Yoshida 4", "RK4")."""
+        return _INTEGRATOR_NAMES[_INTEGRATORS[self._integrator]]
 
     # -- the clock ----------------------------------------------------------
 
@@ -221,7 +242,7 @@ class Simulation:
 
     def step(self) -> None:
         """Advance by one step. Records nothing."""
-        self.system.step(self.timestep, 1, self.integrator_name)
+        self.system.step(self.timestep, 1, self._integrator)
         self._step += 1
 
     def run(self, steps: int) -> None:
@@ -230,14 +251,14 @@ class Simulation:
         steps = int(steps)
         out = self.output
         if out is None:
-            self.system.step(self.timestep, steps, self.integrator_name)
+            self.system.step(self.timestep, steps, self._integrator)
             self._step += steps
             return
         out.record(self, steps == 0)
         end = self._step + steps
         while self._step < end:
             target = out.next_due(self._step, end)
-            self.system.step_async(self.timestep, target - self._step, self.integrator_name)
+            self.system.step_async(self.timestep, target - self._step, self._integrator)
             self._step = target
             out.record(self, self._step == end)
         self.system.synchronize()
@@ -256,11 +277,18 @@ class Simulation:
 
     def restore(self, state: dict, step: int = 0, accelerations_are_current: bool = False):
         """Replace the state and the step counter. Re-establishes the carried
-        accelerations with one evaluation unless they are given as current."""
+        accelerations with one evaluation unless they are given as current.
+        The particle count may differ from the current one
+        (python/src/sim_bindings.cpp:293-309): the state then moves to a new
+        device system of that size, with the same solver settings."""
         keys = ("x", "y", "z", "vx", "vy", "vz", "m")
         arrs = {k: _f64(state[k]) for k in keys}
-        if len(arrs["m"]) != self.n:
-            raise OrreryError(ERROR_INVALID_ARGUMENT, "a restored state keeps the particle count")
+        n = len(arrs["m"])
+        if any(len(a) != n for a in arrs.values()):
+            raise OrreryError(ERROR_INVALID_ARGUMENT, "the state arrays differ in length")
+        if n != self.n:
+            self.system = DeviceSystem(n, *self._solver)
+            self.n = n
         if accelerations_are_current:
             acc = {k: _f64(state[k]) for k in ("ax", "ay", "az")}
             lib = load_library()

@@ -103,6 +103,31 @@ def test_run_output_records_where_the_reference_does(b200, reference, tmp_path):
     assert (tmp_path / "run.csv").read_bytes() == (tmp_path / "ref.csv").read_bytes()
 
 
+def test_restore_takes_another_particle_count(b200, reference, tmp_path):
+    # The reference's restore accepts any count (python/src/sim_bindings.cpp:
+    # 293-309); its trajectory writer then skips frames of the wrong length
+    # (src/sim/trajectory.cpp:73-79) while diagnostics rows go on.
+    out = b200.FileOutput(trajectory_path=tmp_path / "t.tj", trajectory_stride=1,
+                          diagnostics_path=tmp_path / "d.csv", diagnostics_stride=1)
+    sim = b200.Simulation(plummer(300), timestep=1e-3, softening=0.01, precision="fp64",
+                          output=out)
+    sim.run(2)
+    other = plummer(200, seed=9)
+    sim.restore(other, step=2)
+    assert sim.n == 200 and sim.step_index == 2
+    sim.run(3)
+    out.close()
+    fresh = b200.Simulation(other, timestep=1e-3, softening=0.01, precision="fp64")
+    fresh.run(3)
+    got, want = sim.particles, fresh.particles
+    for k in KEYS:
+        assert np.array_equal(got[k], want[k]), k
+    tj = reference.read_trajectory(tmp_path / "t.tj", max_frames=8, max_n=300)
+    assert tj["n"] == 300 and [f[0] for f in tj["frames"]] == [0, 1, 2]
+    rows = (tmp_path / "d.csv").read_text().splitlines()[1:]
+    assert [int(r.split(",")[0]) for r in rows] == [0, 1, 2, 2, 3, 4, 5]
+
+
 @pytest.mark.parametrize("solver,precision,integrator", [("direct", "fp32", "vv"),
                                                          ("tree", "fp32", "rk4"),
                                                          ("tree", "fp64", "yoshida4")])

@@ -33,7 +33,7 @@ def stub_simulation(output):
     sim = Simulation.__new__(Simulation)  # no device: only the loop is exercised
     sim.system = StubSystem()
     sim.timestep = 1e-3
-    sim.integrator_name = "vv"
+    sim._integrator = "vv"
     sim.output = output
     sim._step = 0
     sim.n = 0
@@ -120,6 +120,23 @@ def test_virial_ratio_follows_the_reference_division():
             assert math.isnan(d["virial_ratio"])
         else:
             assert d["virial_ratio"] == expected
+
+
+def test_integrator_names_are_the_reference_integrators_names():
+    # Integrator::name (include/orrery/integrators/*.hpp), whichever of the
+    # configuration's spellings chose it.
+    sim = stub_simulation(None)
+    for key, name in (("vv", "velocity Verlet"), ("velocity-verlet", "velocity Verlet"),
+                      ("yoshida4", "Yoshida 4"), ("rk4", "RK4"), ("runge-kutta4", "RK4")):
+        sim._integrator = key
+        assert sim.integrator_name == name
+
+
+def test_an_unknown_integrator_is_refused_before_the_device_is_touched():
+    import pytest
+
+    with pytest.raises(ob.OrreryError):
+        Simulation({"m": [1.0]}, timestep=1e-3, integrator="euler")
 
 
 def test_the_package_exports_the_run_surface():
