@@ -455,9 +455,10 @@ def direct_shapes(precision: str = "fp32"):
 
 
 def _split_xyz(positions):
-    p = np.asarray(positions, dtype=np.float64)
-    if isinstance(positions, (tuple, list)) and len(positions) == 3:
+    if isinstance(positions, (tuple, list)) and len(positions) == 3 and \
+            all(np.ndim(a) == 1 for a in positions):
         return tuple(_f64(a) for a in positions)
+    p = np.asarray(positions, dtype=np.float64)
     if p.ndim == 2 and p.shape[0] == 3 and p.shape[1] != 3:
         return tuple(_f64(p[k]) for k in range(3))
     if p.ndim == 2 and p.shape[1] == 3:
@@ -899,11 +900,49 @@ def work_units(count: int, steps: int, solver: str) -> float:
     return load_library().ob_work_units(int(count), int(steps), kind)
 
 
+_PARTICLE_ARRAYS = ("position_x", "position_y", "position_z", "mass",
+                    "acceleration_x", "acceleration_y", "acceleration_z")
+
+
 def compute_accelerations(positions, masses, softening: float = 0.0, solver: str = "direct",
-                          precision: str = "fp32", opening_angle: float = 0.5,
-                          leaf_capacity: int = 32, quadrupole: bool = False) -> np.ndarray:
+                          precision: str = None, opening_angle: float = 0.5,
+                          leaf_capacity: int = 32, quadrupole: bool = False):
     """One force evaluation, the counterpart of the reference's Python
-    ``orrery.compute_accelerations`` (python/src/sim_bindings.cpp:383-410)."""
+    ``orrery.compute_accelerations`` (python/src/sim_bindings.cpp:383-410).
+
+    Two forms:
+
+    * ``compute_accelerations(positions, masses, ...)``: positions (N, 3) or
+      (3, N) and masses (N,); returns the (N, 3) accelerations. Precision
+      defaults to "fp32".
+    * ``compute_accelerations(configuration, particles)``, the reference's own
+      call: ``configuration.solver`` supplies the kind ("direct" or
+      "barnes-hut"; the reference's "sycl-direct" and "sycl-tree" name the
+      same algorithms on a device), softening, opening angle, leaf capacity
+      and quadrupole flag; ``particles`` is the reference's ParticleData (or
+      anything with its position_x ... mass and acceleration_x ... arrays).
+      The accelerations are written into the particles in place and the
+      InteractionCount is returned. Precision defaults to "fp64", whose forces
+      equal the reference's DirectSolver and BarnesHutSolver (scalar kernels)
+      bit for bit; the other settings of the configuration are not read.
+    """
+    if hasattr(positions, "solver") and all(hasattr(masses, k) for k in _PARTICLE_ARRAYS):
+        settings, particles = positions.solver, masses
+        kind = str(settings.kind)
+        precision = precision or "fp64"
+        if kind in ("direct", "sycl-direct"):
+            s = B200DirectSolver(float(settings.softening), precision)
+        elif kind in ("barnes-hut", "sycl-tree"):
+            s = B200TreeSolver(float(settings.softening), float(settings.opening_angle),
+                               int(settings.leaf_capacity), bool(settings.quadrupole),
+                               precision)
+        else:
+            raise OrreryError(ERROR_INVALID_ARGUMENT, f"unknown solver kind {kind!r}")
+        xyz = [np.asarray(getattr(particles, k)) for k in _PARTICLE_ARRAYS[:3]]
+        s.evaluate(xyz, np.asarray(particles.mass),
+                   [np.asarray(getattr(particles, k)) for k in _PARTICLE_ARRAYS[4:]])
+        return s.interaction_count()
+    precision = precision or "fp32"
     if solver == "direct":
         s = B200DirectSolver(softening, precision)
     elif solver in ("tree", "barnes-hut"):

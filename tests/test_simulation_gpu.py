@@ -103,6 +103,35 @@ def test_run_output_records_where_the_reference_does(b200, reference, tmp_path):
     assert (tmp_path / "run.csv").read_bytes() == (tmp_path / "ref.csv").read_bytes()
 
 
+@pytest.mark.parametrize("kind", ["direct", "barnes-hut"])
+def test_compute_accelerations_in_the_reference_call_form(b200, reference, kind):
+    # compute_accelerations(configuration, particles) writes the particles'
+    # acceleration arrays in place and returns the count
+    # (python/src/sim_bindings.cpp:383-410); at its default FP64 precision the
+    # forces are the reference solvers' (scalar kernels) bit for bit.
+    from types import SimpleNamespace
+
+    d = plummer(900, seed=4)
+    p = SimpleNamespace(position_x=d["x"].copy(), position_y=d["y"].copy(),
+                        position_z=d["z"].copy(), mass=d["m"].copy(),
+                        acceleration_x=np.zeros(900), acceleration_y=np.zeros(900),
+                        acceleration_z=np.zeros(900))
+    cfg = SimpleNamespace(solver=SimpleNamespace(kind=kind, softening=0.02, opening_angle=0.5,
+                                                 leaf_capacity=32, quadrupole=True))
+    count = b200.compute_accelerations(cfg, p)
+    got = np.stack([p.acceleration_x, p.acceleration_y, p.acceleration_z], axis=1)
+    if kind == "direct":
+        want, pairs = reference.direct(d["x"], d["y"], d["z"], d["m"], 0.02)
+        assert count.particle_particle == pairs
+    else:
+        want, counts, _ = reference.barnes_hut(d["x"], d["y"], d["z"], d["m"], 0.02, 0.5, 32,
+                                               True, with_tree=False)
+        assert (count.particle_particle, count.particle_cell) == (int(counts[1]),
+                                                                  int(counts[2]))
+    assert count.evaluations == 1
+    assert np.array_equal(got, want)
+
+
 def test_restore_takes_another_particle_count(b200, reference, tmp_path):
     # The reference's restore accepts any count (python/src/sim_bindings.cpp:
     # 293-309); its trajectory writer then skips frames of the wrong length
