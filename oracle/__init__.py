@@ -262,6 +262,7 @@ class Reference:
         self.lib = lib
         lib.ref_default_worker_count.restype = C.c_uint
         lib.ref_plummer.argtypes = [C.c_size_t, C.c_double, C.c_double, C.c_uint64] + [_dp] * 7
+        lib.ref_kepler_orbit.argtypes = [C.c_double] * 4 + [_dp] * 8
         lib.ref_direct.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, C.c_int, C.c_int,
                                    _dp, _dp, _dp, _u64p]
         lib.ref_direct_timed.argtypes = [C.c_size_t, _dp, _dp, _dp, _dp, C.c_double, C.c_int,
@@ -417,6 +418,17 @@ class Reference:
         if rc != 0:
             raise RuntimeError("reference Plummer sampler failed")
         return dict(zip(("x", "y", "z", "vx", "vy", "vz", "m"), arrs))
+
+    def kepler_orbit(self, primary_mass=1.0, secondary_mass=1.0, semi_major_axis=1.0,
+                     eccentricity=0.0):
+        """initial_conditions::make_kepler_orbit and kepler_period: (state, period),
+        or None where the reference refuses the parameters."""
+        arrs = [np.zeros(2) for _ in range(7)]
+        period = np.zeros(1)
+        if self.lib.ref_kepler_orbit(primary_mass, secondary_mass, semi_major_axis, eccentricity,
+                                     *(_d(a) for a in arrs), _d(period)) != 0:
+            return None
+        return dict(zip(("x", "y", "z", "vx", "vy", "vz", "m"), arrs)), float(period[0])
 
     def direct(self, x, y, z, m, softening, kernel="scalar", threads=1):
         n = len(m)

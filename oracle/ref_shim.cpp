@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <exception>
 #include <memory>
 #include <span>
 #include <vector>
@@ -19,6 +20,7 @@
 #include "orrery/core/particle_data.hpp"
 #include "orrery/core/random.hpp"
 #include "orrery/core/softening.hpp"
+#include "orrery/initial_conditions/kepler.hpp"
 #include "orrery/initial_conditions/plummer.hpp"
 #include "orrery/integrators/runge_kutta4.hpp"
 #include "orrery/integrators/velocity_verlet.hpp"
@@ -102,6 +104,27 @@ int ref_plummer(std::size_t count, double total_mass, double scale_radius, std::
     const ParticleData data = orrery::initial_conditions::make_plummer_sphere(params, random);
     copy_out(data, x, y, z, vx, vy, vz, nullptr, nullptr, nullptr, m);
     return static_cast<int>(data.size() == count ? 0 : -1);
+}
+
+// make_kepler_orbit and kepler_period: the two bodies' state (2 entries per
+// array) and the period. Returns -1, writing nothing, where the reference
+// refuses the parameters.
+int ref_kepler_orbit(double primary_mass, double secondary_mass, double semi_major_axis,
+                     double eccentricity, double* x, double* y, double* z, double* vx, double* vy,
+                     double* vz, double* m, double* period) {
+    orrery::initial_conditions::KeplerParameters params;
+    params.primary_mass = primary_mass;
+    params.secondary_mass = secondary_mass;
+    params.semi_major_axis = semi_major_axis;
+    params.eccentricity = eccentricity;
+    try {
+        const ParticleData data = orrery::initial_conditions::make_kepler_orbit(params);
+        copy_out(data, x, y, z, vx, vy, vz, nullptr, nullptr, nullptr, m);
+        *period = orrery::initial_conditions::kepler_period(params);
+    } catch (const std::exception&) {
+        return -1;
+    }
+    return 0;
 }
 
 int ref_direct(std::size_t n, const double* x, const double* y, const double* z, const double* m,

@@ -213,3 +213,39 @@ def galaxy_collision(n: int, total_mass: float = 1.0, mass_ratio: float = 1.0 / 
         out[k] = pos[:, a].copy()
         out["v" + k] = vel[:, a].copy()
     return out
+
+
+def _require_bound_orbit(primary_mass, secondary_mass, semi_major_axis, eccentricity):
+    # src/initial_conditions/kepler.cpp:24-39: comparisons written so that NaN fails.
+    if not (primary_mass > 0) or not (secondary_mass > 0):
+        raise ValueError("A Kepler orbit needs two positive masses")
+    if not (semi_major_axis > 0):
+        raise ValueError("A Kepler orbit needs a positive semi-major axis")
+    if not (eccentricity >= 0) or not (eccentricity < 1):
+        raise ValueError("A bound Kepler orbit needs an eccentricity in [0, 1)")
+
+
+def kepler_orbit(primary_mass: float = 1.0, secondary_mass: float = 1.0,
+                 semi_major_axis: float = 1.0, eccentricity: float = 0.0) -> dict:
+    """Two bodies on a bound Kepler orbit, at periapsis on the x axis and moving
+    along y, in the centre-of-mass frame: make_kepler_orbit
+    (src/initial_conditions/kepler.cpp:51-80), with the same operations in the
+    same order, so the state is the reference's bit for bit."""
+    _require_bound_orbit(primary_mass, secondary_mass, semi_major_axis, eccentricity)
+    total = primary_mass + secondary_mass
+    separation = semi_major_axis * (1 - eccentricity)           # kepler_periapsis_distance
+    speed = math.sqrt(total * (1 + eccentricity) / separation)  # vis-viva at periapsis, G = 1
+    primary_fraction = primary_mass / total
+    secondary_fraction = secondary_mass / total
+    return dict(x=np.array([-secondary_fraction * separation, primary_fraction * separation]),
+                y=np.zeros(2), z=np.zeros(2), vx=np.zeros(2),
+                vy=np.array([-secondary_fraction * speed, primary_fraction * speed]),
+                vz=np.zeros(2), m=np.array([float(primary_mass), float(secondary_mass)]))
+
+
+def kepler_period(primary_mass: float = 1.0, secondary_mass: float = 1.0,
+                  semi_major_axis: float = 1.0, eccentricity: float = 0.0) -> float:
+    """The orbital period 2 pi sqrt(a^3 / (G M)) (src/initial_conditions/kepler.cpp:82-88)."""
+    _require_bound_orbit(primary_mass, secondary_mass, semi_major_axis, eccentricity)
+    axis = semi_major_axis
+    return 2 * math.pi * math.sqrt(axis * axis * axis / (primary_mass + secondary_mass))

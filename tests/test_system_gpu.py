@@ -167,3 +167,74 @@ def test_yoshida_energy_error_below_velocity_verlet(b200):
         ke, pe = s.energy()
         errs[integ] = abs((ke + pe) - (ke0 + pe0)) / abs(ke0 + pe0)
     assert errs["yoshida4"] < errs["vv"]
+
+
+# -- the reference's integrator validation on Kepler orbits, on the device -----
+# (tests/integrators/convergence_test.cpp, energy_behaviour_test.cpp; the
+# figures are docs/validation.md's, which the oracle reproduces in
+# tests/test_integrator_validation.py).
+
+def _kepler_system(b200, orbit):
+    s = b200.DeviceSystem(2, 0.0, precision="fp64")
+    s.set_state(orbit["x"], orbit["y"], orbit["z"], orbit["vx"], orbit["vy"], orbit["vz"],
+                orbit["m"])
+    return s
+
+
+@pytest.mark.parametrize("integrator", ["vv", "yoshida4", "rk4"])
+def test_device_integrators_converge_at_the_published_orders(b200, integrator):
+    import math
+
+    from test_integrator_validation import COARSE, PUBLISHED_ORDERS, closure_order
+
+    from orrery_b200 import initial_conditions as ic
+
+    def closure(steps):
+        start = ic.kepler_orbit(1.0, 1.0, 1.0, 0.0)
+        s = _kepler_system(b200, start)
+        s.step(ic.kepler_period(1.0, 1.0, 1.0, 0.0) / steps, steps, integrator)
+        end = s.snapshot()
+        return max(math.dist((end["x"][i], end["y"][i], end["z"][i]),
+                             (start["x"][i], start["y"][i], start["z"][i])) for i in range(2))
+
+    assert f"{closure_order(closure, COARSE[integrator]):.4f}" == PUBLISHED_ORDERS[integrator]
+
+
+@pytest.mark.parametrize("integrator", ["vv", "yoshida4", "rk4"])
+def test_device_integrators_hold_the_published_energy_envelopes(b200, integrator):
+    from test_integrator_validation import STEPS_PER_ORBIT, check_envelope, envelope
+
+    from orrery_b200 import initial_conditions as ic
+
+    s = _kepler_system(b200, ic.kepler_orbit(1.0, 1.0, 1.0, 0.5))
+    dt = ic.kepler_period(1.0, 1.0, 1.0, 0.5) / STEPS_PER_ORBIT
+
+    def energy():
+        d = s.diagnostics()
+        return d["kinetic_energy"] + d["potential_energy"]
+
+    check_envelope(integrator, *envelope(lambda k: s.step(dt, k, integrator), energy))
+
+
+def test_the_device_orbit_takes_keplers_period(b200):
+    # convergence_test.cpp: Yoshida-4 at 2000 steps an orbit; the period read
+    # from the upward crossing of the separation's y component, within 1e-4
+    # of Kepler's third law.
+    from orrery_b200 import initial_conditions as ic
+
+    params = (2.0, 1.0, 1.5, 0.5)
+    expected = ic.kepler_period(*params)
+    s = _kepler_system(b200, ic.kepler_orbit(*params))
+    dt = expected / 2000
+    measured = 0.0
+    y = s.snapshot()["y"]
+    previous = y[1] - y[0]
+    for step in range(1, 4001):
+        s.step(dt, 1, "yoshida4")
+        y = s.snapshot()["y"]
+        current = y[1] - y[0]
+        if previous < 0 <= current:
+            measured = (step - 1 + (-previous / (current - previous))) * dt
+            break
+        previous = current
+    assert measured > 0 and abs(measured - expected) <= expected / 10000
