@@ -17,6 +17,7 @@ and fails with an error when the library or the device is missing.
 from __future__ import annotations
 
 import ctypes as C
+import operator
 import os
 from dataclasses import dataclass
 
@@ -235,8 +236,33 @@ def load_library():
     lib.ob_trajectory_flush.argtypes = [vp]
     lib.ob_trajectory_frames.argtypes = [vp, _u64p]
     lib.ob_trajectory_close.argtypes = [vp]
+    # Every unsigned 64-bit argument (counts, steps, step indices, job ids)
+    # refuses a value it cannot hold instead of wrapping it: -1 steps would
+    # otherwise become 2^64 - 1 of them.
+    for fn in list(vars(lib).values()):
+        if isinstance(fn, C._CFuncPtr) and fn.argtypes:
+            fn.argtypes = [_Unsigned64 if t is C.c_uint64 else t for t in fn.argtypes]
     _lib = lib
     return lib
+
+
+def _count(value, what: str = "count") -> int:
+    """An integer a uint64_t can hold: a count, a number of steps, a step index."""
+    v = operator.index(value)
+    if not 0 <= v < 1 << 64:
+        raise OrreryError(ERROR_INVALID_ARGUMENT, f"{what} must be in [0, 2^64), not {v}")
+    return v
+
+
+class _Unsigned64(C.c_uint64):
+    """A uint64_t argument that accepts only integers in [0, 2^64); ctypes
+    reports a refused one as an ArgumentError."""
+
+    @classmethod
+    def from_param(cls, value):
+        if isinstance(value, C.c_uint64):
+            return value
+        return C.c_uint64(_count(value))
 
 
 def _check(rc: int) -> None:
@@ -337,7 +363,8 @@ class _Solver:
         """Device-pointer form (integers or objects with ``data_ptr()``)."""
         ptrs = [p.data_ptr() if hasattr(p, "data_ptr") else int(p)
                 for p in (x, y, z, m, ax, ay, az)]
-        _check(self._lib.ob_solver_evaluate_device(self._handle, int(n), *ptrs, stream or None))
+        _check(self._lib.ob_solver_evaluate_device(self._handle, _count(n, "n"), *ptrs,
+                                                   stream or None))
 
     def interaction_count(self) -> InteractionCount:
         c = Counts()
@@ -355,13 +382,13 @@ class _Solver:
         else:
             t = tuple(shape)
             s = DirectShape(*(t + (1,) * (4 - len(t))))
-        _check(self._lib.ob_solver_set_direct_shape(self._handle, int(n), C.byref(s)))
+        _check(self._lib.ob_solver_set_direct_shape(self._handle, _count(n, "n"), C.byref(s)))
 
     def autotune(self, n: int):
         """Times every direct kernel shape for n particles; keeps and returns the best."""
         s = DirectShape()
         ms = C.c_double()
-        _check(self._lib.ob_solver_autotune(self._handle, int(n), C.byref(s), C.byref(ms)))
+        _check(self._lib.ob_solver_autotune(self._handle, _count(n, "n"), C.byref(s), C.byref(ms)))
         return (s.threads, s.targets_per_thread, s.split, s.groups), ms.value
 
     def timings(self) -> dict:
@@ -482,10 +509,10 @@ class DeviceSystem:
         handle = C.c_void_p()
         params = make_params(kind, precision, softening, opening_angle, leaf_capacity,
                              quadrupole)
-        _check(lib.ob_system_create(C.byref(params), int(n), C.byref(handle)))
+        _check(lib.ob_system_create(C.byref(params), _count(n, "n"), C.byref(handle)))
         self._lib = lib
         self._handle = handle
-        self.n = int(n)
+        self.n = _count(n, "n")
 
     def __del__(self):
         h = getattr(self, "_handle", None)
@@ -509,7 +536,7 @@ class DeviceSystem:
 
     def step(self, dt: float, steps: int = 1, integrator: str = "vv") -> None:
         _check(self._lib.ob_system_step(self._handle, _INTEGRATORS[integrator], float(dt),
-                                        int(steps)))
+                                        _count(steps, "steps")))
 
     def step_host(self, state: dict, dt: float, steps: int = 1, integrator: str = "vv") -> None:
         """Integrator::step over host arrays: state holds x y z vx vy vz ax ay az m
@@ -520,11 +547,12 @@ class DeviceSystem:
             if a.dtype != np.float64 or not a.flags.c_contiguous or len(a) != self.n:
                 raise OrreryError(ERROR_INVALID_ARGUMENT, f"{k} must be contiguous FP64 of n")
         _check(self._lib.ob_system_step_host(self._handle, _INTEGRATORS[integrator], float(dt),
-                                             int(steps), *(_ptr(state[k]) for k in keys)))
+                                             _count(steps, "steps"),
+                                             *(_ptr(state[k]) for k in keys)))
 
     def step_async(self, dt: float, steps: int = 1, integrator: str = "vv") -> None:
         _check(self._lib.ob_system_step_async(self._handle, _INTEGRATORS[integrator], float(dt),
-                                              int(steps)))
+                                              _count(steps, "steps")))
 
     def synchronize(self) -> None:
         _check(self._lib.ob_system_synchronize(self._handle))
@@ -534,8 +562,8 @@ class DeviceSystem:
         (sim::write_checkpoint); `configuration` is the reference's
         configuration text, stored as is."""
         text = configuration.encode()
-        _check(self._lib.ob_system_write_checkpoint(self._handle, os.fsencode(path), int(step),
-                                                    text, len(text)))
+        _check(self._lib.ob_system_write_checkpoint(self._handle, os.fsencode(path),
+                                                    _count(step, "step"), text, len(text)))
 
     def read_checkpoint(self, path):
         """Restores the state (carried accelerations included) from an ORRERYCK
@@ -596,7 +624,7 @@ class DeviceSystem:
 
     def profile(self, steps: int) -> None:
         """Record per-phase events for the next ``steps`` steps."""
-        _check(self._lib.ob_system_profile(self._handle, int(steps)))
+        _check(self._lib.ob_system_profile(self._handle, _count(steps, "steps")))
 
     def phase_times(self):
         """Per-evaluation average phase times (ms) over the profiled steps."""
@@ -676,11 +704,11 @@ class DeviceBatch:
 
     def step(self, dt: float, steps: int = 1, integrator: str = "yoshida4") -> None:
         _check(self._lib.ob_batch_step(self._handle, _INTEGRATORS[integrator], float(dt),
-                                       int(steps)))
+                                       _count(steps, "steps")))
 
     def step_async(self, dt: float, steps: int = 1, integrator: str = "yoshida4") -> None:
         _check(self._lib.ob_batch_step_async(self._handle, _INTEGRATORS[integrator], float(dt),
-                                             int(steps)))
+                                             _count(steps, "steps")))
 
     def synchronize(self) -> None:
         _check(self._lib.ob_batch_synchronize(self._handle))
@@ -751,7 +779,7 @@ class Server:
                leaf_capacity: int = 32, quadrupole: bool = True) -> int:
         n = len(state["m"])
         spec = JobSpec(SOLVER_DIRECT if kind == "direct" else SOLVER_TREE,
-                       _INTEGRATORS[integrator], n, int(steps), float(dt),
+                       _INTEGRATORS[integrator], n, _count(steps, "steps"), float(dt),
                        float(softening) * float(softening), float(opening_angle),
                        int(leaf_capacity), 1 if quadrupole else 0, 0)
         arrs = [_f64(state[k]) if state.get(k) is not None else None
@@ -799,7 +827,7 @@ def write_checkpoint(path, step: int, state: dict, configuration: str = "") -> N
         raise OrreryError(ERROR_INVALID_ARGUMENT, "every state array needs the same length")
     text = configuration.encode()
     lib = load_library()
-    _check(lib.ob_checkpoint_write(os.fsencode(path), int(step), text, len(text), n,
+    _check(lib.ob_checkpoint_write(os.fsencode(path), _count(step, "step"), text, len(text), n,
                                    *(_ptr(a) for a in arrs)))
 
 
@@ -856,12 +884,12 @@ class Trajectory:
         """A frame from host arrays (x y z, and vx vy vz when the file carries
         them), or, with no `state`, a snapshot of the bound system."""
         if state is None:
-            _check(self._lib.ob_trajectory_write_system_frame(self._handle, int(step),
+            _check(self._lib.ob_trajectory_write_system_frame(self._handle, _count(step, "step"),
                                                               float(time)))
             return
         keys = ("x", "y", "z", "vx", "vy", "vz") if self.with_velocities else ("x", "y", "z")
         arrs = [_f64(state[k]) for k in keys] + [None] * (6 - len(keys))
-        _check(self._lib.ob_trajectory_write_frame(self._handle, int(step), float(time),
+        _check(self._lib.ob_trajectory_write_frame(self._handle, _count(step, "step"), float(time),
                                                    *(_ptr(a) for a in arrs)))
 
     def flush(self) -> None:
@@ -897,7 +925,7 @@ def work_units(count: int, steps: int, solver: str) -> float:
     as the server's admission counts it: count^2 * steps for "direct",
     count * log2(count) * steps for the tree ("barnes-hut" or "tree")."""
     kind = SOLVER_DIRECT if solver == "direct" else SOLVER_TREE
-    return load_library().ob_work_units(int(count), int(steps), kind)
+    return load_library().ob_work_units(_count(count, "count"), _count(steps, "steps"), kind)
 
 
 _PARTICLE_ARRAYS = ("position_x", "position_y", "position_z", "mass",

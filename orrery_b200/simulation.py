@@ -19,7 +19,7 @@ import numpy as np
 
 from . import (DeviceSystem, OrreryError, Trajectory, SOLVER_DIRECT, SOLVER_TREE,
                ERROR_INVALID_ARGUMENT, INTEGRATOR_RK4, INTEGRATOR_VV, INTEGRATOR_YOSHIDA4,
-               _INTEGRATORS, _check, _f64, _ptr, load_library)
+               _INTEGRATORS, _check, _count, _f64, _ptr, load_library)
 
 _STATE = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
 
@@ -248,7 +248,7 @@ class Simulation:
     def run(self, steps: int) -> None:
         """Advance by `steps` steps, recording through the output (if any) at
         the start, wherever a stride falls and at the last step."""
-        steps = int(steps)
+        steps = _count(steps, "steps")
         out = self.output
         if out is None:
             self.system.step(self.timestep, steps, self._integrator)
@@ -297,7 +297,7 @@ class Simulation:
                                          *(_ptr(acc[k]) for k in ("ax", "ay", "az"))))
         else:
             self.system.set_state(*(arrs[k] for k in keys))
-        self._step = int(step)
+        self._step = _count(step, "step")
 
     def measure(self) -> dict:
         """core::measure_diagnostics of the current state: kinetic, potential

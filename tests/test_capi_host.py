@@ -70,6 +70,28 @@ def test_null_handles_are_errors_not_crashes(lib):
     lib.ob_system_destroy(None)
 
 
+def test_negative_counts_are_refused_not_wrapped(lib):
+    # A uint64_t cannot hold -1; passed through, it would become 2^64 - 1
+    # steps. The binding's argument type refuses it (ctypes reports that as an
+    # ArgumentError), and the Python surface refuses it first with an
+    # invalid-argument error, before anything reaches the library.
+    with pytest.raises(C.ArgumentError):
+        lib.ob_system_step(None, 0, 1e-3, -1)
+    with pytest.raises(C.ArgumentError):
+        lib.ob_system_step(None, 0, 1e-3, 1 << 64)
+    assert lib.ob_system_step(None, 0, 1e-3, np.uint64(3)) == ob.ERROR_INVALID_ARGUMENT
+    system = ob.DeviceSystem.__new__(ob.DeviceSystem)  # no device: refused before the call
+    system._lib, system._handle = lib, None
+    for call in (lambda: system.step(1e-3, -1), lambda: system.step_async(1e-3, -2),
+                 lambda: system.write_checkpoint("never.ck", -1),
+                 lambda: ob.work_units(1000, -1, "direct")):
+        with pytest.raises(ob.OrreryError, match="must be in") as e:
+            call()
+        assert e.value.code == ob.ERROR_INVALID_ARGUMENT
+    with pytest.raises(TypeError):
+        ob.work_units(1000, 2.5, "direct")  # a count is an integer, as the reference's Index is
+
+
 def test_try_create_without_a_device_returns_none(lib):
     if ob.device_count() > 0:
         pytest.skip("a device is present; the no-device contract is tested without one")

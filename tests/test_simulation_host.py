@@ -98,6 +98,15 @@ def test_next_due_takes_the_nearest_stride():
     assert FileOutput(diagnostics_path="d", diagnostics_stride=3).next_due(3, 50) == 6
 
 
+def test_a_negative_run_is_refused_before_anything_is_enqueued():
+    import pytest
+
+    sim = stub_simulation(Recorder(checkpoint_path="c", checkpoint_stride=2))
+    with pytest.raises(ob.OrreryError, match="must be in"):
+        sim.run(-3)
+    assert sim.system.enqueued == [] and sim.output.points == [] and sim.step_index == 0
+
+
 def test_a_run_without_output_is_one_enqueue():
     sim = stub_simulation(None)
     sim.run(17)
