@@ -238,3 +238,32 @@ def test_the_device_orbit_takes_keplers_period(b200):
             break
         previous = current
     assert measured > 0 and abs(measured - expected) <= expected / 10000
+
+
+@pytest.mark.parametrize("integrator", ["vv", "yoshida4", "rk4"])
+def test_device_integrators_conserve_momenta_as_the_reference_requires(b200, reference,
+                                                                        integrator):
+    # conservation_test.cpp: 64 particles of the reference's Plummer sampler
+    # (seed 20260810), softening 0.03, 200 steps of 0.001. Linear momentum
+    # holds to round-off for every method; angular momentum to round-off for
+    # the symmetric ones and to 1e-3 of itself for RK4.
+    eps = float(np.finfo(np.float64).eps)
+
+    def drift(a, b):
+        return float(np.linalg.norm(np.asarray(b) - np.asarray(a)))
+
+    d = reference.plummer(64, seed=20260810)
+    s = b200.DeviceSystem(64, 0.03, precision="fp64")
+    s.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+    before = s.diagnostics()
+    s.step(0.001, 200, integrator)
+    after = s.diagnostics()
+    bound = 64 * 200 * eps  # round_off_bound, times each quantity's scale
+    linear_scale = np.sqrt(2 * before["kinetic_energy"])
+    assert drift(before["linear_momentum"], after["linear_momentum"]) <= bound * linear_scale
+    angular_scale = float(np.linalg.norm(before["angular_momentum"]))
+    angular = drift(before["angular_momentum"], after["angular_momentum"])
+    if integrator == "rk4":
+        assert angular <= angular_scale / 1000
+    else:
+        assert angular <= bound * angular_scale
