@@ -267,3 +267,39 @@ def test_device_integrators_conserve_momenta_as_the_reference_requires(b200, ref
         assert angular <= angular_scale / 1000
     else:
         assert angular <= bound * angular_scale
+
+
+@pytest.mark.parametrize("integrator", ["vv", "yoshida4", "rk4"])
+def test_a_step_leaves_the_accelerations_agreeing_with_the_positions(b200, integrator):
+    # integrator_test.cpp: after two steps of 0.01 on a Kepler orbit (masses 2
+    # and 1, a = 1, e = 0.3) the carried accelerations are exactly those a
+    # fresh evaluation of the positions gives.
+    from orrery_b200 import initial_conditions as ic
+
+    orbit = ic.kepler_orbit(2.0, 1.0, 1.0, 0.3)
+    s = _kepler_system(b200, orbit)
+    s.step(0.01, 2, integrator)
+    st = s.state()
+    fresh = b200.B200DirectSolver(0.0, "fp64").evaluate((st["x"], st["y"], st["z"]), orbit["m"])
+    assert np.array_equal(np.stack([st["ax"], st["ay"], st["az"]], axis=1), fresh)
+
+
+@pytest.mark.parametrize("integrator", ["vv", "yoshida4"])
+def test_the_symmetric_methods_run_backwards_to_where_they_started(b200, integrator):
+    # integrator_test.cpp: 200 steps of 0.002 and 200 of -0.002 on a Kepler
+    # orbit (masses 3 and 1, a = 1, e = 0.4, softening 0.01) return positions
+    # and velocities to within 64 * 200 machine epsilons.
+    from orrery_b200 import initial_conditions as ic
+
+    start = ic.kepler_orbit(3.0, 1.0, 1.0, 0.4)
+    s = b200.DeviceSystem(2, 0.01, precision="fp64")
+    s.set_state(start["x"], start["y"], start["z"], start["vx"], start["vy"], start["vz"],
+                start["m"])
+    s.step(0.002, 200, integrator)
+    s.step(-0.002, 200, integrator)
+    end = s.state()
+    tolerance = 64 * 200 * float(np.finfo(np.float64).eps)
+    for i in range(2):
+        for keys in (("x", "y", "z"), ("vx", "vy", "vz")):
+            error = np.linalg.norm([end[k][i] - start[k][i] for k in keys])
+            assert error <= tolerance, (i, keys, error)
