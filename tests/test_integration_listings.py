@@ -28,6 +28,35 @@ def test_there_are_listings():
     assert len(listings()) >= 3
 
 
+def python_listings():
+    with open(os.path.join(ROOT, "INTEGRATION.md")) as fh:
+        return re.findall(r"```python\n(.*?)```", fh.read(), re.S)
+
+
+@pytest.mark.parametrize("index", range(len(python_listings())))
+def test_python_listing_parses_and_calls_what_the_package_has(index):
+    # Each `ob.<name>(...)` call names something the package exports and
+    # passes only keywords its signature accepts.
+    import ast
+    import inspect
+
+    import orrery_b200 as ob
+
+    tree = ast.parse(python_listings()[index])
+    for node in ast.walk(tree):
+        if not (isinstance(node, ast.Call) and isinstance(node.func, ast.Attribute) and
+                isinstance(node.func.value, ast.Name) and node.func.value.id == "ob"):
+            continue
+        target = getattr(ob, node.func.attr, None)
+        assert target is not None, f"ob.{node.func.attr} does not exist"
+        params = inspect.signature(target).parameters
+        if any(p.kind is p.VAR_KEYWORD for p in params.values()):
+            continue
+        for kw in node.keywords:
+            if kw.arg is not None:
+                assert kw.arg in params, f"ob.{node.func.attr} takes no {kw.arg}="
+
+
 @pytest.mark.parametrize("index", range(len(listings())))
 def test_listing_compiles_against_the_reference(tmp_path, index):
     if shutil.which("g++") is None or not os.path.isdir(REFERENCE_INCLUDE):
