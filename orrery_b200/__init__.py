@@ -111,7 +111,9 @@ class ServerSummary(C.Structure):
                 ("hbm_peak", C.c_uint64)]
 
 
-class Diagnostics(C.Structure):
+class DiagnosticsRecord(C.Structure):
+    """ob_diagnostics, as the C ABI fills it."""
+
     _fields_ = [("kinetic_energy", C.c_double), ("potential_energy", C.c_double),
                 ("linear_momentum", C.c_double * 3), ("angular_momentum", C.c_double * 3)]
 
@@ -182,7 +184,7 @@ def load_library():
     lib.ob_probe_fp32.argtypes = [_dp, _dp]
     lib.ob_probe_fp32x2.argtypes = [_dp]
     lib.ob_probe_fp64.argtypes = [_dp]
-    lib.ob_system_diagnostics.argtypes = [vp, C.POINTER(Diagnostics)]
+    lib.ob_system_diagnostics.argtypes = [vp, C.POINTER(DiagnosticsRecord)]
     lib.ob_system_device_arrays.argtypes = [vp, C.POINTER(vp)]
     lib.ob_system_snapshot.argtypes = [vp] + [_dp] * 10
     lib.ob_system_restore.argtypes = [vp] + [_dp] * 10
@@ -586,7 +588,7 @@ class DeviceSystem:
     def diagnostics(self) -> dict:
         """core::measure_diagnostics of the state: kinetic_energy,
         potential_energy, linear_momentum (3), angular_momentum (3)."""
-        d = Diagnostics()
+        d = DiagnosticsRecord()
         _check(self._lib.ob_system_diagnostics(self._handle, C.byref(d)))
         return {"kinetic_energy": d.kinetic_energy, "potential_energy": d.potential_energy,
                 "linear_momentum": np.array(d.linear_momentum[:]),
@@ -980,5 +982,5 @@ def compute_accelerations(positions, masses, softening: float = 0.0, solver: str
     return s.evaluate(positions, masses)
 
 
-from .simulation import (DeviceArrayView, DiagnosticsLog, FileOutput, Simulation,  # noqa: E402,F401
-                         device_arrays)
+from .simulation import (DeviceArrayView, Diagnostics, DiagnosticsLog, FileOutput,  # noqa: E402,F401
+                         Simulation, Vec3, device_arrays)

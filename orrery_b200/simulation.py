@@ -12,6 +12,7 @@ of it (``__cuda_array_interface__``, readable by torch, CuPy or Numba).
 """
 from __future__ import annotations
 
+import collections
 import ctypes as C
 import math
 
@@ -74,6 +75,28 @@ def _virial_ratio(kinetic: float, potential: float) -> float:
     with np.errstate(divide="ignore", invalid="ignore"):
         return float(np.float64(2 * kinetic) /
                      np.float64(-potential if potential < 0 else potential))
+
+
+Vec3 = collections.namedtuple("Vec3", "x y z")
+Vec3.__doc__ = """A momentum as the reference's Python Vec3 gives it: x, y, z by name,
+a sequence of three (unpacking, tuple(), numpy.asarray())."""
+
+
+class Diagnostics(dict):
+    """core::Diagnostics as the reference's Python binding exposes it
+    (python/src/core_bindings.cpp:139-158): kinetic_energy, potential_energy,
+    linear_momentum and angular_momentum, and the derived total_energy and
+    virial_ratio, read as attributes; the same values by key."""
+
+    def __getattr__(self, name):
+        try:
+            return self[name]
+        except KeyError:
+            raise AttributeError(name) from None
+
+    def __repr__(self):
+        return ("Diagnostics(" + ", ".join(f"{k}={_real(self[k])}" for k in (
+            "kinetic_energy", "potential_energy", "total_energy", "virial_ratio")) + ")")
 
 
 class DiagnosticsLog:
@@ -299,13 +322,16 @@ class Simulation:
             self.system.set_state(*(arrs[k] for k in keys))
         self._step = _count(step, "step")
 
-    def measure(self) -> dict:
+    def measure(self) -> "Diagnostics":
         """core::measure_diagnostics of the current state: kinetic, potential
         and total energy, linear and angular momentum, virial ratio."""
         d = self.system.diagnostics()
-        d["total_energy"] = d["kinetic_energy"] + d["potential_energy"]
-        d["virial_ratio"] = _virial_ratio(d["kinetic_energy"], d["potential_energy"])
-        return d
+        kinetic, potential = float(d["kinetic_energy"]), float(d["potential_energy"])
+        return Diagnostics(kinetic_energy=kinetic, potential_energy=potential,
+                           linear_momentum=Vec3(*(float(v) for v in d["linear_momentum"])),
+                           angular_momentum=Vec3(*(float(v) for v in d["angular_momentum"])),
+                           total_energy=kinetic + potential,
+                           virial_ratio=_virial_ratio(kinetic, potential))
 
     @property
     def interaction_count(self):

@@ -122,13 +122,35 @@ def test_virial_ratio_follows_the_reference_division():
     for kinetic, potential, expected in ((0.25, -0.5, 1.0), (0.5, 0.0, math.inf),
                                          (0.0, 0.0, math.nan), (0.125, 0.5, 0.5)):
         sim.system.diagnostics = lambda k=kinetic, p=potential: {
-            "kinetic_energy": k, "potential_energy": p}
+            "kinetic_energy": k, "potential_energy": p, "linear_momentum": [0.0] * 3,
+            "angular_momentum": [0.0] * 3}
         d = sim.measure()
         assert d["total_energy"] == kinetic + potential
         if math.isnan(expected):
             assert math.isnan(d["virial_ratio"])
         else:
             assert d["virial_ratio"] == expected
+
+
+def test_measure_reads_as_the_references_diagnostics():
+    # core::Diagnostics through the reference's binding
+    # (python/src/core_bindings.cpp:139-158): attributes, derived properties,
+    # momenta as (x, y, z) vectors; the same values by key.
+    import numpy as np
+
+    d = stub_simulation(None).measure()
+    assert isinstance(d, ob.Diagnostics)
+    assert (d.kinetic_energy, d.potential_energy) == (0.25, -0.5)
+    assert d.total_energy == -0.25 and d.virial_ratio == 1.0
+    x, y, z = d.angular_momentum
+    assert (x, y, z) == (0.0, 0.0, 1.0) and d.angular_momentum.z == 1.0
+    assert np.array_equal(np.asarray(d.linear_momentum), np.zeros(3))
+    assert d["total_energy"] == d.total_energy
+    assert repr(d) == ("Diagnostics(kinetic_energy=0.25, potential_energy=-0.5, "
+                       "total_energy=-0.25, virial_ratio=1)")
+    import pytest
+    with pytest.raises(AttributeError):
+        d.energy
 
 
 def test_integrator_names_are_the_reference_integrators_names():
