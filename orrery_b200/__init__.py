@@ -983,4 +983,4 @@ def compute_accelerations(positions, masses, softening: float = 0.0, solver: str
 
 
 from .simulation import (DeviceArrayView, Diagnostics, DiagnosticsLog, FileOutput,  # noqa: E402,F401
-                         Simulation, Vec3, device_arrays)
+                         Particles, Simulation, Vec3, device_arrays)

@@ -99,6 +99,40 @@ class Diagnostics(dict):
             "kinetic_energy", "potential_energy", "total_energy", "virial_ratio")) + ")")
 
 
+# The reference's ParticleData names (python/src/core_bindings.cpp:253-300) and
+# the keys this package uses for the same arrays.
+_PARTICLE_NAMES = {"position_x": "x", "position_y": "y", "position_z": "z",
+                   "velocity_x": "vx", "velocity_y": "vy", "velocity_z": "vz",
+                   "acceleration_x": "ax", "acceleration_y": "ay", "acceleration_z": "az",
+                   "mass": "m"}
+
+
+class Particles(dict):
+    """A host copy of a simulation's state: arrays by key (x y z vx vy vz ax
+    ay az m), or by the names of the reference's ParticleData (position_x ...
+    acceleration_z, mass, and size)."""
+
+    def __getattr__(self, name):
+        key = _PARTICLE_NAMES.get(name)
+        if key is not None:
+            return self[key]
+        if name == "size":
+            return len(self["m"])
+        raise AttributeError(name)
+
+
+def _state_of(state) -> dict:
+    """A state given as a dict keyed x ... m, or as the reference's
+    ParticleData (anything with position_x ... mass), as a dict keyed x ... m."""
+    if hasattr(state, "keys") and "m" in state:
+        return state
+    if all(hasattr(state, name) for name in _PARTICLE_NAMES if not name.startswith("acc")):
+        return {key: getattr(state, name) for name, key in _PARTICLE_NAMES.items()
+                if hasattr(state, name)}
+    raise OrreryError(ERROR_INVALID_ARGUMENT,
+                      "a state is a dict of x y z vx vy vz m or a ParticleData")
+
+
 class DiagnosticsLog:
     """sim::DiagnosticsLog (src/sim/diagnostics_log.cpp): a CSV of the
     conserved quantities, one row per measurement, every number at full
@@ -232,6 +266,7 @@ class Simulation:
             raise OrreryError(ERROR_INVALID_ARGUMENT, f"unknown solver {solver!r}")
         if integrator not in _INTEGRATORS:
             raise OrreryError(ERROR_INVALID_ARGUMENT, f"unknown integrator {integrator!r}")
+        state = _state_of(state)
         arrs = {k: _f64(state[k]) for k in ("x", "y", "z", "vx", "vy", "vz", "m")}
         self.n = len(arrs["m"])
         self._solver = (softening, kind, precision, opening_angle, leaf_capacity, quadrupole)
@@ -289,9 +324,10 @@ class Simulation:
     # -- state --------------------------------------------------------------
 
     @property
-    def particles(self) -> dict:
-        """A host copy of the state: x y z vx vy vz ax ay az and m."""
-        return self.system.snapshot()
+    def particles(self) -> "Particles":
+        """A host copy of the state, read by key (x y z vx vy vz ax ay az m) or
+        by the reference's names (position_x ... acceleration_z, mass)."""
+        return Particles(self.system.snapshot())
 
     def device_particles(self) -> dict:
         """Zero-copy views of the device state (see DeviceArrayView)."""
@@ -305,6 +341,7 @@ class Simulation:
         (python/src/sim_bindings.cpp:293-309): the state then moves to a new
         device system of that size, with the same solver settings."""
         keys = ("x", "y", "z", "vx", "vy", "vz", "m")
+        state = _state_of(state)
         arrs = {k: _f64(state[k]) for k in keys}
         n = len(arrs["m"])
         if any(len(a) != n for a in arrs.values()):

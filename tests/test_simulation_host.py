@@ -24,6 +24,13 @@ class StubSystem:
     def write_checkpoint(self, path, step, configuration=""):
         self.last_checkpoint = (path, step, configuration)
 
+    def set_state(self, *arrays):
+        self.state = arrays
+
+    def snapshot(self):
+        keys = ("m", "x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+        return {k: [float(i)] * 2 for i, k in enumerate(keys)}
+
     def diagnostics(self):
         return {"kinetic_energy": 0.25, "potential_energy": -0.5,
                 "linear_momentum": [0.0, 0.0, 0.0], "angular_momentum": [0.0, 0.0, 1.0]}
@@ -151,6 +158,33 @@ def test_measure_reads_as_the_references_diagnostics():
     import pytest
     with pytest.raises(AttributeError):
         d.energy
+
+
+def test_particles_read_by_the_references_names():
+    p = stub_simulation(None).particles
+    assert isinstance(p, ob.Particles)
+    assert p.mass == p["m"] == [0.0, 0.0] and p.position_y == p["y"] == [2.0, 2.0]
+    assert p.acceleration_z == p["az"] and p.velocity_x == p["vx"] and p.size == 2
+
+
+def test_restore_takes_the_references_particle_data():
+    # ParticleData (python/src/core_bindings.cpp:241-300) as the reference's
+    # restore takes it; a dict keyed x ... m as before.
+    from types import SimpleNamespace
+
+    import numpy as np
+
+    sim = stub_simulation(None)
+    sim.n = 2
+    names = ("position_x", "position_y", "position_z", "velocity_x", "velocity_y",
+             "velocity_z", "mass")
+    data = SimpleNamespace(**{k: np.full(2, float(i)) for i, k in enumerate(names)})
+    sim.restore(data, step=5)
+    assert [a[0] for a in sim.system.state] == [0.0, 1.0, 2.0, 3.0, 4.0, 5.0, 6.0]
+    assert sim.step_index == 5
+    import pytest
+    with pytest.raises(ob.OrreryError):
+        sim.restore(SimpleNamespace(position_x=[1.0]))
 
 
 def test_integrator_names_are_the_reference_integrators_names():
