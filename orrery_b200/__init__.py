@@ -483,6 +483,26 @@ def direct_shapes(precision: str = "fp32"):
     return [(s.threads, s.targets_per_thread, s.split, s.groups) for s in arr]
 
 
+# The reference's ParticleData names (python/src/core_bindings.cpp:253-300) and
+# the keys this package uses for the same arrays.
+_PARTICLE_NAMES = {"position_x": "x", "position_y": "y", "position_z": "z",
+                   "velocity_x": "vx", "velocity_y": "vy", "velocity_z": "vz",
+                   "acceleration_x": "ax", "acceleration_y": "ay", "acceleration_z": "az",
+                   "mass": "m"}
+
+
+def _state_of(state) -> dict:
+    """A state given as a dict keyed x ... m, or as the reference's
+    ParticleData (anything with position_x ... mass), as a dict keyed x ... m."""
+    if hasattr(state, "keys") and "m" in state:
+        return state
+    if all(hasattr(state, name) for name in _PARTICLE_NAMES if not name.startswith("acc")):
+        return {key: getattr(state, name) for name, key in _PARTICLE_NAMES.items()
+                if hasattr(state, name)}
+    raise OrreryError(ERROR_INVALID_ARGUMENT,
+                      "a state is a dict of x y z vx vy vz m or a ParticleData")
+
+
 def _split_xyz(positions):
     if isinstance(positions, (tuple, list)) and len(positions) == 3 and \
             all(np.ndim(a) == 1 for a in positions):
@@ -779,6 +799,7 @@ class Server:
     def submit(self, state: dict, steps: int, dt: float, softening: float, kind: str = "direct",
                integrator: str = "yoshida4", opening_angle: float = 0.5,
                leaf_capacity: int = 32, quadrupole: bool = True) -> int:
+        state = _state_of(state)
         n = len(state["m"])
         spec = JobSpec(SOLVER_DIRECT if kind == "direct" else SOLVER_TREE,
                        _INTEGRATORS[integrator], n, _count(steps, "steps"), float(dt),

@@ -20,7 +20,8 @@ import numpy as np
 
 from . import (DeviceSystem, OrreryError, Trajectory, SOLVER_DIRECT, SOLVER_TREE,
                ERROR_INVALID_ARGUMENT, INTEGRATOR_RK4, INTEGRATOR_VV, INTEGRATOR_YOSHIDA4,
-               _INTEGRATORS, _check, _count, _f64, _ptr, load_library)
+               _INTEGRATORS, _PARTICLE_NAMES, _check, _count, _f64, _ptr, _state_of,
+               load_library)
 
 _STATE = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az", "m")
 
@@ -99,14 +100,6 @@ class Diagnostics(dict):
             "kinetic_energy", "potential_energy", "total_energy", "virial_ratio")) + ")")
 
 
-# The reference's ParticleData names (python/src/core_bindings.cpp:253-300) and
-# the keys this package uses for the same arrays.
-_PARTICLE_NAMES = {"position_x": "x", "position_y": "y", "position_z": "z",
-                   "velocity_x": "vx", "velocity_y": "vy", "velocity_z": "vz",
-                   "acceleration_x": "ax", "acceleration_y": "ay", "acceleration_z": "az",
-                   "mass": "m"}
-
-
 class Particles(dict):
     """A host copy of a simulation's state: arrays by key (x y z vx vy vz ax
     ay az m), or by the names of the reference's ParticleData (position_x ...
@@ -119,18 +112,6 @@ class Particles(dict):
         if name == "size":
             return len(self["m"])
         raise AttributeError(name)
-
-
-def _state_of(state) -> dict:
-    """A state given as a dict keyed x ... m, or as the reference's
-    ParticleData (anything with position_x ... mass), as a dict keyed x ... m."""
-    if hasattr(state, "keys") and "m" in state:
-        return state
-    if all(hasattr(state, name) for name in _PARTICLE_NAMES if not name.startswith("acc")):
-        return {key: getattr(state, name) for name, key in _PARTICLE_NAMES.items()
-                if hasattr(state, name)}
-    raise OrreryError(ERROR_INVALID_ARGUMENT,
-                      "a state is a dict of x y z vx vy vz m or a ParticleData")
 
 
 class DiagnosticsLog:

@@ -40,6 +40,21 @@ def test_jobs_complete_and_return_their_state(server):
     assert st["step_latency_p50_ms"] > 0
 
 
+def test_a_job_is_submitted_as_the_references_particle_data(server):
+    # The reference's make_initial_conditions gives a ParticleData
+    # (position_x ... mass); it is submitted as it is.
+    from types import SimpleNamespace
+
+    st = _state(800, 3)
+    data = SimpleNamespace(position_x=st["x"], position_y=st["y"], position_z=st["z"],
+                           velocity_x=st["vx"], velocity_y=st["vy"], velocity_z=st["vz"],
+                           mass=st["m"])
+    report, final = server.wait(server.submit(data, steps=4, dt=1e-3, softening=0.01),
+                                timeout=30)
+    assert report["status"] == ob.JOB_DONE and report["steps_done"] == 4
+    assert np.array_equal(final["y"], st["y"])  # fake mode returns the input
+
+
 def test_direct_jobs_share_batched_steps(server):
     # Eight direct jobs submitted together step together: all finish after
     # about the time of their 10 shared steps, not 8 x 10 separate ones.
