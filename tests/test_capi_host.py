@@ -122,3 +122,20 @@ def test_collision_generator_geometry():
     assert np.allclose(g["m"], g["m"][0])
     b = ic.collision_impact_parameter(1.0, 20.0, 0.8, 3.0)
     assert 0 < b < 20
+
+
+def test_positions_are_accepted_in_every_documented_layout():
+    # ForceSolver::evaluate takes three spans; the Python surface accepts
+    # three arrays, (N, 3) or (3, N), and refuses anything else.
+    rng = np.random.default_rng(3)
+    xyz = [rng.normal(size=5) for _ in range(3)]
+    for positions in (tuple(xyz), list(xyz), np.stack(xyz, axis=1), np.stack(xyz, axis=0)):
+        got = ob._split_xyz(positions)
+        assert all(np.array_equal(g, w) for g, w in zip(got, xyz))
+        assert all(g.dtype == np.float64 and g.flags.c_contiguous for g in got)
+    square = rng.normal(size=(3, 3))  # ambiguous: read as (N, 3), rows are particles
+    assert all(np.array_equal(g, square[:, k]) for k, g in enumerate(ob._split_xyz(square)))
+    with pytest.raises(ValueError):
+        ob._split_xyz(np.zeros((4, 4)))
+    with pytest.raises(ValueError):
+        ob._split_xyz(np.zeros(6))
