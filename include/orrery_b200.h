@@ -483,13 +483,16 @@ int ob_server_submit(ob_server *server, const ob_job_spec *spec, const double *x
                      const double *y, const double *z, const double *vx, const double *vy,
                      const double *vz, const double *m, uint64_t *job_id);
 /* Waits up to timeout_s for the job to end (OB_ERROR_TIMEOUT otherwise), then
- * fills the report and any non-NULL output arrays (n each). */
+ * fills the report and any non-NULL output arrays (n each). A timeout that is
+ * negative or NaN waits not at all; one above 1e9 s (infinity included) waits
+ * 1e9 s. */
 int ob_server_wait(ob_server *server, uint64_t job_id, double timeout_s, ob_job_report *report,
                    double *x, double *y, double *z, double *vx, double *vy, double *vz,
                    double *ax, double *ay, double *az);
 int ob_server_cancel(ob_server *server, uint64_t job_id);
 int ob_server_stats(ob_server *server, ob_server_summary *stats);
-/* Waits until no job is queued or running (OB_ERROR_TIMEOUT otherwise). */
+/* Waits until no job is queued or running (OB_ERROR_TIMEOUT otherwise); the
+ * timeout as for ob_server_wait. */
 int ob_server_drain(ob_server *server, double timeout_s);
 
 /* Measured FP32 FFMA and SFU rsqrt lane operations per second on the current

@@ -41,6 +41,15 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// The moment `seconds` from now. The wait is clamped to [0, 1e9 s] so that the
+// conversion to the clock's integer ticks cannot overflow: a negative or NaN
+// timeout waits not at all, an infinite one about 31 years.
+Clock::time_point deadline_after(double seconds) {
+    const double clamped = std::min(std::max(0.0, seconds), 1e9);
+    return Clock::now() +
+           std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(clamped));
+}
+
 double percentile(std::vector<double> v, double q) {
     if (v.empty()) {
         return 0.0;
@@ -165,9 +174,7 @@ public:
             throw Error(OB_ERROR_INVALID_ARGUMENT, "no such job");
         }
         Job *job = it->second.get();
-        const auto deadline =
-            Clock::now() + std::chrono::duration_cast<Clock::duration>(
-                               std::chrono::duration<double>(std::max(0.0, timeout_s)));
+        const auto deadline = deadline_after(timeout_s);
         while (job->status == OB_JOB_QUEUED || job->status == OB_JOB_RUNNING) {
             if (cv_.wait_until(lock, deadline) == std::cv_status::timeout &&
                 (job->status == OB_JOB_QUEUED || job->status == OB_JOB_RUNNING)) {
@@ -201,9 +208,7 @@ public:
 
     void drain(double timeout_s) {
         std::unique_lock<std::mutex> lock(mutex_);
-        const auto deadline =
-            Clock::now() + std::chrono::duration_cast<Clock::duration>(
-                               std::chrono::duration<double>(std::max(0.0, timeout_s)));
+        const auto deadline = deadline_after(timeout_s);
         while (!idle_locked()) {
             if (cv_.wait_until(lock, deadline) == std::cv_status::timeout && !idle_locked()) {
                 throw Error(OB_ERROR_TIMEOUT, "the server did not drain in time");

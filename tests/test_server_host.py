@@ -202,3 +202,21 @@ def test_wait_times_out_while_a_job_runs():
         s.wait(j, timeout=30, outputs=False)
     finally:
         s.close()
+
+
+def test_any_timeout_is_a_deadline_the_clock_can_hold():
+    # An infinite wait must not overflow the deadline's conversion to clock
+    # ticks; NaN or a negative timeout waits not at all.
+    s = ob.Server(hbm_budget_bytes=1 << 34, direct_pairs_cap=10**9, max_tree_jobs=1, fake=True,
+                  fake_direct_gint_s=100.0, fake_tree_ns_per_particle=50.0)
+    try:
+        slow = s.submit(_state(3000, 5), steps=2000, dt=1e-3, softening=0.01)  # ~0.2 s modelled
+        for timeout in (float("nan"), -1.0):
+            with pytest.raises(ob.OrreryError) as e:
+                s.wait(slow, timeout=timeout)
+            assert e.value.code == ob.ERROR_TIMEOUT
+        report, _ = s.wait(slow, timeout=float("inf"))
+        assert report["status"] == ob.JOB_DONE and report["steps_done"] == 2000
+        s.drain(timeout=float("inf"))
+    finally:
+        s.close()
