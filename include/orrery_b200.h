@@ -149,18 +149,25 @@ int ob_tree_copy_order(ob_solver *solver, uint64_t *codes, uint32_t *indices, do
  * particles whose FP64 positions are in device memory, written to the
  * caller's device arrays codes[n] and indices[n], enqueued on `stream`
  * without synchronising. It allocates nothing: for callers that cannot
- * allocate device memory when they need an ordering -- code running in a
- * stream or host callback, where calls that may synchronise are forbidden,
- * and services that take device memory only from their own fixed pool.
+ * allocate device memory when they need an ordering -- services that take
+ * device memory only from their own fixed pool, or that must not grow or
+ * fragment the device heap once running. (Like every entry point here it
+ * makes CUDA calls, so it must not be called from a stream or host callback.)
  * Every intermediate buffer lives in one fixed device array of about 14 MB
  * that each device holds from the library's loading until the process exits;
  * n above 1,048,576 is refused with OB_ERROR_CAPACITY. The first call on a
  * device looks up that array's device address, so make it before any stream
  * capture. All calls share the one array: calls whose work overlaps on the
- * GPU race and must be ordered by the caller. No counterpart in the
- * reference (its MortonOrdering allocates on the host). */
+ * GPU race and must be ordered by the caller.
+ * status: a device word (or NULL) that receives, on the stream after the
+ * ordering, 0 when it completed or a nonzero value when a bounded device wait
+ * ran out (OB_DEVICE_STATUS_TIMEOUT): the outputs are then incomplete and
+ * must not be used. With NULL such a failure cannot be detected.
+ * No counterpart in the reference (its MortonOrdering allocates on the host). */
+#define OB_DEVICE_STATUS_TIMEOUT 1u
 int ob_morton_order_noalloc(uint64_t n, const double *x, const double *y, const double *z,
-                            uint64_t *codes, uint32_t *indices, void *stream);
+                            uint64_t *codes, uint32_t *indices, uint32_t *status,
+                            void *stream);
 
 /* Tile shape of the direct kernels: threads per CTA, targets per thread, the
  * number of CTAs (one thread-block cluster) that split the sources of a

@@ -26,6 +26,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_PATH = os.path.join(HERE, "_lib", "liboracle.so")
 REFERENCE_PATH = os.path.join(HERE, "_ref", "libref_orrery.so")
 REFERENCE_CUDA_PATH = os.path.join(HERE, "_ref", "libref_orrery_cuda.so")
+REFERENCE_CUDA_SINGLE_PATH = os.path.join(HERE, "_ref", "libref_orrery_cuda_single.so")
+REFERENCE_ROOT_RECORD = os.path.join(HERE, "_ref", "reference_root.txt")
 
 _dp = C.POINTER(C.c_double)
 _u64p = C.POINTER(C.c_uint64)
@@ -40,12 +42,31 @@ def _u(a):
 
 
 def build(reference_root: str | None = None, with_reference: bool = True) -> None:
-    """Compile the restatement (and the reference library when its sources exist)."""
+    """Compile the restatement, and -- given the reference's checkout, by argument
+    or by the ORRERY_REFERENCE_ROOT environment variable -- the reference's own
+    libraries and the adapter test driver. Without a checkout the reference
+    libraries are left as they are (built ones travel with the repository)."""
     subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
-    root = reference_root or os.environ.get("ORRERY_REFERENCE_ROOT", "/root/reference")
-    if with_reference and os.path.isdir(os.path.join(root, "src", "solvers")):
-        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "ref_cuda", f"REF={root}"],
-                       check=True)
+    root = reference_root or os.environ.get("ORRERY_REFERENCE_ROOT")
+    if not with_reference or not root:
+        return
+    if not os.path.isdir(os.path.join(root, "src", "solvers")):
+        raise FileNotFoundError(f"{root} holds no reference checkout (src/solvers is missing)")
+    subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", "ref_cuda", "ref_cuda_single",
+                    "ref_adapter", f"REF={root}"], check=True)
+    with open(REFERENCE_ROOT_RECORD, "w") as fh:
+        fh.write(os.path.abspath(root))
+
+
+def reference_root() -> str | None:
+    """The reference checkout: ORRERY_REFERENCE_ROOT, else the one the last
+    build() used (recorded beside the libraries it built); None when neither
+    names an existing directory."""
+    root = os.environ.get("ORRERY_REFERENCE_ROOT")
+    if not root and os.path.exists(REFERENCE_ROOT_RECORD):
+        with open(REFERENCE_ROOT_RECORD) as fh:
+            root = fh.read().strip()
+    return root if root and os.path.isdir(root) else None
 
 
 class Counts(C.Structure):
@@ -565,3 +586,68 @@ class ReferenceCuda:
         if rc != 0:
             raise RuntimeError("the reference's CUDA tree solver found no device")
         return wall.value, kern.value, np.stack(a, axis=1), (int(counts[0]), int(counts[1]))
+
+
+REFERENCE_ADAPTER_PATH = os.path.join(HERE, "_ref", "libref_adapter.so")
+
+
+class AdapterDriver:
+    """ctypes binding of ref_adapter_shim.cpp: the reference's own integrators
+    (VelocityVerlet, Yoshida4, RungeKutta4) driven over the reference's CPU
+    solvers or over the B200 ForceSolver adapters, or B200Integrator."""
+
+    FIELDS = {"reference-direct": 0, "reference-tree": 1, "b200-direct": 2, "b200-tree": 3}
+    METHODS = {"vv": 0, "yoshida4": 1, "rk4": 2}
+    PRECISIONS = {"fp32": 0, "split": 1, "fp64": 2}
+    STATE = ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az")
+
+    @staticmethod
+    def built() -> bool:
+        return os.path.exists(REFERENCE_ADAPTER_PATH)
+
+    def __init__(self, path: str = REFERENCE_ADAPTER_PATH):
+        lib = C.CDLL(path)
+        lib.ra_last_error.restype = C.c_char_p
+        lib.ra_try_create.argtypes = [C.c_int, C.c_int]
+        lib.ra_integrator_traits.argtypes = [C.c_int, C.c_int, C.c_char_p, C.c_size_t,
+                                             C.POINTER(C.c_int), C.POINTER(C.c_int), _u64p]
+        lib.ra_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double,
+                               C.c_uint64, C.c_int, C.c_size_t] + [_dp] * 10 + [
+            C.c_double, C.c_uint64, _u64p, C.c_char_p, C.c_size_t]
+        self.lib = lib
+
+    def last_error(self) -> str:
+        return self.lib.ra_last_error().decode()
+
+    def try_create(self, tree: bool, precision: str = "fp32") -> int:
+        """1: a solver; 0: null (no usable device); other: an error code."""
+        return self.lib.ra_try_create(int(tree), self.PRECISIONS[precision])
+
+    def traits(self, adapter: bool, method: str):
+        name = C.create_string_buffer(64)
+        order, symplectic = C.c_int(), C.c_int()
+        evaluations = np.zeros(1, np.uint64)
+        self.lib.ra_integrator_traits(int(adapter), self.METHODS[method], name, 64,
+                                      C.byref(order), C.byref(symplectic), _u(evaluations))
+        return name.value.decode(), order.value, bool(symplectic.value), int(evaluations[0])
+
+    def run(self, field, state, m, dt, steps, method="vv", precision="fp64",
+            device_integrator=False, softening=0.01, opening_angle=0.5, leaf_capacity=32,
+            quadrupole=False):
+        """(return code, final state dict, counts (evaluations, pairs, cells), field name).
+
+        The accelerations are established by the field before the first step
+        (integrators::refresh_accelerations); any given in `state` are ignored."""
+        n = len(m)
+        arrays = {k: np.ascontiguousarray(state[k], dtype=np.float64).copy()
+                  for k in ("x", "y", "z", "vx", "vy", "vz")}
+        for k in ("ax", "ay", "az"):
+            arrays[k] = np.zeros(n)
+        mass = np.ascontiguousarray(m, dtype=np.float64)
+        counts = np.zeros(3, np.uint64)
+        name = C.create_string_buffer(64)
+        rc = self.lib.ra_run(self.FIELDS[field], self.PRECISIONS[precision], self.METHODS[method],
+                             int(device_integrator), softening, opening_angle, leaf_capacity,
+                             int(quadrupole), n, *(_d(arrays[k]) for k in self.STATE), _d(mass),
+                             dt, steps, _u(counts), name, 64)
+        return rc, arrays, tuple(int(c) for c in counts), name.value.decode()

@@ -2,9 +2,11 @@
 // CudaTreeSolver), so that the benchmark can time the reference's GPU path on
 // the same device and inputs as this backend's kernels.
 //
-// MEASUREMENT AND TEST INFRASTRUCTURE ONLY. Compiled by oracle/Makefile (target
-// ref_cuda) with the reference's sources, read where they lie, into
-// oracle/_ref/libref_orrery_cuda.so. Nothing in the product links it.
+// MEASUREMENT AND TEST INFRASTRUCTURE ONLY. Compiled by oracle/Makefile with
+// the reference's sources, read where they lie: target ref_cuda (double
+// precision) into oracle/_ref/libref_orrery_cuda.so, target ref_cuda_single
+// (ORRERY_SINGLE_PRECISION, Real = float) into
+// oracle/_ref/libref_orrery_cuda_single.so. Nothing in the product links it.
 #include <algorithm>
 #include <chrono>
 #include <cstdint>
@@ -19,14 +21,18 @@
 namespace {
 
 using orrery::core::ParticleData;
+using orrery::core::Real;
 using orrery::core::Vec3;
 
+// The inputs are FP64; a single-precision build (Real = float) rounds them
+// as its own callers would.
 ParticleData make_data(std::size_t n, const double* x, const double* y, const double* z,
                        const double* m) {
     ParticleData data;
     data.reserve(n);
     for (std::size_t i = 0; i < n; ++i) {
-        data.add(Vec3{x[i], y[i], z[i]}, Vec3{}, m[i]);
+        data.add(Vec3{static_cast<Real>(x[i]), static_cast<Real>(y[i]), static_cast<Real>(z[i])},
+                 Vec3{}, static_cast<Real>(m[i]));
     }
     return data;
 }
@@ -46,9 +52,13 @@ double seconds(orrery::backend::Duration d) { return std::chrono::duration<doubl
 
 extern "C" {
 
+// sizeof(Real) of this build: 8 (double) or 4 (single precision).
+int ref_cuda_real_bytes() { return static_cast<int>(sizeof(Real)); }
+
 // 1 when the reference's CUDA direct solver finds a usable device.
 int ref_cuda_available() {
-    return orrery::solvers::CudaDirectSolver::try_create(orrery::core::Softening{0.01}) ? 1 : 0;
+    const orrery::core::Softening softening{static_cast<Real>(0.01)};
+    return orrery::solvers::CudaDirectSolver::try_create(softening) ? 1 : 0;
 }
 
 // `repeats` evaluations after one warm-up; wall seconds per evaluation (the
@@ -58,7 +68,7 @@ int ref_cuda_direct_timed(std::size_t n, const double* x, const double* y, const
                           const double* m, double softening, int repeats, double* wall,
                           double* kernel, double* ax, double* ay, double* az) {
     auto solver = orrery::solvers::CudaDirectSolver::try_create(
-        orrery::core::Softening{softening});
+        orrery::core::Softening{static_cast<Real>(softening)});
     if (!solver) {
         return -1;
     }
@@ -96,7 +106,7 @@ int ref_cuda_tree_timed(std::size_t n, const double* x, const double* y, const d
             static_cast<unsigned>(threads));
     }
     auto solver = orrery::solvers::CudaTreeSolver::try_create(
-        params, orrery::core::Softening{softening}, executor.get());
+        params, orrery::core::Softening{static_cast<Real>(softening)}, executor.get());
     if (!solver) {
         return -1;
     }

@@ -799,9 +799,15 @@ class Server:
     def submit(self, state: dict, steps: int, dt: float, softening: float, kind: str = "direct",
                integrator: str = "yoshida4", opening_angle: float = 0.5,
                leaf_capacity: int = 32, quadrupole: bool = True) -> int:
+        solvers = {"direct": SOLVER_DIRECT, "tree": SOLVER_TREE}
+        if kind not in solvers:
+            raise OrreryError(ERROR_INVALID_ARGUMENT,
+                              f"unknown job kind {kind!r} (expected 'direct' or 'tree')")
+        if integrator not in _INTEGRATORS:
+            raise OrreryError(ERROR_INVALID_ARGUMENT, f"unknown integrator {integrator!r}")
         state = _state_of(state)
         n = len(state["m"])
-        spec = JobSpec(SOLVER_DIRECT if kind == "direct" else SOLVER_TREE,
+        spec = JobSpec(solvers[kind],
                        _INTEGRATORS[integrator], n, _count(steps, "steps"), float(dt),
                        float(softening) * float(softening), float(opening_angle),
                        int(leaf_capacity), 1 if quadrupole else 0, 0)

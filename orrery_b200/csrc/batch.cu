@@ -19,6 +19,7 @@
 
 #include "batch.hpp"
 #include "common.cuh"
+#include "runtime.hpp"
 #include "split_math.cuh"
 
 namespace ob {
@@ -231,10 +232,11 @@ cudaError_t launch_batch_t(const BatchArgs &args, int sm_count, cudaStream_t str
     const size_t smem = 8 * kDirectTile * sizeof(float4) + 2 * sizeof(uint64_t) +
                         (K > 1 ? 3 * THREADS * R * sizeof(double) : 0);
     auto kernel = batch_split_kernel<THREADS, R, K>;
-    static const cudaError_t configured = cudaFuncSetAttribute(
-        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (configured != cudaSuccess) {
-        return configured;
+    static std::atomic<uint64_t> configured{0};
+    const cudaError_t err = set_smem_limit_once(reinterpret_cast<const void *>(kernel),
+                                                static_cast<int>(smem), configured);
+    if (err != cudaSuccess) {
+        return err;
     }
     static int resident = 0;
     if (resident == 0) {

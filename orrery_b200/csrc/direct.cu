@@ -26,6 +26,7 @@
 #include <type_traits>
 
 #include "common.cuh"
+#include "runtime.hpp"
 #include "internal.hpp"
 #include "split_math.cuh"
 
@@ -578,12 +579,13 @@ cudaError_t launch_direct_t(const DirectArgs &args, int split, cudaStream_t stre
     const dim3 grid(static_cast<unsigned>(split), ceil_div(args.n, bt), 1);
     const size_t smem = direct_smem_bytes<THREADS, R, K, SPLIT>();
     auto kernel = direct_kernel_for<THREADS, R, K, SPLIT>();
-    // Set once per process (one process drives one device), before any graph
-    // capture reaches this launch.
-    static const cudaError_t configured = cudaFuncSetAttribute(
-        kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-    if (configured != cudaSuccess) {
-        return configured;
+    // Set once per device, on the first launch there (before any graph
+    // capture reaches it: solvers evaluate once before they capture).
+    static std::atomic<uint64_t> configured{0};
+    const cudaError_t err = set_smem_limit_once(reinterpret_cast<const void *>(kernel),
+                                                static_cast<int>(smem), configured);
+    if (err != cudaSuccess) {
+        return err;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;

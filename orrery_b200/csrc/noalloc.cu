@@ -1,11 +1,11 @@
 // Morton ordering that allocates nothing: ob_morton_order_noalloc.
 //
 // Some callers cannot allocate device memory at the moment they need an
-// ordering: code running inside a host callback or another library's stream
-// callback (where CUDA calls that may synchronise are forbidden), callers that
-// hand out device memory only from their own fixed pool and forbid other
-// allocations, and long-running services that must not fragment or grow the
-// device heap once they are up. This entry point serves them: the caller
+// ordering: callers that hand out device memory only from their own fixed pool
+// and forbid other allocations, and long-running services that must not
+// fragment or grow the device heap once they are up (a cudaMalloc can also
+// synchronise the device, which such a service's other streams would feel).
+// This entry point serves them: the caller
 // passes device memory for the inputs and the outputs, and every intermediate
 // buffer the ordering needs -- the second key/index buffer of the radix sort,
 // the digit histograms, the onesweep look-back words and tile tickets, the
@@ -27,6 +27,8 @@
 
 namespace ob {
 namespace {
+
+static_assert(OB_DEVICE_STATUS_TIMEOUT == kStatusTimeout, "the header names the timeout bit");
 
 // Largest particle count the fixed scratch holds.
 constexpr uint32_t kNoAllocMaxParticles = 1u << 20;
@@ -51,10 +53,8 @@ constexpr size_t kStatusBytes = align256(sizeof(unsigned));
 constexpr size_t kMetaOffset = kStatusOffset + kStatusBytes;
 constexpr size_t kMetaBytes = align256(sizeof(TreeMeta));
 constexpr size_t kCubeOffset = kMetaOffset + kMetaBytes;
-constexpr size_t kCubeBytes = align256(sizeof(double) * 6 * 592);
+constexpr size_t kCubeBytes = align256(sizeof(double) * 6 * kCubeBlocks);
 constexpr size_t kScratchBytes = kCubeOffset + kCubeBytes;
-
-static_assert(kCubeBytes >= sizeof(double) * 6 * 592, "cube partials fit");
 
 // The fixed scratch (about 14 MB). Host code must not use this name as a
 // device address: its host-side value is a stand-in, and the device address
@@ -88,7 +88,7 @@ unsigned char *scratch_for_current_device() {
 
 extern "C" int ob_morton_order_noalloc(uint64_t n, const double *x, const double *y,
                                        const double *z, uint64_t *codes, uint32_t *indices,
-                                       void *stream) {
+                                       uint32_t *status_out, void *stream) {
     using namespace ob;
     try {
         if (n > kNoAllocMaxParticles) {
@@ -104,6 +104,9 @@ extern "C" int ob_morton_order_noalloc(uint64_t n, const double *x, const double
         const auto s = static_cast<cudaStream_t>(stream);
         unsigned char *base = scratch_for_current_device();
         if (count == 0) {
+            if (status_out != nullptr) {
+                check(cudaMemsetAsync(status_out, 0, sizeof(uint32_t), s), "clearing status");
+            }
             return OB_OK;
         }
         auto *alt_keys = reinterpret_cast<unsigned long long *>(base + kKeysOffset);
@@ -140,6 +143,14 @@ extern "C" int ob_morton_order_noalloc(uint64_t n, const double *x, const double
                                   lookback + static_cast<size_t>(pass) * tiles * kRadix,
                                   tickets + pass, status, s),
                   "radix sort pass");
+        }
+        // A pass whose bounded look-back wait ran out set a bit in the status
+        // word and left its tile unscattered; hand the word to the caller, on
+        // the stream, so the failure is visible without a host wait here.
+        if (status_out != nullptr) {
+            check(cudaMemcpyAsync(status_out, status, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                                  s),
+                  "reporting the status word");
         }
         return OB_OK;
     } catch (const Error &e) {

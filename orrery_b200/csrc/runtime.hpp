@@ -1,6 +1,7 @@
 // Host-side runtime pieces shared by the C ABI: errors, device buffers.
 #pragma once
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <stdexcept>
@@ -30,6 +31,28 @@ inline void check(cudaError_t err, const char *what) {
         throw Error(code, std::string(what) + ": " + cudaGetErrorName(err) + " (" +
                               cudaGetErrorString(err) + ")");
     }
+}
+
+// Raises `kernel`'s dynamic shared-memory limit to `bytes` on the current
+// device. The attribute belongs to each device's context, so it is set once
+// per device: `configured` is the caller's per-kernel set of devices done
+// (bit d for device d; devices from 64 on are set on every call).
+inline cudaError_t set_smem_limit_once(const void *kernel, int bytes,
+                                       std::atomic<uint64_t> &configured) {
+    int device = 0;
+    cudaError_t err = cudaGetDevice(&device);
+    if (err != cudaSuccess) {
+        return err;
+    }
+    const uint64_t bit = device >= 0 && device < 64 ? (1ull << device) : 0ull;
+    if (bit != 0 && (configured.load(std::memory_order_acquire) & bit) != 0) {
+        return cudaSuccess;
+    }
+    err = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (err == cudaSuccess && bit != 0) {
+        configured.fetch_or(bit, std::memory_order_acq_rel);
+    }
+    return err;
 }
 
 // Sets the calling thread's last-error text and returns `code`.

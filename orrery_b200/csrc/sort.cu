@@ -17,71 +17,49 @@
 // global offsets by decoupled look-back over earlier tiles (every wait bounded)
 // and scatters through shared memory so the global writes are contiguous runs.
 #include "common.cuh"
+#include "runtime.hpp"
 #include "tree_kernels.hpp"
 
 namespace ob {
 namespace {
 
-constexpr uint32_t kReduceThreads = 256;
-constexpr uint32_t kReduceBlocks = 592; // 4 per SM
+constexpr uint32_t kReduceThreads = kCubeThreads;
+constexpr uint32_t kReduceBlocks = kCubeBlocks;
 
 __device__ __forceinline__ void min_max(double v, double &lo, double &hi) {
     lo = v < lo ? v : lo;
     hi = hi < v ? v : hi;
 }
 
-__global__ void __launch_bounds__(kReduceThreads)
-    cube_partial_kernel(const double *__restrict__ x, const double *__restrict__ y,
-                        const double *__restrict__ z, uint32_t n, double *partials) {
-    double lo[3] = {INFINITY, INFINITY, INFINITY};
-    double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        min_max(x[i], lo[0], hi[0]);
-        min_max(y[i], lo[1], hi[1]);
-        min_max(z[i], lo[2], hi[2]);
-    }
+// Block-wide min (k < 3) / max (k >= 3) of the six values each thread holds
+// in v[]; thread k < 6 receives component k in `out`.
+__device__ __forceinline__ void block_min_max(double (&v)[6], double &out) {
     __shared__ double s[6][kReduceThreads / 32];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) {
+    for (int k = 0; k < 6; ++k) {
         for (int off = 16; off > 0; off >>= 1) {
-            const double l = __shfl_down_sync(0xffffffffu, lo[a], off);
-            const double h = __shfl_down_sync(0xffffffffu, hi[a], off);
-            lo[a] = l < lo[a] ? l : lo[a];
-            hi[a] = hi[a] < h ? h : hi[a];
+            const double o = __shfl_down_sync(0xffffffffu, v[k], off);
+            v[k] = k < 3 ? (o < v[k] ? o : v[k]) : (v[k] < o ? o : v[k]);
         }
         if (lane == 0) {
-            s[a][warp] = lo[a];
-            s[3 + a][warp] = hi[a];
+            s[k][warp] = v[k];
         }
     }
     __syncthreads();
     if (threadIdx.x < 6) {
         const int k = threadIdx.x;
-        double v = s[k][0];
+        double r = s[k][0];
         for (uint32_t w = 1; w < kReduceThreads / 32; ++w) {
-            v = k < 3 ? (s[k][w] < v ? s[k][w] : v) : (v < s[k][w] ? s[k][w] : v);
+            r = k < 3 ? (s[k][w] < r ? s[k][w] : r) : (r < s[k][w] ? s[k][w] : r);
         }
-        partials[blockIdx.x * 6 + k] = v;
+        out = r;
     }
 }
 
-__global__ void cube_final_kernel(const double *partials, uint32_t blocks, uint32_t n,
-                                  TreeMeta *meta) {
-    __shared__ double s[6];
-    if (threadIdx.x < 6) {
-        const int k = threadIdx.x;
-        double v = partials[k];
-        for (uint32_t b = 1; b < blocks; ++b) {
-            const double p = partials[b * 6 + k];
-            v = k < 3 ? (p < v ? p : v) : (v < p ? p : v);
-        }
-        s[k] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x != 0) {
-        return;
-    }
+// The cube from the extremes (morton.cpp:60-104): edge = the largest extent
+// (1 when it is not positive), centred on the box.
+__device__ void write_cube(const double *ext, uint32_t n, TreeMeta *meta) {
     if (n == 0) {
         for (int a = 0; a < 3; ++a) {
             meta->origin[a] = 0.0;
@@ -90,9 +68,9 @@ __global__ void cube_final_kernel(const double *partials, uint32_t blocks, uint3
         meta->size = 0.0;
         return;
     }
-    const double ex = __dsub_rn(s[3], s[0]);
-    const double ey = __dsub_rn(s[4], s[1]);
-    const double ez = __dsub_rn(s[5], s[2]);
+    const double ex = __dsub_rn(ext[3], ext[0]);
+    const double ey = __dsub_rn(ext[4], ext[1]);
+    const double ez = __dsub_rn(ext[5], ext[2]);
     double size = ex;
     size = size < ey ? ey : size;
     size = size < ez ? ez : size;
@@ -101,13 +79,67 @@ __global__ void cube_final_kernel(const double *partials, uint32_t blocks, uint3
     }
     const double half = __ddiv_rn(size, 2.0);
     for (int a = 0; a < 3; ++a) {
-        const double centre = __ddiv_rn(__dadd_rn(s[a], s[3 + a]), 2.0);
+        const double centre = __ddiv_rn(__dadd_rn(ext[a], ext[3 + a]), 2.0);
         const double origin = __dsub_rn(centre, half);
         meta->origin[a] = origin;
         // BoundingCube::centre (morton.hpp:93-95): origin + size/2.
         meta->root_centre[a] = __dadd_rn(origin, half);
     }
     meta->size = size;
+}
+
+// One pass over the positions: each block writes its six extremes, and the
+// last block to finish (an atomic count in meta) folds all blocks' partials
+// with the whole block and writes the cube. Min and max are exact, so the
+// order of the fold does not change the result.
+__global__ void __launch_bounds__(kReduceThreads)
+    cube_kernel(const double *__restrict__ x, const double *__restrict__ y,
+                const double *__restrict__ z, uint32_t n, double *partials, TreeMeta *meta) {
+    double v[6] = {INFINITY, INFINITY, INFINITY, -INFINITY, -INFINITY, -INFINITY};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        min_max(x[i], v[0], v[3]);
+        min_max(y[i], v[1], v[4]);
+        min_max(z[i], v[2], v[5]);
+    }
+    double mine = 0.0;
+    block_min_max(v, mine);
+    __shared__ bool last;
+    if (threadIdx.x < 6) {
+        partials[blockIdx.x * 6 + threadIdx.x] = mine;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        last = atomicAdd(&meta->cube_blocks_done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) {
+        return;
+    }
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        v[k] = k < 3 ? INFINITY : -INFINITY;
+    }
+    for (uint32_t b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            // Empty blocks hold (+inf, -inf): lows only lower, highs only raise.
+            const double p = __ldcg(partials + b * 6 + k);
+            v[k] = k < 3 ? (p < v[k] ? p : v[k]) : (v[k] < p ? p : v[k]);
+        }
+    }
+    __syncthreads(); // block_min_max's shared array is reused
+    __shared__ double ext[6];
+    double folded = 0.0;
+    block_min_max(v, folded);
+    if (threadIdx.x < 6) {
+        ext[threadIdx.x] = folded;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        write_cube(ext, n, meta);
+    }
 }
 
 // Dilation by table: each 7-bit chunk of a grid coordinate maps to 21 bits
@@ -432,12 +464,11 @@ size_t onesweep_smem() {
 
 uint32_t sort_tiles(uint32_t n) { return ceil_div(n == 0 ? 1 : n, kSortTile); }
 
-size_t cube_partials_needed(uint32_t) { return 6ull * kReduceBlocks; }
+size_t cube_partials_needed(uint32_t) { return 6ull * kCubeBlocks; }
 
 cudaError_t launch_bounding_cube(const double *x, const double *y, const double *z, uint32_t n,
                                  double *partials, TreeMeta *meta, cudaStream_t stream) {
-    cube_partial_kernel<<<kReduceBlocks, kReduceThreads, 0, stream>>>(x, y, z, n, partials);
-    cube_final_kernel<<<1, 32, 0, stream>>>(partials, kReduceBlocks, n, meta);
+    cube_kernel<<<kCubeBlocks, kCubeThreads, 0, stream>>>(x, y, z, n, partials, meta);
     return cudaGetLastError();
 }
 
@@ -458,11 +489,11 @@ cudaError_t launch_onesweep(const unsigned long long *keys_in, const uint32_t *v
                             unsigned long long *keys_out, uint32_t *vals_out, uint32_t n,
                             int pass, const uint32_t *offsets, uint32_t *lookback,
                             uint32_t *ticket, unsigned *status, cudaStream_t stream) {
-    static const cudaError_t configured =
-        cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(onesweep_smem()));
-    if (configured != cudaSuccess) {
-        return configured;
+    static std::atomic<uint64_t> configured{0};
+    const cudaError_t err = set_smem_limit_once(reinterpret_cast<const void *>(onesweep_kernel),
+                                                static_cast<int>(onesweep_smem()), configured);
+    if (err != cudaSuccess) {
+        return err;
     }
     onesweep_kernel<<<sort_tiles(n), kSortThreads, onesweep_smem(), stream>>>(
         keys_in, vals_in, keys_out, vals_out, n, static_cast<uint32_t>(kRadixBits * pass),

@@ -56,6 +56,8 @@ struct TreeMeta {
     uint32_t leaf_count;
     uint32_t depth;
     uint32_t required;  // nodes the layout needed (reported on overflow)
+    uint32_t cube_blocks_done; // bounding-cube blocks finished (the last one folds)
+    uint32_t reserved;
     unsigned long long pairs;
     unsigned long long cells;
 };

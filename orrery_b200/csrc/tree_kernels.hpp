@@ -20,6 +20,11 @@ constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;
 
+// Bounding-cube reduction: blocks of the min/max pass (4 per SM); the
+// partials buffer holds 6 doubles per block.
+constexpr uint32_t kCubeThreads = 256;
+constexpr uint32_t kCubeBlocks = 592;
+
 // Largest particle count the onesweep status words can carry (30-bit counts).
 constexpr uint32_t kMaxTreeParticles = (1u << 30) - 1;
 
@@ -27,7 +32,9 @@ uint32_t sort_tiles(uint32_t n);
 size_t cube_partials_needed(uint32_t n);
 
 // Bounding cube (src/solvers/morton.cpp:60-104) into meta->origin/size and
-// meta->root_centre; `partials` holds 6 doubles per reduction block.
+// meta->root_centre; `partials` holds cube_partials_needed() doubles and
+// meta->cube_blocks_done starts at zero (the last block to finish folds the
+// partials).
 cudaError_t launch_bounding_cube(const double *x, const double *y, const double *z, uint32_t n,
                                  double *partials, TreeMeta *meta, cudaStream_t stream);
 

@@ -2,7 +2,7 @@
 reference's own code (service/orrery_service/limits.py, work_units and
 MAX_WORK), for cases the server's admission tests use.
 
-    python tests/golden/make_golden_work_units.py
+    ORRERY_REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden_work_units.py
 """
 from __future__ import annotations
 
@@ -11,11 +11,14 @@ import json
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIMITS = "/root/reference/service/orrery_service/limits.py"
 
 
 def main() -> None:
-    spec = importlib.util.spec_from_file_location("reference_limits", LIMITS)
+    root = os.environ.get("ORRERY_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("set ORRERY_REFERENCE_ROOT to the reference's checkout")
+    limits_path = os.path.join(root, "service", "orrery_service", "limits.py")
+    spec = importlib.util.spec_from_file_location("reference_limits", limits_path)
     limits = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(limits)
     cases = [(0, 10, "direct"), (1, 10, "barnes-hut"), (2, 7, "direct"), (1000, 20, "direct"),

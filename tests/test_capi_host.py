@@ -139,3 +139,15 @@ def test_positions_are_accepted_in_every_documented_layout():
         ob._split_xyz(np.zeros((4, 4)))
     with pytest.raises(ValueError):
         ob._split_xyz(np.zeros(6))
+
+
+def test_noalloc_ordering_checks_its_arguments_before_the_device(lib):
+    # Refusals come before any CUDA call, so they hold on a machine without a
+    # device too: above the fixed scratch's capacity, and NULL arrays.
+    fn = lib.ob_morton_order_noalloc
+    fn.argtypes = [C.c_uint64] + [C.c_void_p] * 7
+    fn.restype = C.c_int
+    assert fn((1 << 20) + 1, None, None, None, None, None, None, None) == ob.ERROR_CAPACITY
+    assert b"1048576" in lib.ob_last_error()
+    fake = C.c_void_p(16)  # never dereferenced: the NULL check refuses first
+    assert fn(10, fake, fake, None, fake, fake, None, None) == ob.ERROR_INVALID_ARGUMENT

@@ -220,3 +220,12 @@ def test_any_timeout_is_a_deadline_the_clock_can_hold():
         s.drain(timeout=float("inf"))
     finally:
         s.close()
+
+
+def test_an_unknown_job_kind_or_integrator_is_refused(server):
+    # A misspelt kind must not quietly become a Barnes-Hut job.
+    for kw in (dict(kind="drect"), dict(kind="barnes-hut"), dict(integrator="leapfrog")):
+        with pytest.raises(ob.OrreryError) as e:
+            server.submit(_state(100), steps=2, dt=1e-3, softening=0.01, **kw)
+        assert e.value.code == ob.ERROR_INVALID_ARGUMENT
+    assert server.stats()["queued"] == 0
