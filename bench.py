@@ -137,6 +137,43 @@ def step_units(w):
     return 1
 
 
+def dtype_of(w):
+    """The arithmetic the force path computes in."""
+    return {"fp32": "f32", "split": "f32-split (hi/lo FP32 pair math, FP64 sums)",
+            "fp64": "f64"}[w["precision"]]
+
+
+def relative_errors(got, exact):
+    """Per-particle |a - a_ref| / |a_ref| over particles with a nonzero a_ref."""
+    mag = np.linalg.norm(exact, axis=1)
+    ok = mag > 0
+    return np.linalg.norm(got - exact, axis=1)[ok] / mag[ok]
+
+
+def error_summary(err, against):
+    return {"median": float(np.median(err)), "max": float(np.max(err)),
+            "rms": float(np.sqrt(np.mean(err ** 2))), "particles": int(err.size),
+            "against": against}
+
+
+def direct_fp64_sampled(torch, device, st, m, eps, targets, chunk=1 << 14):
+    """FP64 direct sum sum_j m_j d / (|d|^2 + eps^2)^(3/2) at the sampled
+    targets over every source, on the device (torch FP64; a measurement of the
+    error, not the product path). The target's own term is exactly zero under
+    softening, as the reference's skip makes it."""
+    pos = torch.tensor(np.stack([st["x"], st["y"], st["z"]], axis=1), dtype=torch.float64,
+                       device=device)
+    mass = torch.tensor(m, dtype=torch.float64, device=device)
+    tgt = pos[torch.as_tensor(targets, device=device)]
+    acc = torch.zeros_like(tgt)
+    for start in range(0, pos.shape[0], chunk):
+        d = pos[start:start + chunk][None, :, :] - tgt[:, None, :]
+        r2 = (d * d).sum(-1) + eps * eps
+        w = mass[start:start + chunk][None, :] / (r2 * torch.sqrt(r2))
+        acc += (w[:, :, None] * d).sum(1)
+    return acc.cpu().numpy()
+
+
 # ---------------------------------------------------------------------------
 # Clocks during the timed region
 # ---------------------------------------------------------------------------
@@ -268,14 +305,24 @@ def cpu_baseline(w, data, budget_s=20.0):
         sec = ref.direct_seconds(x, y, z, m, w["eps"], threads, repeats=reps)
         value = n * (n - 1) / sec / 1e9
         return dict(value=value, unit="Gint/s", cores=threads, kind="reference",
+                    evaluations_timed=reps,
+                    steps_timed=reps / evaluations_per_step(w),
                     sample=f"{reps} DirectSolver evaluations (AVX2, {threads} threads) "
                            f"of the full {n}-particle input")
-    sec = ref.barnes_hut_seconds(x, y, z, m, w["eps"], w["theta"], w["leaf"], w["quadrupole"],
+    one = ref.barnes_hut_seconds(x, y, z, m, w["eps"], w["theta"], w["leaf"], w["quadrupole"],
                                  threads, repeats=1)
+    reps = max(1, min(int(budget_s / max(one, 1e-6)) - 1, 10))
+    sec = one
+    if reps > 1:
+        sec = ref.barnes_hut_seconds(x, y, z, m, w["eps"], w["theta"], w["leaf"],
+                                     w["quadrupole"], threads, repeats=reps)
     return dict(value=sec * 1e3 * evaluations_per_step(w), unit="ms/step", cores=threads,
-                kind="reference",
-                sample=f"one BarnesHutSolver evaluation (AVX2 leaves, {threads} threads) of the "
-                       f"full {len(m)}-particle input = one VV step's force evaluation")
+                kind="reference", evaluations_timed=reps,
+                steps_timed=reps / evaluations_per_step(w),
+                sample=f"{reps} BarnesHutSolver evaluation(s) (AVX2 leaves, {threads} threads) "
+                       f"of the full {len(m)}-particle input, after one untimed; one "
+                       "evaluation is one VV step's force work (the O(N) kicks are not "
+                       "timed: under 0.1 % of the step)")
 
 
 def cpu_baseline_batch(w, sizes, radii, systems, budget_s=15.0):
@@ -391,19 +438,32 @@ def reference_gpu(w, data):
             return None
         x, y, z, m = (np.ascontiguousarray(data[k]) for k in ("x", "y", "z", "m"))
         n = len(m)
-        if w["kind"] == "direct":
-            wall, kern, _ = ref.direct_timed(x, y, z, m, w["eps"], repeats=3)
-            return {"solver": "CudaDirectSolver (FP64 Real, the reference's direct_kernel)",
-                    "kernel_gint_s": n * (n - 1) / kern / 1e9,
-                    "evaluate_gint_s": n * (n - 1) / wall / 1e9,
-                    "kernel_ms": kern * 1e3, "evaluate_ms": wall * 1e3}
+        builds = [("f64", ref)]
+        if oracle.ReferenceCuda.built(single=True):
+            builds.append(("f32", oracle.ReferenceCuda(single=True)))
+        out = {}
         threads = oracle.Reference().worker_count() if oracle.Reference.available() else 1
-        wall, kern, _, counts = ref.tree_timed(x, y, z, m, w["eps"], w["theta"], w["leaf"],
-                                               w["quadrupole"], threads, repeats=1)
-        return {"solver": "CudaTreeSolver (host sort and build on "
-                          f"{threads} threads, coherent traversal on the device)",
-                "evaluate_ms": wall * 1e3, "kernel_ms": kern * 1e3,
-                "pairs": counts[0], "cells": counts[1]}
+        for real, r in builds:
+            if w["kind"] == "direct":
+                wall, kern, _ = r.direct_timed(x, y, z, m, w["eps"], repeats=3)
+                out[real] = {"solver": f"CudaDirectSolver ({real} Real build, the reference's "
+                                       "direct_kernel)",
+                             "kernel_gint_s": n * (n - 1) / kern / 1e9,
+                             "evaluate_gint_s": n * (n - 1) / wall / 1e9,
+                             "kernel_ms": kern * 1e3, "evaluate_ms": wall * 1e3}
+            else:
+                wall, kern, _, counts = r.tree_timed(x, y, z, m, w["eps"], w["theta"], w["leaf"],
+                                                     w["quadrupole"], threads, repeats=1)
+                out[real] = {"solver": f"CudaTreeSolver ({real} Real build; host sort and "
+                                       f"build on {threads} threads, coherent traversal on "
+                                       "the device)",
+                             "evaluate_ms": wall * 1e3, "kernel_ms": kern * 1e3,
+                             "pairs": counts[0], "cells": counts[1]}
+        # The double-precision build's figures stay at the top level.
+        line = dict(out["f64"])
+        if "f32" in out:
+            line["single_precision_build"] = out["f32"]
+        return line
     except (OSError, RuntimeError) as err:
         return {"unavailable": str(err)}
 
@@ -462,11 +522,16 @@ def run_reference(args, w):
     else:
         ms_per_step = value if w["unit"] == "ms/step" else \
             step_units(w) / (value * 1e9) * 1e3
+    # `steps`: the steps' worth of work actually timed (a bounded sample: the
+    # CPU takes seconds per 2M evaluation), not the requested K.
+    timed = base.get("steps_timed", steps)
     line = {
         "impl": "reference", "metric": w["metric"], "value": value, "unit": w["unit"],
-        "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
-        "ms_per_step": ms_per_step, "higher_is_better": w["higher"], "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "n_gpus": args.gpus, "steps": timed, "steps_requested": steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": w["higher"],
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "sampled": f"value measured on {base.get('evaluations_timed', '?')} evaluation(s) of "
+                   "the full input and stated per step",
         "config": config_of(args, w), "cpu_baseline": base,
         "e2e": {"value": value, "unit": w["unit"], "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -727,24 +792,51 @@ def e2e_drop_in(ob, w, data, steps, torch):
         outer, inner = 1.0 / (2.0 - c), -c / (2.0 - c)
         weights = [outer * w["dt"], inner * w["dt"], outer * w["dt"]]
 
+    tmp = np.empty(n)
+    clock = {"host": 0.0, "evaluate": 0.0, "transfer_in": 0.0, "transfer_out": 0.0,
+             "device": 0.0}
+
+    def kick(half):
+        # v += (dt/2) a in place, as the reference's kick (no temporaries).
+        for v, a in ((vx, ax), (vy, ay), (vz, az)):
+            np.multiply(a, half, out=tmp)
+            v += tmp
+
     def step():
         for h in weights:
             half = h / 2.0
-            for v, a in ((vx, ax), (vy, ay), (vz, az)):
-                v += half * a
+            t = time.perf_counter()
+            kick(half)
             for p, v in ((x, vx), (y, vy), (z, vz)):
-                p += h * v
+                np.multiply(v, h, out=tmp)
+                p += tmp
+            t1 = time.perf_counter()
             solver.evaluate((x, y, z), m, (ax, ay, az))
-            for v, a in ((vx, ax), (vy, ay), (vz, az)):
-                v += half * a
+            t2 = time.perf_counter()
+            kick(half)
+            t3 = time.perf_counter()
+            clock["host"] += (t1 - t) + (t3 - t2)
+            clock["evaluate"] += t2 - t1
+            tm = solver.timings()
+            clock["transfer_in"] += tm["transfer_in_ms"] * 1e-3
+            clock["transfer_out"] += tm["transfer_out_ms"] * 1e-3
+            clock["device"] += (tm["ordering_ms"] + tm["construction_ms"] +
+                                tm["traversal_ms"]) * 1e-3
 
     step()
+    for k in clock:
+        clock[k] = 0.0
     t0 = time.perf_counter()
     for _ in range(steps):
         step()
     sec = (time.perf_counter() - t0) / steps
     evals = len(weights)
-    return sec, evals * 4 * 8 * n, evals * 3 * 8 * n, solver
+    breakdown = {f"{k}_ms": v / steps * 1e3 for k, v in clock.items()}
+    breakdown["note"] = ("per step: host = the integrator's NumPy kick/drift arithmetic; "
+                         "evaluate = ob_solver_evaluate's wall time, of which transfer_in / "
+                         "transfer_out are its host<->device copies and device its kernels "
+                         "(CUDA events)")
+    return sec, evals * 4 * 8 * n, evals * 3 * 8 * n, solver, breakdown
 
 
 def run_batch(args, w):
@@ -806,8 +898,8 @@ def run_batch(args, w):
         line = {
             "metric": w["metric"], "value": value, "unit": w["unit"], "n_gpus": world,
             "steps": K, "warmup": max(args.warmup, 3), "ms_per_step": total_ms / K,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "state_dtype": "f64", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": dtype_of(w), "state_dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "systems": len(sizes),
                        "particles": total_n, "pairs_per_evaluation": pairs,
                        "precision": "split", "integrator": "yoshida4", "dt": w["dt"],
@@ -942,7 +1034,8 @@ def plain_arm(ob, torch, jobs, states, precision, sample, horizon):
     order, as the reference's Simulation drives a ForceSolver: host integrator
     arithmetic on FP64 arrays in pinned memory and ob_solver_evaluate (host
     buffers in, accelerations out) per force evaluation. Stops early once the
-    stream clock passes `horizon` seconds (jobs not reached are reported)."""
+    stream clock passes `horizon` seconds when one is given (the line then
+    reports the arm as undrained); by default every job runs."""
     c = 1.2599210498948731647672106
     weights = {"yoshida4": [1.0 / (2.0 - c), -c / (2.0 - c), 1.0 / (2.0 - c)], "vv": [1.0]}
     solvers = {"direct": ob.B200DirectSolver(0.01, precision),
@@ -952,7 +1045,7 @@ def plain_arm(ob, torch, jobs, states, precision, sample, horizon):
     start = time.perf_counter()
     for k, job in enumerate(jobs):
         now = time.perf_counter() - start
-        if now > horizon:
+        if horizon and now > horizon:
             break
         if job["t"] > now:
             time.sleep(job["t"] - now)
@@ -961,19 +1054,24 @@ def plain_arm(ob, torch, jobs, states, precision, sample, horizon):
         x, y, z, m = (pin(st[q]) for q in ("x", "y", "z", "m"))
         vx, vy, vz = (pin(st[q]) for q in ("vx", "vy", "vz"))
         ax, ay, az = (pin(np.zeros(job["n"])) for _ in range(3))
+        tmp = np.empty(job["n"])
         solver.evaluate((x, y, z), m, (ax, ay, az))
         for _ in range(job["steps"]):
             t0 = time.perf_counter()
             for wgt in weights[p["integrator"]]:
                 h = wgt * p["dt"]
                 half = h / 2.0
+                # In place, as the reference's kick and drift (no temporaries).
                 for v, a in ((vx, ax), (vy, ay), (vz, az)):
-                    v += half * a
+                    np.multiply(a, half, out=tmp)
+                    v += tmp
                 for q, v in ((x, vx), (y, vy), (z, vz)):
-                    q += h * v
+                    np.multiply(v, h, out=tmp)
+                    q += tmp
                 solver.evaluate((x, y, z), m, (ax, ay, az))
                 for v, a in ((vx, ax), (vy, ay), (vz, az)):
-                    v += half * a
+                    np.multiply(a, half, out=tmp)
+                    v += tmp
             step_times.append(time.perf_counter() - t0)
         finishes.append(time.perf_counter() - start)
         if k in sample:
@@ -1004,7 +1102,8 @@ def latency_summary(jobs, finishes):
     lat = [finishes[k] - jobs[k]["t"] for k in range(done)]
     makespan = max(finishes) if finishes else float("inf")
     pct = lambda v, q: float(np.percentile(v, q)) if v else None  # noqa: E731
-    return {"completed": done, "makespan_s": makespan, "jobs_per_s": done / makespan,
+    return {"completed": done, "drained": done == len(jobs), "makespan_s": makespan,
+            "jobs_per_s": done / makespan,
             "job_latency_p50_s": pct(lat, 50), "job_latency_p99_s": pct(lat, 99)}
 
 
@@ -1050,7 +1149,7 @@ def run_serving(args, w):
             "metric": w["metric"], "value": served["jobs_per_s"], "unit": "jobs/s",
             "n_gpus": world, "steps": len(jobs), "warmup": 0,
             "ms_per_step": served["step_latency_p50_ms"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "state_dtype": "f64",
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(w), "state_dtype": "f64",
             "data": "synthetic",
             "config": {"workload": args.workload, "arrival_window_s": args.window,
                        "arrival_rate_per_s": 20.0, "jobs": len(jobs),
@@ -1058,8 +1157,8 @@ def run_serving(args, w):
                        "direct_particles": sum(j["n"] for j in jobs if j["kind"] == "direct"),
                        "tree_particles": sum(j["n"] for j in jobs if j["kind"] == "tree"),
                        "hbm_budget_gb": 150, "max_tree_jobs": 2, "direct_pairs_cap": 1 << 34,
-                       "jobs_per_s": "jobs / (last completion - stream start); every arm "
-                                     "drains the whole stream"},
+                       "jobs_per_s": "jobs / (last completion - stream start); an arm "
+                                     "that did not drain the stream says so (drained)"},
             "served": served,
             "plain": plains,
             "served_over_plain": {k: served["jobs_per_s"] / v["jobs_per_s"]
@@ -1095,10 +1194,11 @@ def run_b200(args, w):
                              quadrupole=w.get("quadrupole", False))
     system.set_state(data["x"], data["y"], data["z"], data["vx"], data["vy"], data["vz"],
                      data["m"])
-    # The precision form states its energy drift from t = 0 (FP64 energies
-    # on the device, outside the timed region).
-    track_accuracy = w["kind"] == "direct" and w["precision"] == "split"
-    energy0 = sum(system.energy()) if track_accuracy else None
+    # Direct workloads state their energy drift from t = 0 (FP64 energies on
+    # the device, outside the timed region); at 2M the O(N^2) FP64 potential
+    # takes about a minute, so tree workloads give it only with --energy.
+    track_energy = w["kind"] == "direct" or args.energy
+    energy0 = sum(system.energy()) if track_energy else None
     tuned = None
     if w["kind"] == "direct" and w["precision"] != "fp64":
         tuned = system.autotune()
@@ -1160,24 +1260,42 @@ def run_b200(args, w):
     cell_count = counts_end.particle_cell - counts_start.particle_cell
 
     ms_per_step = total_ms / K
-    accuracy = None
-    if track_accuracy:
-        taken = max(args.warmup, 3) + 2 * K  # warm-up, timed and profiled steps
-        extra = max(0, args.accuracy_steps - taken)
-        if extra:
-            system.step(w["dt"], extra, w["integrator"])
+    # Stated error of the result, outside the timed region: the final state's
+    # accelerations against FP64 solvers on the same positions.
+    taken = max(args.warmup, 3) + 2 * K  # warm-up, timed and profiled steps
+    extra = max(0, args.accuracy_steps - taken)
+    if extra:
+        system.step(w["dt"], extra, w["integrator"])
+    st = system.state()
+    got = np.stack([st["ax"], st["ay"], st["az"]], axis=1)
+    accuracy = {"steps": taken + extra}
+    if energy0 is not None:
         energy1 = sum(system.energy())
-        st = system.state()
+        accuracy["relative_energy_drift"] = (energy1 - energy0) / abs(energy0)
+    if w["kind"] == "direct":
         exact = ob.B200DirectSolver(w["eps"], "fp64").evaluate((st["x"], st["y"], st["z"]),
                                                                data["m"])
-        got = np.stack([st["ax"], st["ay"], st["az"]], axis=1)
-        err = np.linalg.norm(got - exact, axis=1) / np.linalg.norm(exact, axis=1)
-        accuracy = {"steps": taken + extra,
-                    "relative_energy_drift": (energy1 - energy0) / abs(energy0),
-                    "force_error_vs_fp64": {"median": float(np.median(err)),
-                                            "max": float(np.max(err)),
-                                            "at": "the final state, against the bit-exact "
-                                                  "FP64 direct solver"}}
+        accuracy["force_error_vs_fp64"] = error_summary(
+            relative_errors(got, exact),
+            "the final state's accelerations against the FP64 direct solver (bit-identical "
+            "to the reference's DirectSolver)")
+    else:
+        if w["precision"] != "fp64":
+            tree64 = ob.B200TreeSolver(w["eps"], w["theta"], w["leaf"], w["quadrupole"],
+                                       precision="fp64")
+            exact = tree64.evaluate((st["x"], st["y"], st["z"]), data["m"])
+            del tree64
+            accuracy["force_error_vs_fp64_tree"] = error_summary(
+                relative_errors(got, exact),
+                f"every particle against the FP64 tree at the same theta {w['theta']} (the "
+                "reference's BarnesHutSolver, bit-identical), same positions")
+        rng = np.random.default_rng(20261203)
+        targets = np.sort(rng.choice(n, size=min(n, 4096), replace=False))
+        direct = direct_fp64_sampled(torch, device, st, data["m"], w["eps"], targets)
+        accuracy["force_error_vs_fp64_direct"] = error_summary(
+            relative_errors(got[targets], direct),
+            f"{len(targets)} sampled particles against the FP64 direct sum over all "
+            f"{n} sources (the tree's own theta {w['theta']} approximation included)")
     if w["unit"] == "ms/step":
         value = ms_per_step / world  # whole-job time per 2M step across replicas
     else:
@@ -1239,7 +1357,8 @@ def run_b200(args, w):
     if rank == 0:
         e2e_steps = max(2, min(K, 10 if w["kind"] == "tree" else 50))
         sec, h2d, d2h = e2e_integrator_plugin(system, w, data, e2e_steps, torch)
-        sec_solver, h2d_solver, d2h_solver, solver = e2e_drop_in(ob, w, data, e2e_steps, torch)
+        sec_solver, h2d_solver, d2h_solver, solver, split = e2e_drop_in(ob, w, data, e2e_steps,
+                                                                         torch)
         if w["kind"] == "tree":
             nodes, leaves, depth = solver.tree_stats()
             # Algorithmic bytes of one walk launch: each target's FP64 position
@@ -1268,7 +1387,7 @@ def run_b200(args, w):
             "metric": w["metric"], "value": value, "unit": w["unit"], "n_gpus": world,
             "steps": K, "warmup": max(args.warmup, 3), "ms_per_step": ms_per_step,
             "higher_is_better": w["higher"], "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "state_dtype": "f64", "data": "synthetic",
+            "dtype": dtype_of(w), "state_dtype": "f64", "data": "synthetic",
             "config": config_of(args, w),
             "phases_ms": {k: phases[k] for k in ("ordering_ms", "construction_ms",
                                                   "traversal_ms")},
@@ -1287,7 +1406,8 @@ def run_b200(args, w):
                                   "d2h_bytes_per_step": d2h_solver,
                                   "path": "the reference's host integrator arithmetic (NumPy) "
                                           "around ob_solver_evaluate (ForceSolver::evaluate) "
-                                          "on pinned host buffers"},
+                                          "on pinned host buffers",
+                                  "breakdown": split},
             "gpu_launches": kernels_per_step * K,
             "clocks": clocks,
         }
@@ -1310,13 +1430,17 @@ def main():
     ap.add_argument("--window", type=float, default=3.0,
                     help="serving: seconds of Poisson arrivals (every arm drains them all)")
     ap.add_argument("--accuracy-steps", type=int, default=0,
-                    help="split direct workloads: total steps after which energy drift and "
-                         "force error are stated (default: the warm-up and timed steps)")
+                    help="total steps after which the energy drift and force error are "
+                         "stated (default: the warm-up, timed and profiled steps)")
+    ap.add_argument("--energy", action="store_true",
+                    help="tree workloads: also state the FP64 energy drift (the O(N^2) "
+                         "potential at 2M takes about a minute of device time)")
     ap.add_argument("--plain-precision", default="fp32",
                     help="serving: comma-separated direct precisions of the plain arms")
-    ap.add_argument("--plain-horizon-factor", type=float, default=4.0,
+    ap.add_argument("--plain-horizon-factor", type=float, default=0.0,
                     help="serving: a plain arm stops once its clock passes this multiple "
-                         "of the served makespan")
+                         "of the served makespan and is reported undrained (0: every arm "
+                         "drains the whole stream)")
     args = ap.parse_args()
     w = WORKLOADS[args.workload]
     if args.impl == "reference":

@@ -542,11 +542,16 @@ class ReferenceCuda:
     CudaTreeSolver (its own GPU path) on this machine's device."""
 
     @staticmethod
-    def built() -> bool:
-        return os.path.exists(REFERENCE_CUDA_PATH)
+    def built(single: bool = False) -> bool:
+        return os.path.exists(REFERENCE_CUDA_SINGLE_PATH if single else REFERENCE_CUDA_PATH)
 
-    def __init__(self, path: str = REFERENCE_CUDA_PATH):
+    def __init__(self, path: str | None = None, single: bool = False):
+        """single: the reference's single-precision build (Real = float, its
+        cuda-single-precision preset) instead of its double-precision one."""
+        path = path or (REFERENCE_CUDA_SINGLE_PATH if single else REFERENCE_CUDA_PATH)
         lib = C.CDLL(path)
+        lib.ref_cuda_real_bytes.restype = C.c_int
+        self.real_bytes = lib.ref_cuda_real_bytes()
         lib.ref_cuda_direct_timed.argtypes = [C.c_size_t] + [_dp] * 4 + [
             C.c_double, C.c_int, _dp, _dp, _dp, _dp, _dp]
         lib.ref_cuda_tree_timed.argtypes = [C.c_size_t] + [_dp] * 4 + [

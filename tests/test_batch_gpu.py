@@ -52,6 +52,44 @@ def test_every_system_matches_the_fp64_oracle(b200, restatement):
     assert pairs == sum(int(n) * (int(n) - 1) for n in sizes) and evals == 1
 
 
+@pytest.fixture(scope="module")
+def full_range(restatement):
+    """The batched configuration's whole size range, [256, 16384]: its two
+    ends, three systems above 8192 (whose sources span 17 to 32 tiles of 512)
+    and log-uniform draws between, each with its own scale radius and
+    softening 0.01 x radius; with the FP64 oracle's accelerations."""
+    from orrery_b200 import initial_conditions as ic
+    rng = np.random.default_rng(41)
+    sizes = np.concatenate([[256, 16384, 12288, 9001],
+                            np.exp(rng.uniform(np.log(256), np.log(16384), 8)).astype(int)])
+    radii = rng.uniform(0.5, 2.0, len(sizes))
+    systems = [ic.plummer_sphere(int(n), scale_radius=float(a), seed=4100 + k)
+               for k, (n, a) in enumerate(zip(sizes, radii))]
+    exact = [restatement.direct(d["x"], d["y"], d["z"], d["m"], 0.01 * radii[k])[0]
+             for k, d in enumerate(systems)]
+    return sizes, radii, systems, exact
+
+
+# Default items (a whole system's sources each) and chunked items of 4 and 8
+# source tiles, whose partial sums batch_reduce_kernel adds in chunk order.
+@pytest.mark.parametrize("shape", [None, (256, 4, 4, 8), (128, 2, 8, 4)])
+def test_the_full_size_range_matches_the_fp64_oracle(b200, full_range, shape):
+    sizes, radii, systems, exact = full_range
+    assert sizes.min() == 256 and sizes.max() == 16384 and (sizes > 8192).sum() >= 3
+    batch = b200.DeviceBatch(sizes, 0.01 * radii)
+    if shape is not None:
+        batch.set_shape(*shape)
+    for k, d in enumerate(systems):
+        batch.set_state(k, d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+    batch.refresh()
+    for k in range(len(systems)):
+        st = batch.state(k)
+        a = np.stack([st["ax"], st["ay"], st["az"]], axis=1)
+        err = relative_errors(a, exact[k])
+        assert err.max() < SPLIT_WORST, (k, int(sizes[k]), err.max())
+        assert np.median(err) < SPLIT_MEDIAN, (k, int(sizes[k]))
+
+
 @pytest.mark.parametrize("shape", [(128, 2, 0), (128, 2, 4), (128, 4, 1), (256, 2, 0),
                                    (256, 4, 2), (128, 2, 0, 4), (256, 2, 4, 8), (256, 4, 0, 4),
                                    (256, 4, 2, 8)])
