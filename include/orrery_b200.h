@@ -516,6 +516,26 @@ int ob_probe_fp32x2(double *ffma2_flop_lanes_per_s);
  * denominator of the FP64 (parity-mode) tree walk's roofline. */
 int ob_probe_fp64(double *dfma_lane_per_s);
 
+/* ------------------------------------------------------------------------ */
+/* Test support: failure paths driven without faulting the device            */
+/* ------------------------------------------------------------------------ */
+/* Runs one onesweep radix-sort pass over n (<= 2^24) synthetic keys with its
+ * own buffers, its tiles polling a predecessor's look-back word at most
+ * poll_limit times. With skip_first_tile nonzero no CTA takes the first tile,
+ * whose words therefore are never published: the waits run out, the pass sets
+ * its timeout bit and OB_ERROR_TIMEOUT is returned, the device staying usable.
+ * Otherwise the pass must complete and sort (OB_OK). Exercises the bounded
+ * look-back wait of the Morton ordering; no reference counterpart. */
+int ob_test_lookback_timeout(uint64_t n, uint32_t poll_limit, int skip_first_tile);
+
+/* Bounds the FP32 tree walk's per-warp traversal stack of `solver` to `cap`
+ * entries (0 restores the full 320) from its next evaluation on. A warp whose
+ * stack fills discards its partial sums and finishes with the per-target
+ * union walk (the fallback a valid tree rarely needs); a small cap forces it,
+ * so tests can hold that path to the oracle. OB_ERROR_UNSUPPORTED for direct
+ * or FP64 solvers. No reference counterpart. */
+int ob_test_set_walk_stack_cap(ob_solver *solver, uint32_t cap);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,6 +14,7 @@
 #include "output.hpp"
 #include "system.hpp"
 #include "tree.hpp"
+#include "tree_kernels.hpp"
 
 namespace ob {
 
@@ -657,6 +658,18 @@ int ob_solver_timings(const ob_solver *solver, ob_timings *timings) {
     return guarded([&] {
         require(solver != nullptr && timings != nullptr, "NULL argument");
         *timings = solver->impl->timings();
+    });
+}
+
+int ob_test_set_walk_stack_cap(ob_solver *solver, uint32_t cap) {
+    return guarded([&] {
+        require(solver != nullptr, "solver is NULL");
+        require(cap <= ob::walk_stack_capacity(), "stack cap above the walk's capacity");
+        const ob_solver_params &p = solver->impl->params();
+        if (p.kind != OB_SOLVER_TREE || p.precision == OB_PRECISION_FP64) {
+            throw ob::Error(OB_ERROR_UNSUPPORTED, "the stack cap applies to the FP32 tree walk");
+        }
+        solver->impl->tree().set_walk_stack_cap(cap);
     });
 }
 

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kSortThreads)
                     const uint32_t *__restrict__ vals_in, unsigned long long *keys_out,
                     uint32_t *vals_out, uint32_t n, uint32_t shift,
                     const uint32_t *__restrict__ offsets, uint32_t *lookback, uint32_t *ticket,
-                    unsigned *status) {
+                    unsigned *status, uint32_t poll_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long *s_keys = reinterpret_cast<unsigned long long *>(smem);
     uint32_t *s_vals = reinterpret_cast<uint32_t *>(s_keys + kSortTile);
@@ -307,7 +307,7 @@ __global__ void __launch_bounds__(kSortThreads)
             const uint32_t s = load_volatile(lookback + static_cast<size_t>(j) * kRadix + d);
             const uint32_t flag = s & ~kCountMask;
             if (flag == 0u) {
-                if (++polls > kSpinLimit) {
+                if (++polls > poll_limit) {
                     atomicOr(status, kStatusTimeout);
                     ok = false;
                     break;
@@ -488,7 +488,9 @@ cudaError_t launch_scan_histograms(uint32_t *hist, cudaStream_t stream) {
 cudaError_t launch_onesweep(const unsigned long long *keys_in, const uint32_t *vals_in,
                             unsigned long long *keys_out, uint32_t *vals_out, uint32_t n,
                             int pass, const uint32_t *offsets, uint32_t *lookback,
-                            uint32_t *ticket, unsigned *status, cudaStream_t stream) {
+                            uint32_t *ticket, unsigned *status, cudaStream_t stream,
+                            uint32_t poll_limit) {
+    static_assert(kLookbackPollLimit == kSpinLimit, "one bound for every device wait");
     static std::atomic<uint64_t> configured{0};
     const cudaError_t err = set_smem_limit_once(reinterpret_cast<const void *>(onesweep_kernel),
                                                 static_cast<int>(onesweep_smem()), configured);
@@ -497,7 +499,7 @@ cudaError_t launch_onesweep(const unsigned long long *keys_in, const uint32_t *v
     }
     onesweep_kernel<<<sort_tiles(n), kSortThreads, onesweep_smem(), stream>>>(
         keys_in, vals_in, keys_out, vals_out, n, static_cast<uint32_t>(kRadixBits * pass),
-        offsets + pass * kRadix, lookback, ticket, status);
+        offsets + pass * kRadix, lookback, ticket, status, poll_limit);
     return cudaGetLastError();
 }
 

@@ -281,9 +281,13 @@ __device__ __forceinline__ uint32_t next_child(const DeviceNode *nodes, uint32_t
     return next > child ? next : stop;
 }
 
-// Writes the walk's compact record of node k (see WalkNode).
+// Writes the walk's compact record of node k (see WalkNode). `sibling`: the
+// node has a next sibling, i.e. its escape index lies inside its parent's
+// subtree (carried in the top bit of the count word).
 __device__ void store_walk_node(WalkNode *walk, uint32_t *first_of, uint32_t k,
-                                const DeviceNode &node, const DeviceQuadrupole *q) {
+                                const DeviceNode &node, const DeviceQuadrupole *q,
+                                bool sibling) {
+    const uint32_t count_word = node.count | (sibling ? kWalkSiblingBit : 0u);
     const float hx = __double2float_rn(node.com_x);
     const float hy = __double2float_rn(node.com_y);
     const float hz = __double2float_rn(node.com_z);
@@ -297,10 +301,10 @@ __device__ void store_walk_node(WalkNode *walk, uint32_t *first_of, uint32_t k,
         w.c = make_float4(__double2float_rn(q->xx), __double2float_rn(q->xy),
                           __double2float_rn(q->xz), __double2float_rn(q->yy));
         w.d = make_float4(__double2float_rn(q->yz), __double2float_rn(q->zz),
-                          __uint_as_float(node.next), __uint_as_float(node.count));
+                          __uint_as_float(node.next), __uint_as_float(count_word));
     } else {
         w.c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        w.d = make_float4(0.0f, 0.0f, __uint_as_float(node.next), __uint_as_float(node.count));
+        w.d = make_float4(0.0f, 0.0f, __uint_as_float(node.next), __uint_as_float(count_word));
     }
     walk[k] = w;
     first_of[k] = node.first;
@@ -364,7 +368,12 @@ __global__ void __launch_bounds__(kThreads)
         if (with_quads) {
             quads[k] = q;
         }
-        store_walk_node(walk, first_of, k, nodes[k], with_quads ? &q : nullptr);
+        {
+            // Escape indices and parents were written by the layout kernel.
+            const uint32_t up = nodes[k].parent;
+            const bool sibling = up != k && nodes[k].next < nodes[up].next;
+            store_walk_node(walk, first_of, k, nodes[k], with_quads ? &q : nullptr, sibling);
+        }
 
         // Climb while this thread completes its parent (gather_moments,
         // octree.cpp:142-185). A cell has at most 22 ancestors.
@@ -444,7 +453,9 @@ __global__ void __launch_bounds__(kThreads)
                 copy.count = 0;
                 copy.first = pfirst;
                 const DeviceQuadrupole *pq = with_quads ? &quads[parent] : nullptr;
-                store_walk_node(walk, first_of, parent, copy, pq);
+                const uint32_t up = __ldcg(&nodes[parent].parent);
+                const bool sibling = up != parent && stop < __ldcg(&nodes[up].next);
+                store_walk_node(walk, first_of, parent, copy, pq, sibling);
             }
             current = parent;
         }
@@ -614,7 +625,7 @@ void TreePipeline::evaluate(uint32_t n, const double *x, const double *y, const 
     check(launch_walk(nodes_.data(), walk_nodes_.data(), first_of_.data(), leaf_rel_.data(),
                       sorted_.data(), perm, n, params_.softening_squared,
                       params_.quadrupole != 0, ax, ay, az, meta_.data(), counters_.data(),
-                      status, stream),
+                      status, stream, walk_stack_cap_),
           "tree walk");
 }
 

@@ -34,12 +34,17 @@ static_assert(sizeof(DeviceNode) == 64, "DeviceNode is four 16-byte words");
 //   a = (com_x hi, com_y hi, com_z hi, mass)       FP32
 //   b = (com_x lo, com_y lo, com_z lo, r2)         FP32 (r2 rounded to nearest)
 //   c = (Qxx, Qxy, Qxz, Qyy)                       FP32 quadrupole
-//   d = (Qyz, Qzz, next, count)                    next/count as uint32 bits
+//   d = (Qyz, Qzz, next, count)                    next/count as uint32 bits;
+//                                                   the top bit of count is set
+//                                                   when the node has a next
+//                                                   sibling (next < parent's next)
 // hi + lo carries each FP64 coordinate to ~2^-48 relative, so offsets to the
 // target (also split) come out in FP32 to ~1e-7 relative without conversions.
 struct alignas(16) WalkNode {
     float4 a, b, c, d;
 };
+constexpr uint32_t kWalkSiblingBit = 0x80000000u;
+constexpr uint32_t kWalkCountMask = 0x7fffffffu;
 static_assert(sizeof(WalkNode) == 64, "WalkNode is four 16-byte words");
 
 // Traceless quadrupole (include/orrery/solvers/octree.hpp:89-96).
@@ -91,6 +96,11 @@ public:
     // Raises the node capacity used from the next evaluation on.
     void grow_nodes(uint32_t at_least);
 
+    // Bounds the walk's per-warp traversal stack (0 = its full capacity) from
+    // the next evaluation on; a warp whose stack fills finishes with the
+    // per-target union walk. For tests of that fallback.
+    void set_walk_stack_cap(uint32_t cap) noexcept { walk_stack_cap_ = cap; }
+
     // The device scalars of the last evaluation (synchronous).
     TreeMeta meta();
 
@@ -108,6 +118,7 @@ private:
     uint32_t grow_to_ = 0;
     uint64_t generation_ = 0;
     uint32_t last_n_ = 0;
+    uint32_t walk_stack_cap_ = 0;
     int sm_count_ = 148;
     DeviceArray<unsigned long long> keys_[2];    // Morton codes (double-buffered)
     DeviceArray<uint32_t> perm_[2];              // particle index payload

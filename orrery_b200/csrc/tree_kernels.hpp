@@ -49,11 +49,15 @@ cudaError_t launch_scan_histograms(uint32_t *hist, cudaStream_t stream);
 
 // One onesweep pass (stable) over digit `pass`. `lookback` holds
 // sort_tiles(n) * kRadix status words for this pass and `ticket` one counter,
-// both zeroed beforehand.
+// both zeroed beforehand. A tile polls a predecessor's look-back word at most
+// `poll_limit` times (the default is far above any legitimate wait); when the
+// polls run out it sets the timeout bit in `status` and returns unscattered.
+constexpr uint32_t kLookbackPollLimit = 1u << 24;
 cudaError_t launch_onesweep(const unsigned long long *keys_in, const uint32_t *vals_in,
                             unsigned long long *keys_out, uint32_t *vals_out, uint32_t n,
                             int pass, const uint32_t *offsets, uint32_t *lookback,
-                            uint32_t *ticket, unsigned *status, cudaStream_t stream);
+                            uint32_t *ticket, unsigned *status, cudaStream_t stream,
+                            uint32_t poll_limit = kLookbackPollLimit);
 
 // sorted[k * n + i] = source_k[perm[i]] for x, y, z, m.
 cudaError_t launch_gather(const double *x, const double *y, const double *z, const double *m,
@@ -89,12 +93,16 @@ cudaError_t launch_moments(const double *sorted, const unsigned long long *codes
 // ------------------------------------------------------------------- walk
 
 // Accelerations written in the caller's (unsorted) order through perm;
-// pair and cell counts added to counters[0] and counters[1].
+// pair and cell counts added to counters[0] and counters[1]. stack_cap (0 =
+// the walk's full per-warp stack) bounds the group traversal's stack; a warp
+// whose stack fills finishes with the per-target union walk.
+uint32_t walk_stack_capacity();
 cudaError_t launch_walk(const DeviceNode *nodes, const WalkNode *walk_nodes,
                         const uint32_t *first_of, const float4 *leaf_rel, const double *sorted,
                         const uint32_t *perm, uint32_t n, double eps2, bool quadrupole,
                         double *ax, double *ay, double *az, TreeMeta *meta,
-                        unsigned long long *counters, unsigned *status, cudaStream_t stream);
+                        unsigned long long *counters, unsigned *status, cudaStream_t stream,
+                        uint32_t stack_cap = 0);
 
 // The FP64 walk of the parity mode (walk_f64.cu); `quads` NULL without
 // quadrupoles; `sorted` = x, y, z, m in Morton order.

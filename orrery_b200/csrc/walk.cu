@@ -10,44 +10,48 @@
 //
 // Group traversal. The warp walks the tree once for its 32 targets, carrying
 // with every node the mask of targets whose own walks reach it (those that
-// opened all its ancestors). A node is classified against the FP64 bounding
-// box of the targets: with d_min / d_max the per-axis distances from the
-// centre of mass to the nearest / farthest box face, computed with the
-// reference's FP64 operations in its order, every target's own |d|^2 lies in
-// [d_min^2, d_max^2] because rounding is monotone, so
-//   d_min^2 >= r2  ->  every target accepts the cell (exactly the reference);
-//   d_max^2 <  r2  ->  every target opens it;
-//   otherwise      ->  mixed: each target decides for itself (an FP32 hi/lo
-//                      test with a 4e-6 relative margin, the reference's FP64
-//                      test inside the margin).
-// Lanes take different nodes of a depth-first stack of (node, reach mask,
-// end of the parent's range) items, 32 per round; an item pushes its next
-// sibling and, when opened, its first child. Accepted cells and opened leaves
-// go to per-warp lists with their target masks, which are evaluated in
-// batches: every lane evaluates every entry for its own target (a lane outside
-// an entry's mask contributes exactly zero), two entries per packed FP32x2
-// instruction, reading the entries as shared-memory broadcasts.
+// opened all its ancestors). Lanes take different nodes of a depth-first
+// stack of (node, reach mask) items, up to 32 per round; an item pushes its
+// next sibling (a bit of the node record says whether it has one) and, when
+// opened, its first child. Each lane classifies its node against the
+// bounding box of the warp's targets from the node's compact record: the
+// per-axis distances from the centre of mass to the nearest and farthest box
+// faces are formed from FP32 hi + lo parts (so each is accurate to a few ulps
+// of itself), and with a 4e-6 relative margin on the acceptance radius
+//   nearest^2 >= r2 (1 + m)  ->  every target accepts the cell,
+//   farthest^2 <  r2 (1 - m)  ->  every target opens it,
+// exactly as the reference's FP64 test decides for each target (every target
+// lies in the box; the margin covers the FP32 error of the distances and of
+// r2). The remaining ("mixed") nodes are decided per target: an FP32 hi/lo
+// test with the same margin, and the reference's FP64 test inside it.
+//
+// The lane that accepts a cell stages it at once in shared memory (centre of
+// mass relative to the box centre G, mass, 2.5 Q, target mask), packed so that
+// one 16-byte load gives two cells' values; an opened leaf is queued with its
+// centre relative to G, its particle range and mask. Batches of cells are then
+// evaluated by every lane for its own target, two cells per packed FP32x2
+// instruction (a lane outside a cell's mask contributes exactly zero), and
+// queued leaves likewise, their sources staged in shared memory per leaf.
 //
 // Arithmetic. Positions and centres of mass are carried as FP32 hi + lo pairs
-// (exact to ~2^-48 relative), so the offset to a cell comes out in FP32 to
-// about 2e-7 relative with no FP64 work. Force terms are FP32, summed in FP32
-// within a batch (or leaf) and flushed into FP64 per-target sums.
+// (exact to ~2^-48 relative); force terms are FP32, summed in FP32 within a
+// batch and flushed into FP64 per-target sums.
 //
-// A round takes no more items than the stack has room to push back, so the
-// stack (160 entries per warp; the 2M collision needs about 120) only stops
-// the traversal if it is completely full; the warp then discards its partial
-// sums and walks its targets with the per-target union walk (union_walk
-// below), which gives the same counts.
+// A round takes no more items than the stack has room to push back (each
+// pushes at most two), so the stack (320 entries per warp; the 2M two-disc
+// collision peaks near 280) only stops the traversal when completely full;
+// the warp then discards its partial sums and walks its targets with the
+// per-target union walk (union_walk below), which gives the same counts.
 //
-// Warp discipline. Between the warp's votes and barriers there is no
+// Warp discipline. Between the warp's votes and barriers there is no long
 // lane-divergent stretch of work: lanes outside a leaf's or cell's mask run
 // the same arithmetic with zero weight, and the FP64 accept test runs on
 // every lane once any lane needs it. (Votes and warp barriers of the same kind
 // may be satisfied by lanes standing at different instructions, so a warp
 // whose lanes spent long, different times in divergent code was seen to fall
-// out of step: lanes of different rounds then shared one vote.) Node and
-// particle indices are checked before every gather; an index out of range
-// (which a valid tree never produces) sets kStatusInvalid and is skipped.
+// out of step.) Node and particle indices are checked before every gather; an
+// index out of range (which a valid tree never produces) sets kStatusInvalid
+// and is skipped.
 #include "common.cuh"
 #include "tree_kernels.hpp"
 
@@ -59,65 +63,61 @@ constexpr int kWalkThreads = kWalkWarps * 32;
 constexpr float kAcceptMargin = 4e-6f;
 constexpr uint32_t kFull = 0xffffffffu;
 
-// Per-warp shared-memory capacities (entries). A round processes at most 32
-// items; each adds at most two stack items (its next sibling and, opened, its
-// first child) and at most one cell or one leaf, so a round of t items adds at
-// most 2t stack items, t cells and t leaves. A round takes at most
-// kStackCap - size items, so the stack cannot overflow while it has room.
+// Per-warp shared-memory capacities (entries). A round takes at most 32 items;
+// each adds at most two stack items (its next sibling and, opened, its first
+// child) and at most one cell or one leaf, so a round of t items adds at most
+// 2t stack items, t cells and t leaves. A round takes at most stack room
+// (capacity - size) items, so the stack cannot overflow while it has room;
+// cells and leaves are evaluated once more than capacity - 32 are queued.
 // Sized so that 8 CTAs of 4 warps fit in an SM's shared memory.
-constexpr uint32_t kStackCap = 160;
-constexpr uint32_t kCellCap = 96;
-constexpr uint32_t kLeafCap = 64;
-
-struct GroupItem {
-    uint32_t node;
-    uint32_t mask; // targets whose walks reach the node
-    uint32_t end;  // end of the parent's subtree: the next sibling exists below it
-};
-
-// Entries staged for a batch of 32 cells (or one leaf chunk), as float4
-// quads of packed pairs: quad f of pair p holds (a_j, a_j+1, b_j, b_j+1) for
-// the two fields a, b of group f and the entries j = 2p, 2p+1, so one 16-byte
-// shared load yields two FP32x2 operands. 17 pairs: an odd count reads one
-// neutral partner past its end.
-//   cells:  (x, y) (z, mass) (target mask bits, 0) (Qxx, Qxy) (Qxz, Qyy)
-//           (Qyz, Qzz), centres relative to the warp's box centre
-//   leaves: (x, y) (z, mass), leaf-relative
-constexpr int kCellQuads = 6;
+constexpr uint32_t kStackCap = 320;
+constexpr uint32_t kCellCap = 48;
+constexpr uint32_t kLeafCap = 40;
+// Staged cell fields, as quads of packed pairs: quad f of pair p holds
+// (a_j, a_j+1, b_j, b_j+1) for the two fields a, b of group f and the cells
+// j = 2p, 2p+1: (x, y) (z, mass) (2.5 Qxx, 2.5 Qxy) (2.5 Qxz, 2.5 Qyy)
+// (2.5 Qyz, 2.5 Qzz), centres relative to the box centre G.
+constexpr int kCellQuads = 5;
+// Leaf sources staged per chunk of 32: (x, y) (z, mass), leaf-relative.
 constexpr int kLeafQuads = 2;
 // Offset given to lanes outside a leaf's mask and to the neutral partner: the
 // terms it produces underflow to exactly zero in FP32.
 constexpr float kFar = 1e18f;
 
 struct __align__(16) WarpSpace {
-    GroupItem stack[kStackCap];
-    GroupItem mixed[32];    // this round's mixed items
-    uint2 cells[kCellCap];  // (node, target mask)
-    uint2 leaves[kLeafCap]; // (node, target mask)
-    union {                 // used one at a time
-        float4 cell_quads[kCellQuads][17];
-        float4 leaf_pos[kLeafCap]; // queued leaves: centre - G (FP32), particle count bits
-        float4 union_staged[32];   // the union walk's leaf staging (after a fallback)
+    float4 cells[kCellQuads][kCellCap / 2 + 1]; // +1: the neutral partner of an odd count
+    uint32_t cell_mask[kCellCap + 2];
+    float4 leaf_pos[kLeafCap];  // leaf centre of mass - G (FP32), particle count bits
+    uint2 leaf_meta[kLeafCap];  // (first particle | may-hold-a-target bit, target mask)
+    uint2 stack[kStackCap];     // (node, reach mask)
+    uint2 mixed[32];            // this round's mixed items
+    union {                     // used one at a time
+        float4 leaf_quads[kLeafQuads][17];
+        float4 union_staged[32]; // the union walk's leaf staging (after a fallback)
     };
-    float4 leaf_quads[kLeafQuads][17];
-    double box[9]; // lo xyz, hi xyz and centre G of the warp's targets (FP64)
+    // Box of the warp's targets as FP32 hi + lo parts: lo hi, lo lo, hi hi,
+    // hi lo; then the box centre G hi, G lo (x, y, z; w unused).
+    float4 box[6];
 };
 
-// Writes entry j's two fields a, b into quad array q (see cell_quads).
-__device__ __forceinline__ void put(float4 *q, uint32_t j, float a, float b) {
-    float4 &slot = q[j >> 1];
-    if (j & 1u) {
-        slot.y = a;
-        slot.w = b;
-    } else {
-        slot.x = a;
-        slot.z = b;
-    }
-}
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 __device__ __forceinline__ uint32_t warp_min(uint32_t v) { return __reduce_min_sync(kFull, v); }
 
 __device__ __forceinline__ uint32_t lanes_below(uint32_t lane) { return (1u << lane) - 1u; }
+
+// Writes fields (a, b) of staged entry j into quad array q (see kCellQuads).
+__device__ __forceinline__ void put(float4 *q, uint32_t j, float a, float b) {
+    float *slot = reinterpret_cast<float *>(&q[j >> 1]) + (j & 1u);
+    slot[0] = a;
+    slot[2] = b;
+}
+
+// Splits an FP64 value into FP32 hi + lo with hi + lo = v to ~2^-48.
+__device__ __forceinline__ void split(double v, float &hi, float &lo) {
+    hi = __double2float_rn(v);
+    lo = __double2float_rn(v - static_cast<double>(hi));
+}
 
 // The reference's accept test in FP64 (tree_walk.cpp:44-46), for cells whose
 // FP32 test fell inside the margin.
@@ -179,7 +179,7 @@ __device__ void union_walk(const DeviceNode *__restrict__ nodes,
         const float4 B = walk[cur].b;
         const float4 D = walk[cur].d;
         const uint32_t next = __float_as_uint(D.z);
-        const uint32_t count = __float_as_uint(D.w);
+        const uint32_t count = __float_as_uint(D.w) & kWalkCountMask;
         bool open_leaf = false;
         float dx = 0.0f, dy = 0.0f, dz = 0.0f;
         if (cursor == cur) {
@@ -259,162 +259,127 @@ __device__ void union_walk(const DeviceNode *__restrict__ nodes,
     acc_z += static_cast<double>(cz32);
 }
 
-__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-// Evaluates the warp's cell list: every lane sums every cell for its target
-// (zero outside the cell's mask), two cells per FP32x2 instruction. Cell
-// centres are staged relative to the warp's box centre G (rounded to FP32
-// once, from FP64), and each lane holds its target relative to G, so the
-// offset to a cell is one subtraction; both are within the box's reach of the
-// cell, so the offset keeps about FP32 relative accuracy.
+// A node's centre of mass relative to the box centre G, from hi + lo parts.
+__device__ __forceinline__ float3 centre_rel(const float4 A, const float4 B, const float4 Gh,
+                                             const float4 Gl) {
+    return make_float3((A.x - Gh.x) + (B.x - Gl.x), (A.y - Gh.y) + (B.y - Gl.y),
+                       (A.z - Gh.z) + (B.z - Gl.z));
+}
+
+// Stages accepted cell j: centre relative to G, mass, 2.5 Q and target mask.
 template <bool QUAD>
-__device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count,
-                                            const DeviceNode *__restrict__ nodes,
-                                            const WalkNode *__restrict__ walk, float2 ntx,
-                                            float2 nty,
-                                            float2 ntz, float2 eps2, uint32_t lane_bit,
-                                            double &acc_x, double &acc_y, double &acc_z,
-                                            uint32_t node_count,
-                                            unsigned *status) {
-    const uint32_t lane = threadIdx.x & 31u;
-    float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
-    for (uint32_t base = 0; base < count; base += 32) {
-        const uint32_t chunk = min(32u, count - base);
-        float4(*cq)[17] = ws.cell_quads;
-        if (lane < chunk) {
-            uint2 e = ws.cells[base + lane];
-            if (e.x >= node_count) {
-                atomicOr(status, kStatusInvalid);
-                e = make_uint2(0u, 0u); // no target: contributes nothing
-            }
-            const DeviceNode *nd = nodes + e.x;
-            const float cx = __double2float_rn(nd->com_x - ws.box[6]);
-            const float cy = __double2float_rn(nd->com_y - ws.box[7]);
-            const float cz = __double2float_rn(nd->com_z - ws.box[8]);
-            const float m = walk[e.x].a.w;
-            put(cq[0], lane, cx, cy);
-            put(cq[1], lane, cz, m);
-            put(cq[2], lane, __uint_as_float(e.y), 0.0f);
-            if (QUAD) {
-                // Staged as 2.5 Q: the loop needs 2.5 (d.Q d) and Q d.
-                const float4 C = walk[e.x].c; // (xx, xy, xz, yy)
-                const float4 D = walk[e.x].d; // (yz, zz, next, count)
-                put(cq[3], lane, 2.5f * C.x, 2.5f * C.y);
-                put(cq[4], lane, 2.5f * C.z, 2.5f * C.w);
-                put(cq[5], lane, 2.5f * D.x, 2.5f * D.y);
-            }
-        } else if (lane == chunk) {
-            // The odd entry's partner: no target, zero mass, at G.
-            for (int q = 0; q < kCellQuads; ++q) {
-                put(cq[q], lane, 0.0f, 0.0f);
-            }
-        }
-        __syncwarp();
-        for (uint32_t j = 0; j < chunk; j += 2) {
-            const uint32_t p = j >> 1;
-            const float4 q0 = cq[0][p], q1 = cq[1][p], q2 = cq[2][p];
-            const float2 dx = __fadd2_rn(f2(q0.x, q0.y), ntx);
-            const float2 dy = __fadd2_rn(f2(q0.z, q0.w), nty);
-            const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
-            const bool in0 = (__float_as_uint(q2.x) & lane_bit) != 0u;
-            const bool in1 = (__float_as_uint(q2.y) & lane_bit) != 0u;
-            const float2 r2e =
-                __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
-            const float inv0 = rsqrt_approx(r2e.x);
-            const float inv1 = rsqrt_approx(r2e.y);
-            const float2 inv = f2(in0 ? inv0 : 0.0f, in1 ? inv1 : 0.0f);
-            const float2 inv2 = __fmul2_rn(inv, inv);
-            // Monopole m d / r^3 (tree_walk.hpp:129-140).
-            float2 coef = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
-            if (QUAD) {
-                // Quadrupole -Q d / r^5 + 2.5 (d.Q d) d / r^7 (tree_walk.hpp:142-181),
-                // folded with the monopole: d (m / r^3 + 2.5 (d.Q d) / r^7) - Q d / r^5.
-                const float4 q3 = cq[3][p], q4 = cq[4][p], q5 = cq[5][p];
-                const float2 xx = f2(q3.x, q3.y), xy = f2(q3.z, q3.w);
-                const float2 xz = f2(q4.x, q4.y), yy = f2(q4.z, q4.w);
-                const float2 yz = f2(q5.x, q5.y), zz = f2(q5.z, q5.w);
-                const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
-                const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
-                const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
-                // q = 2.5 Q d, quadratic = 2.5 d.Q d.
-                const float2 quadratic =
-                    __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
-                const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
-                coef = __ffma2_rn(quadratic, __fmul2_rn(inv5, inv2), coef);
-                const float2 ninv5 = __fmul2_rn(inv5, f2(-0.4f, -0.4f));
-                sx = __ffma2_rn(qx, ninv5, sx);
-                sy = __ffma2_rn(qy, ninv5, sy);
-                sz = __ffma2_rn(qz, ninv5, sz);
-            }
-            sx = __ffma2_rn(dx, coef, sx);
-            sy = __ffma2_rn(dy, coef, sy);
-            sz = __ffma2_rn(dz, coef, sz);
-        }
-        __syncwarp();
+__device__ __forceinline__ void stage_cell(WarpSpace &ws, uint32_t j, float3 c, float m,
+                                           uint32_t mask, const float4 C, const float4 D) {
+    put(ws.cells[0], j, c.x, c.y);
+    put(ws.cells[1], j, c.z, m);
+    if (QUAD) {
+        put(ws.cells[2], j, 2.5f * C.x, 2.5f * C.y);
+        put(ws.cells[3], j, 2.5f * C.z, 2.5f * C.w);
+        put(ws.cells[4], j, 2.5f * D.x, 2.5f * D.y);
     }
+    ws.cell_mask[j] = mask;
+}
+
+// Queues opened leaf k: centre relative to G, size, first particle (with a
+// bit when its range may hold one of the warp's targets) and target mask.
+__device__ __forceinline__ void queue_leaf(WarpSpace &ws, uint32_t k, float3 c, uint32_t size,
+                                           uint32_t first, uint32_t mask, uint32_t warp_first,
+                                           uint32_t warp_end) {
+    const bool holds = first < warp_end && first + size > warp_first;
+    ws.leaf_pos[k] = make_float4(c.x, c.y, c.z, __uint_as_float(size));
+    ws.leaf_meta[k] = make_uint2(first | (holds ? 0x80000000u : 0u), mask);
+}
+
+// A leaf's first particle and size, checked against the particle count.
+__device__ __forceinline__ void leaf_range(const uint32_t *first_of, uint32_t v, uint32_t count,
+                                           uint32_t n, unsigned *status, uint32_t &first,
+                                           uint32_t &size) {
+    first = first_of[v];
+    size = count;
+    if (first > n || size > n - first) {
+        atomicOr(status, kStatusInvalid);
+        first = 0u;
+        size = 0u;
+    }
+}
+
+// Evaluates the staged cells: every lane sums every cell for its target (zero
+// outside the cell's mask), two cells per FP32x2 instruction. Each lane holds
+// its target relative to G, so the offset to a cell is one subtraction.
+template <bool QUAD>
+__device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count, float2 ntx, float2 nty,
+                                            float2 ntz, float2 eps2, uint32_t lane_bit,
+                                            double &acc_x, double &acc_y, double &acc_z) {
+    const uint32_t lane = threadIdx.x & 31u;
+    if ((count & 1u) != 0u && lane == 0) {
+        // The odd entry's partner: no target, zero mass, at G.
+        for (int q = 0; q < kCellQuads; ++q) {
+            put(ws.cells[q], count, 0.0f, 0.0f);
+        }
+        ws.cell_mask[count] = 0u;
+    }
+    __syncwarp();
+    float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
+    for (uint32_t j = 0; j < count; j += 2) {
+        const uint32_t p = j >> 1;
+        const float4 q0 = ws.cells[0][p], q1 = ws.cells[1][p];
+        const uint2 masks = *reinterpret_cast<const uint2 *>(&ws.cell_mask[j]);
+        const float2 dx = __fadd2_rn(f2(q0.x, q0.y), ntx);
+        const float2 dy = __fadd2_rn(f2(q0.z, q0.w), nty);
+        const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
+        const float2 r2e = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
+        const float inv0 = rsqrt_approx(r2e.x);
+        const float inv1 = rsqrt_approx(r2e.y);
+        const float2 inv = f2((masks.x & lane_bit) != 0u ? inv0 : 0.0f,
+                              (masks.y & lane_bit) != 0u ? inv1 : 0.0f);
+        const float2 inv2 = __fmul2_rn(inv, inv);
+        // Monopole m d / r^3 (tree_walk.hpp:129-140).
+        float2 coef = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
+        if (QUAD) {
+            // Quadrupole -Q d / r^5 + 2.5 (d.Q d) d / r^7 (tree_walk.hpp:142-181),
+            // folded with the monopole: d (m / r^3 + 2.5 (d.Q d) / r^7) - Q d / r^5.
+            const float4 q2 = ws.cells[2][p], q3 = ws.cells[3][p], q4 = ws.cells[4][p];
+            const float2 xx = f2(q2.x, q2.y), xy = f2(q2.z, q2.w);
+            const float2 xz = f2(q3.x, q3.y), yy = f2(q3.z, q3.w);
+            const float2 yz = f2(q4.x, q4.y), zz = f2(q4.z, q4.w);
+            const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
+            const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
+            const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
+            // q = 2.5 Q d, quadratic = 2.5 d.Q d.
+            const float2 quadratic = __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
+            const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
+            coef = __ffma2_rn(quadratic, __fmul2_rn(inv5, inv2), coef);
+            const float2 ninv5 = __fmul2_rn(inv5, f2(-0.4f, -0.4f));
+            sx = __ffma2_rn(qx, ninv5, sx);
+            sy = __ffma2_rn(qy, ninv5, sy);
+            sz = __ffma2_rn(qz, ninv5, sz);
+        }
+        sx = __ffma2_rn(dx, coef, sx);
+        sy = __ffma2_rn(dy, coef, sy);
+        sz = __ffma2_rn(dz, coef, sz);
+    }
+    __syncwarp();
     acc_x += static_cast<double>(sx.x) + static_cast<double>(sx.y);
     acc_y += static_cast<double>(sy.x) + static_cast<double>(sy.y);
     acc_z += static_cast<double>(sz.x) + static_cast<double>(sz.y);
 }
 
-// Evaluates the warp's leaf list: for each opened leaf, every lane sums its
-// particles for its own target (staged in shared memory once per chunk of 32;
-// lanes outside the leaf's mask sit far away and add exactly zero), two
-// sources per FP32x2 instruction, skipping the target itself. First, one
-// lane per queued leaf reads its particle range and centre of mass and stores
-// the centre relative to the warp's box centre G, and whether the leaf's range
-// can hold one of the warp's targets (the only leaves that need the
-// self-skip); each leaf then costs its offset (three subtractions) and its
-// sources.
+// Evaluates the queued leaves: for each, every lane sums its particles for its
+// own target (staged in shared memory once per chunk of 32; lanes outside the
+// leaf's mask sit far away and add exactly zero), two sources per FP32x2
+// instruction, skipping the target itself where the leaf's range may hold it.
 __device__ __forceinline__ void flush_leaves(WarpSpace &ws, uint32_t count,
-                                             const DeviceNode *__restrict__ nodes,
-                                             const WalkNode *__restrict__ walk,
-                                             const uint32_t *__restrict__ first_of,
                                              const float4 *__restrict__ leaf_rel, float tgx,
                                              float tgy, float tgz, float eps2, uint32_t i,
-                                             uint32_t warp_first, uint32_t lane_bit,
-                                             double &acc_x, double &acc_y, double &acc_z,
-                                             uint32_t &pairs, uint32_t node_count, uint32_t n,
-                                             unsigned *status) {
+                                             uint32_t lane_bit, double &acc_x, double &acc_y,
+                                             double &acc_z, uint32_t &pairs) {
     const uint32_t lane = threadIdx.x & 31u;
     const float2 e2 = f2(eps2, eps2);
-    const uint32_t warp_end = min(warp_first + 32u, n);
-    // Per-leaf metadata, one leaf per lane: ws.leaf_pos[k] = (centre - G,
-    // count bits); ws.leaves[k].x = first particle, bit 31 set when the leaf
-    // may hold one of the warp's targets.
-    for (uint32_t base = 0; base < count; base += 32) {
-        const uint32_t k = base + lane;
-        if (k < count) {
-            const uint2 e = ws.leaves[k];
-            uint32_t size = 0u, first = 0u;
-            float4 pos = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (e.x < node_count) {
-                size = __float_as_uint(walk[e.x].d.w);
-                first = first_of[e.x];
-                if (first > n || size > n - first) {
-                    atomicOr(status, kStatusInvalid);
-                    size = 0u;
-                }
-                const DeviceNode *nd = nodes + e.x;
-                pos.x = __double2float_rn(nd->com_x - ws.box[6]);
-                pos.y = __double2float_rn(nd->com_y - ws.box[7]);
-                pos.z = __double2float_rn(nd->com_z - ws.box[8]);
-            } else {
-                atomicOr(status, kStatusInvalid);
-            }
-            pos.w = __uint_as_float(size);
-            const bool holds = first < warp_end && first + size > warp_first;
-            ws.leaf_pos[k] = pos;
-            ws.leaves[k].x = first | (holds ? 0x80000000u : 0u);
-        }
-    }
-    __syncwarp();
-    // FP32 sums over the batch's leaves (lanes outside a leaf's mask add
-    // exactly zero), folded into FP64 once per batch like the cell sums.
     float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
     for (uint32_t k = 0; k < count; ++k) {
         const float4 pos = ws.leaf_pos[k];
-        const uint2 e = ws.leaves[k];
+        const uint2 e = ws.leaf_meta[k];
         const uint32_t size = __float_as_uint(pos.w);
         const uint32_t first = e.x & 0x7fffffffu;
         const bool masked = (e.x >> 31) != 0u; // uniform: every lane reads the same entry
@@ -492,7 +457,7 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
                 const uint32_t *__restrict__ first_of, const float4 *__restrict__ leaf_rel,
                 const double *__restrict__ sorted, const uint32_t *__restrict__ perm, uint32_t n,
                 float eps2, double *ax, double *ay, double *az, const TreeMeta *meta,
-                unsigned long long *counters, unsigned *status) {
+                unsigned long long *counters, unsigned *status, uint32_t stack_cap) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t warp = threadIdx.x >> 5;
@@ -505,6 +470,8 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
     }
     const uint32_t node_count = meta->node_count;
     const uint32_t lane_bit = 1u << lane;
+    const uint32_t warp_first = i - lane;
+    const uint32_t warp_end = min(warp_first + 32u, n);
 
     double X = 0.0, Y = 0.0, Z = 0.0;
     float pxh = 0.0f, pyh = 0.0f, pzh = 0.0f, pxl = 0.0f, pyl = 0.0f, pzl = 0.0f;
@@ -512,12 +479,9 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         X = sorted[i];
         Y = sorted[static_cast<size_t>(n) + i];
         Z = sorted[2ull * n + i];
-        pxh = __double2float_rn(X);
-        pyh = __double2float_rn(Y);
-        pzh = __double2float_rn(Z);
-        pxl = __double2float_rn(X - static_cast<double>(pxh));
-        pyl = __double2float_rn(Y - static_cast<double>(pyh));
-        pzl = __double2float_rn(Z - static_cast<double>(pzh));
+        split(X, pxh, pxl);
+        split(Y, pyh, pyl);
+        split(Z, pzh, pzl);
     }
     const float2 eps2v = f2(eps2, eps2);
 
@@ -539,16 +503,18 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
     const float tgx = __double2float_rn(X - gcx), tgy = __double2float_rn(Y - gcy),
                 tgz = __double2float_rn(Z - gcz);
     const float2 ntx = f2(-tgx, -tgx), nty = f2(-tgy, -tgy), ntz = f2(-tgz, -tgz);
-    if (lane == 0) {
-        ws.box[0] = lox;
-        ws.box[1] = loy;
-        ws.box[2] = loz;
-        ws.box[3] = hix;
-        ws.box[4] = hiy;
-        ws.box[5] = hiz;
-        ws.box[6] = gcx;
-        ws.box[7] = gcy;
-        ws.box[8] = gcz;
+    if (lane < 6) {
+        // Lanes 0-5 split one box value each: lo, hi, G (x, y, z).
+        const double v[3] = {lane < 2 ? lox : lane < 4 ? hix : gcx,
+                             lane < 2 ? loy : lane < 4 ? hiy : gcy,
+                             lane < 2 ? loz : lane < 4 ? hiz : gcz};
+        float h[3], l[3];
+        for (int a = 0; a < 3; ++a) {
+            split(v[a], h[a], l[a]);
+        }
+        // Slots: 0 lo hi, 1 lo lo, 2 hi hi, 3 hi lo, 4 G hi, 5 G lo.
+        ws.box[lane] = (lane & 1u) == 0u ? make_float4(h[0], h[1], h[2], 0.0f)
+                                          : make_float4(l[0], l[1], l[2], 0.0f);
     }
     __syncwarp();
 
@@ -558,12 +524,12 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
     bool overflow = false;
     uint32_t rounds = 0;
     if (lane == 0) {
-        ws.stack[0] = GroupItem{0u, live, node_count};
+        ws.stack[0] = make_uint2(0u, live);
     }
     __syncwarp();
     while (size > 0) {
-        // Popping t items and pushing up to 2t needs size + t <= kStackCap.
-        const uint32_t take = min(min(size, 32u), kStackCap - min(size, kStackCap));
+        // Popping t items and pushing up to 2t needs size + t <= stack_cap.
+        const uint32_t take = min(min(size, 32u), stack_cap - min(size, stack_cap));
         // A valid tree visits each node at most once, so more rounds than
         // nodes (or a full stack) hands the warp to the union walk, whose
         // cursors only move forward.
@@ -573,41 +539,45 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         }
         size -= take;
         const bool has = lane < take;
-        GroupItem item{0u, 0u, 0u};
+        uint2 item = make_uint2(0u, 0u);
         if (has) {
             item = ws.stack[size + lane];
-            if (item.node >= node_count) {
+            if (item.x >= node_count) {
                 atomicOr(status, kStatusInvalid);
-                item.node = node_count; // skipped below
+                item.x = node_count; // skipped below
             }
         }
         __syncwarp();
 
-        // Classify the lane's node against the box (FP64, the reference's
-        // operations and order).
+        // Classify the lane's node against the box from its compact record.
         bool sibling = false, child = false, cell = false, leaf = false, mixed = false;
-        uint32_t next = 0;
-        if (has && item.node < node_count) {
-            const DeviceNode *nd = nodes + item.node;
-            const double cx = nd->com_x, cy = nd->com_y, cz = nd->com_z, r2 = nd->r2;
-            next = nd->next;
-            const uint32_t count = nd->count;
-            sibling = next < item.end;
-            const double lox = ws.box[0], loy = ws.box[1], loz = ws.box[2];
-            const double hix = ws.box[3], hiy = ws.box[4], hiz = ws.box[5];
-            const double nx = fmax(fmax(__dsub_rn(lox, cx), __dsub_rn(cx, hix)), 0.0);
-            const double ny = fmax(fmax(__dsub_rn(loy, cy), __dsub_rn(cy, hiy)), 0.0);
-            const double nz = fmax(fmax(__dsub_rn(loz, cz), __dsub_rn(cz, hiz)), 0.0);
-            const double near2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(nx, nx), __dmul_rn(ny, ny)), __dmul_rn(nz, nz));
-            const double fx = fmax(fabs(__dsub_rn(cx, lox)), fabs(__dsub_rn(cx, hix)));
-            const double fy = fmax(fabs(__dsub_rn(cy, loy)), fabs(__dsub_rn(cy, hiy)));
-            const double fz = fmax(fabs(__dsub_rn(cz, loz)), fabs(__dsub_rn(cz, hiz)));
-            const double far2 =
-                __dadd_rn(__dadd_rn(__dmul_rn(fx, fx), __dmul_rn(fy, fy)), __dmul_rn(fz, fz));
-            if (near2 >= r2) {
+        uint32_t next = 0, count = 0;
+        float4 A = make_float4(0.0f, 0.0f, 0.0f, 0.0f), B = A, D = A;
+        if (has && item.x < node_count) {
+            A = walk[item.x].a;
+            B = walk[item.x].b;
+            D = walk[item.x].d;
+            next = __float_as_uint(D.z);
+            const uint32_t word = __float_as_uint(D.w);
+            count = word & kWalkCountMask;
+            sibling = (word & kWalkSiblingBit) != 0u;
+            const float4 loh = ws.box[0], lol = ws.box[1], hih = ws.box[2], hil = ws.box[3];
+            // Signed distances lo - c and c - hi per axis, from hi + lo parts.
+            const float lx = (loh.x - A.x) + (lol.x - B.x), ux = (A.x - hih.x) + (B.x - hil.x);
+            const float ly = (loh.y - A.y) + (lol.y - B.y), uy = (A.y - hih.y) + (B.y - hil.y);
+            const float lz = (loh.z - A.z) + (lol.z - B.z), uz = (A.z - hih.z) + (B.z - hil.z);
+            const float nx = fmaxf(fmaxf(lx, ux), 0.0f);
+            const float ny = fmaxf(fmaxf(ly, uy), 0.0f);
+            const float nz = fmaxf(fmaxf(lz, uz), 0.0f);
+            const float fx = fmaxf(fabsf(lx), fabsf(ux));
+            const float fy = fmaxf(fabsf(ly), fabsf(uy));
+            const float fz = fmaxf(fabsf(lz), fabsf(uz));
+            const float near2 = fmaf(nz, nz, fmaf(ny, ny, nx * nx));
+            const float far2 = fmaf(fz, fz, fmaf(fy, fy, fx * fx));
+            const float r2 = B.w;
+            if (near2 >= r2 * (1.0f + kAcceptMargin) && r2 > 1e-30f) {
                 cell = true;
-            } else if (far2 < r2) {
+            } else if (far2 < r2 * (1.0f - kAcceptMargin)) {
                 leaf = count > 0;
                 child = count == 0;
             } else {
@@ -618,23 +588,32 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         const uint32_t bs = __ballot_sync(kFull, sibling);
         const uint32_t bc = __ballot_sync(kFull, child);
         if (sibling) {
-            ws.stack[size + __popc(bs & below)] = GroupItem{next, item.mask, item.end};
+            ws.stack[size + __popc(bs & below)] = make_uint2(next, item.y);
         }
         if (child) {
-            ws.stack[size + __popc(bs) + __popc(bc & below)] =
-                GroupItem{item.node + 1u, item.mask, next};
+            ws.stack[size + __popc(bs) + __popc(bc & below)] = make_uint2(item.x + 1u, item.y);
         }
         size += __popc(bs) + __popc(bc);
         const uint32_t ba = __ballot_sync(kFull, cell);
-        if (cell) {
-            ws.cells[ncell + __popc(ba & below)] = make_uint2(item.node, item.mask);
-            cells += __popc(item.mask); // every target of the mask takes the cell
+        const uint32_t bl = __ballot_sync(kFull, leaf);
+        if (cell || leaf) {
+            const float4 Gh = ws.box[4], Gl = ws.box[5];
+            const float3 c = centre_rel(A, B, Gh, Gl);
+            if (cell) {
+                float4 C = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (QUAD) {
+                    C = walk[item.x].c;
+                }
+                stage_cell<QUAD>(ws, ncell + __popc(ba & below), c, A.w, item.y, C, D);
+                cells += __popc(item.y); // every target of the mask takes the cell
+            } else {
+                uint32_t first, lsize;
+                leaf_range(first_of, item.x, count, n, status, first, lsize);
+                queue_leaf(ws, nleaf + __popc(bl & below), c, lsize, first, item.y, warp_first,
+                           warp_end);
+            }
         }
         ncell += __popc(ba);
-        const uint32_t bl = __ballot_sync(kFull, leaf);
-        if (leaf) {
-            ws.leaves[nleaf + __popc(bl & below)] = make_uint2(item.node, item.mask);
-        }
         nleaf += __popc(bl);
 
         // Mixed nodes: each target in the mask decides for itself.
@@ -645,20 +624,20 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         __syncwarp();
         const uint32_t nmixed = __popc(bm);
         for (uint32_t k = 0; k < nmixed; ++k) {
-            const GroupItem mi = ws.mixed[k];
-            const uint32_t v = mi.node;
-            const uint32_t mask = mi.mask;
-            const float4 A = walk[v].a;
-            const float4 B = walk[v].b;
-            const float4 D = walk[v].d;
+            const uint2 mi = ws.mixed[k];
+            const uint32_t v = mi.x;
+            const uint32_t mask = mi.y;
+            const float4 MA = walk[v].a;
+            const float4 MB = walk[v].b;
+            const float4 MD = walk[v].d;
             // FP32 test on every lane; the FP64 test, when any lane of the
             // mask falls inside the margin, on every lane too.
             const bool reach = (mask & lane_bit) != 0u;
-            const float dx = (A.x - pxh) + (B.x - pxl);
-            const float dy = (A.y - pyh) + (B.y - pyl);
-            const float dz = (A.z - pzh) + (B.z - pzl);
+            const float dx = (MA.x - pxh) + (MB.x - pxl);
+            const float dy = (MA.y - pyh) + (MB.y - pyl);
+            const float dz = (MA.z - pzh) + (MB.z - pzl);
             const float d2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-            const float r2 = B.w;
+            const float r2 = MB.w;
             const bool sure_accept = d2 >= r2 * (1.0f + kAcceptMargin) && r2 > 1e-30f;
             const bool sure_open = d2 <= r2 * (1.0f - kAcceptMargin);
             bool accept = reach && sure_accept;
@@ -669,19 +648,27 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
             }
             const uint32_t accepted = __ballot_sync(kFull, accept) & mask;
             const uint32_t opened = mask & ~accepted;
-            const uint32_t vnext = __float_as_uint(D.z);
-            const uint32_t vcount = __float_as_uint(D.w);
+            const uint32_t vcount = __float_as_uint(MD.w) & kWalkCountMask;
             if (lane == 0) {
-                if (accepted != 0u) {
-                    ws.cells[ncell] = make_uint2(v, accepted);
-                    cells += __popc(accepted);
-                }
-                if (opened != 0u) {
-                    if (vcount > 0u) {
-                        ws.leaves[nleaf] = make_uint2(v, opened);
-                    } else {
-                        ws.stack[size] = GroupItem{v + 1u, opened, vnext};
+                if (accepted != 0u || (opened != 0u && vcount > 0u)) {
+                    const float4 Gh = ws.box[4], Gl = ws.box[5];
+                    const float3 c = centre_rel(MA, MB, Gh, Gl);
+                    if (accepted != 0u) {
+                        float4 C = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                        if (QUAD) {
+                            C = walk[v].c;
+                        }
+                        stage_cell<QUAD>(ws, ncell, c, MA.w, accepted, C, MD);
+                        cells += __popc(accepted);
                     }
+                    if (opened != 0u && vcount > 0u) {
+                        uint32_t first, lsize;
+                        leaf_range(first_of, v, vcount, n, status, first, lsize);
+                        queue_leaf(ws, nleaf, c, lsize, first, opened, warp_first, warp_end);
+                    }
+                }
+                if (opened != 0u && vcount == 0u) {
+                    ws.stack[size] = make_uint2(v + 1u, opened);
                 }
             }
             ncell += accepted != 0u ? 1u : 0u;
@@ -695,13 +682,12 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         }
         __syncwarp();
         if (ncell > kCellCap - 32u) {
-            flush_cells<QUAD>(ws, ncell, nodes, walk, ntx, nty, ntz, eps2v,
-                              lane_bit, acc_x, acc_y, acc_z, node_count, status);
+            flush_cells<QUAD>(ws, ncell, ntx, nty, ntz, eps2v, lane_bit, acc_x, acc_y, acc_z);
             ncell = 0;
         }
         if (nleaf > kLeafCap - 32u) {
-            flush_leaves(ws, nleaf, nodes, walk, first_of, leaf_rel, tgx, tgy, tgz, eps2, i,
-                         i - lane, lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
+            flush_leaves(ws, nleaf, leaf_rel, tgx, tgy, tgz, eps2, i, lane_bit, acc_x, acc_y,
+                         acc_z, pairs);
             nleaf = 0;
         }
     }
@@ -712,10 +698,9 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
                          pxh, pyh, pzh, pxl, pyl, pzl, ws.union_staged, acc_x, acc_y, acc_z, pairs,
                          cells);
     } else {
-        flush_cells<QUAD>(ws, ncell, nodes, walk, ntx, nty, ntz, eps2v,
-                          lane_bit, acc_x, acc_y, acc_z, node_count, status);
-        flush_leaves(ws, nleaf, nodes, walk, first_of, leaf_rel, tgx, tgy, tgz, eps2, i, i - lane,
-                     lane_bit, acc_x, acc_y, acc_z, pairs, node_count, n, status);
+        flush_cells<QUAD>(ws, ncell, ntx, nty, ntz, eps2v, lane_bit, acc_x, acc_y, acc_z);
+        flush_leaves(ws, nleaf, leaf_rel, tgx, tgy, tgz, eps2, i, lane_bit, acc_x, acc_y, acc_z,
+                     pairs);
     }
 
     if (active) {
@@ -738,25 +723,29 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
 
 } // namespace
 
+uint32_t walk_stack_capacity() { return kStackCap; }
+
 cudaError_t launch_walk(const DeviceNode *nodes, const WalkNode *walk_nodes,
                         const uint32_t *first_of, const float4 *leaf_rel, const double *sorted,
                         const uint32_t *perm, uint32_t n, double eps2, bool quadrupole,
                         double *ax, double *ay, double *az, TreeMeta *meta,
-                        unsigned long long *counters, unsigned *status, cudaStream_t stream) {
+                        unsigned long long *counters, unsigned *status, cudaStream_t stream,
+                        uint32_t stack_cap) {
     if (n == 0) {
         return cudaSuccess;
     }
+    const uint32_t cap = stack_cap == 0u || stack_cap > kStackCap ? kStackCap : stack_cap;
     const uint32_t blocks = ceil_div(n, static_cast<uint32_t>(kWalkThreads));
     const float eps2f = static_cast<float>(eps2);
     const size_t smem = kWalkWarps * sizeof(WarpSpace);
     if (quadrupole) {
         walk_kernel<true><<<blocks, kWalkThreads, smem, stream>>>(
             nodes, walk_nodes, first_of, leaf_rel, sorted, perm, n, eps2f, ax, ay, az, meta,
-            counters, status);
+            counters, status, cap);
     } else {
         walk_kernel<false><<<blocks, kWalkThreads, smem, stream>>>(
             nodes, walk_nodes, first_of, leaf_rel, sorted, perm, n, eps2f, ax, ay, az, meta,
-            counters, status);
+            counters, status, cap);
     }
     return cudaGetLastError();
 }
