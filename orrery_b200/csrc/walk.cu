@@ -90,7 +90,6 @@ struct __align__(16) WarpSpace {
     float4 leaf_pos[kLeafCap];  // leaf centre of mass - G (FP32), particle count bits
     uint2 leaf_meta[kLeafCap];  // (first particle | may-hold-a-target bit, target mask)
     uint2 stack[kStackCap];     // (node, reach mask)
-    uint2 mixed[32];            // this round's mixed items
     union {                     // used one at a time
         float4 leaf_quads[kLeafQuads][17];
         float4 union_staged[32]; // the union walk's leaf staging (after a fallback)
@@ -549,9 +548,11 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         }
         __syncwarp();
 
-        // Classify the lane's node against the box from its compact record.
-        bool sibling = false, child = false, cell = false, leaf = false, mixed = false;
-        uint32_t next = 0, count = 0;
+        // Classify the lane's node against the box from its compact record:
+        // every target accepts it (cell_mask = the item's mask), every target
+        // opens it (open_mask), or each target decides for itself (mixed).
+        bool sibling = false, mixed = false;
+        uint32_t next = 0, count = 0, cell_mask = 0u, open_mask = 0u;
         float4 A = make_float4(0.0f, 0.0f, 0.0f, 0.0f), B = A, D = A;
         if (has && item.x < node_count) {
             A = walk[item.x].a;
@@ -576,60 +577,28 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
             const float far2 = fmaf(fz, fz, fmaf(fy, fy, fx * fx));
             const float r2 = B.w;
             if (near2 >= r2 * (1.0f + kAcceptMargin) && r2 > 1e-30f) {
-                cell = true;
+                cell_mask = item.y;
             } else if (far2 < r2 * (1.0f - kAcceptMargin)) {
-                leaf = count > 0;
-                child = count == 0;
+                open_mask = item.y;
             } else {
                 mixed = true;
             }
         }
         const uint32_t below = lanes_below(lane);
         const uint32_t bs = __ballot_sync(kFull, sibling);
-        const uint32_t bc = __ballot_sync(kFull, child);
         if (sibling) {
             ws.stack[size + __popc(bs & below)] = make_uint2(next, item.y);
         }
-        if (child) {
-            ws.stack[size + __popc(bs) + __popc(bc & below)] = make_uint2(item.x + 1u, item.y);
-        }
-        size += __popc(bs) + __popc(bc);
-        const uint32_t ba = __ballot_sync(kFull, cell);
-        const uint32_t bl = __ballot_sync(kFull, leaf);
-        if (cell || leaf) {
-            const float4 Gh = ws.box[4], Gl = ws.box[5];
-            const float3 c = centre_rel(A, B, Gh, Gl);
-            if (cell) {
-                float4 C = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                if (QUAD) {
-                    C = walk[item.x].c;
-                }
-                stage_cell<QUAD>(ws, ncell + __popc(ba & below), c, A.w, item.y, C, D);
-                cells += __popc(item.y); // every target of the mask takes the cell
-            } else {
-                uint32_t first, lsize;
-                leaf_range(first_of, item.x, count, n, status, first, lsize);
-                queue_leaf(ws, nleaf + __popc(bl & below), c, lsize, first, item.y, warp_first,
-                           warp_end);
-            }
-        }
-        ncell += __popc(ba);
-        nleaf += __popc(bl);
+        size += __popc(bs);
 
-        // Mixed nodes: each target in the mask decides for itself.
-        const uint32_t bm = __ballot_sync(kFull, mixed);
-        if (mixed) {
-            ws.mixed[__popc(bm & below)] = item;
-        }
-        __syncwarp();
-        const uint32_t nmixed = __popc(bm);
-        for (uint32_t k = 0; k < nmixed; ++k) {
-            const uint2 mi = ws.mixed[k];
-            const uint32_t v = mi.x;
-            const uint32_t mask = mi.y;
+        // Mixed nodes: each target in the mask decides for itself; the lane
+        // that classified the node keeps the accepted and opened masks.
+        for (uint32_t bm = __ballot_sync(kFull, mixed); bm != 0u; bm &= bm - 1u) {
+            const uint32_t owner = __ffs(bm) - 1u;
+            const uint32_t v = __shfl_sync(kFull, item.x, owner);
+            const uint32_t mask = __shfl_sync(kFull, item.y, owner);
             const float4 MA = walk[v].a;
             const float4 MB = walk[v].b;
-            const float4 MD = walk[v].d;
             // FP32 test on every lane; the FP64 test, when any lane of the
             // mask falls inside the margin, on every lane too.
             const bool reach = (mask & lane_bit) != 0u;
@@ -647,39 +616,45 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
                 accept = accept || (unsure && exact);
             }
             const uint32_t accepted = __ballot_sync(kFull, accept) & mask;
-            const uint32_t opened = mask & ~accepted;
-            const uint32_t vcount = __float_as_uint(MD.w) & kWalkCountMask;
-            if (lane == 0) {
-                if (accepted != 0u || (opened != 0u && vcount > 0u)) {
-                    const float4 Gh = ws.box[4], Gl = ws.box[5];
-                    const float3 c = centre_rel(MA, MB, Gh, Gl);
-                    if (accepted != 0u) {
-                        float4 C = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                        if (QUAD) {
-                            C = walk[v].c;
-                        }
-                        stage_cell<QUAD>(ws, ncell, c, MA.w, accepted, C, MD);
-                        cells += __popc(accepted);
-                    }
-                    if (opened != 0u && vcount > 0u) {
-                        uint32_t first, lsize;
-                        leaf_range(first_of, v, vcount, n, status, first, lsize);
-                        queue_leaf(ws, nleaf, c, lsize, first, opened, warp_first, warp_end);
-                    }
-                }
-                if (opened != 0u && vcount == 0u) {
-                    ws.stack[size] = make_uint2(v + 1u, opened);
-                }
-            }
-            ncell += accepted != 0u ? 1u : 0u;
-            if (opened != 0u) {
-                if (vcount > 0u) {
-                    ++nleaf;
-                } else {
-                    ++size;
-                }
+            if (lane == owner) {
+                cell_mask = accepted;
+                open_mask = mask & ~accepted;
             }
         }
+
+        // Every lane files its node's outcome: a staged cell for the targets
+        // that accept it, and for those that open it a queued leaf or a pushed
+        // first child.
+        const bool cell = cell_mask != 0u;
+        const bool leaf = open_mask != 0u && count > 0u;
+        const bool child = open_mask != 0u && count == 0u;
+        const uint32_t ba = __ballot_sync(kFull, cell);
+        const uint32_t bl = __ballot_sync(kFull, leaf);
+        const uint32_t bc = __ballot_sync(kFull, child);
+        if (child) {
+            ws.stack[size + __popc(bc & below)] = make_uint2(item.x + 1u, open_mask);
+        }
+        if (cell || leaf) {
+            const float4 Gh = ws.box[4], Gl = ws.box[5];
+            const float3 c = centre_rel(A, B, Gh, Gl);
+            if (cell) {
+                float4 C = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (QUAD) {
+                    C = walk[item.x].c;
+                }
+                stage_cell<QUAD>(ws, ncell + __popc(ba & below), c, A.w, cell_mask, C, D);
+                cells += __popc(cell_mask); // every target of the mask takes the cell
+            }
+            if (leaf) {
+                uint32_t first, lsize;
+                leaf_range(first_of, item.x, count, n, status, first, lsize);
+                queue_leaf(ws, nleaf + __popc(bl & below), c, lsize, first, open_mask,
+                           warp_first, warp_end);
+            }
+        }
+        size += __popc(bc);
+        ncell += __popc(ba);
+        nleaf += __popc(bl);
         __syncwarp();
         if (ncell > kCellCap - 32u) {
             flush_cells<QUAD>(ws, ncell, ntx, nty, ntz, eps2v, lane_bit, acc_x, acc_y, acc_z);
