@@ -283,11 +283,13 @@ __device__ __forceinline__ uint32_t next_child(const DeviceNode *nodes, uint32_t
 
 // Writes the walk's compact record of node k (see WalkNode). `sibling`: the
 // node has a next sibling, i.e. its escape index lies inside its parent's
-// subtree (carried in the top bit of the count word).
+// subtree (carried in the top bit of the count word). A leaf's escape index is
+// always k + 1, so a leaf's record carries its first particle in its place.
 __device__ void store_walk_node(WalkNode *walk, uint32_t *first_of, uint32_t k,
                                 const DeviceNode &node, const DeviceQuadrupole *q,
                                 bool sibling) {
     const uint32_t count_word = node.count | (sibling ? kWalkSiblingBit : 0u);
+    const uint32_t link = node.count > 0 ? node.first : node.next;
     const float hx = __double2float_rn(node.com_x);
     const float hy = __double2float_rn(node.com_y);
     const float hz = __double2float_rn(node.com_z);
@@ -301,10 +303,10 @@ __device__ void store_walk_node(WalkNode *walk, uint32_t *first_of, uint32_t k,
         w.c = make_float4(__double2float_rn(q->xx), __double2float_rn(q->xy),
                           __double2float_rn(q->xz), __double2float_rn(q->yy));
         w.d = make_float4(__double2float_rn(q->yz), __double2float_rn(q->zz),
-                          __uint_as_float(node.next), __uint_as_float(count_word));
+                          __uint_as_float(link), __uint_as_float(count_word));
     } else {
         w.c = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        w.d = make_float4(0.0f, 0.0f, __uint_as_float(node.next), __uint_as_float(count_word));
+        w.d = make_float4(0.0f, 0.0f, __uint_as_float(link), __uint_as_float(count_word));
     }
     walk[k] = w;
     first_of[k] = node.first;

@@ -34,10 +34,15 @@ static_assert(sizeof(DeviceNode) == 64, "DeviceNode is four 16-byte words");
 //   a = (com_x hi, com_y hi, com_z hi, mass)       FP32
 //   b = (com_x lo, com_y lo, com_z lo, r2)         FP32 (r2 rounded to nearest)
 //   c = (Qxx, Qxy, Qxz, Qyy)                       FP32 quadrupole
-//   d = (Qyz, Qzz, next, count)                    next/count as uint32 bits;
-//                                                   the top bit of count is set
-//                                                   when the node has a next
-//                                                   sibling (next < parent's next)
+//   d = (Qyz, Qzz, link, count)                    link/count as uint32 bits:
+//                                                   link is the escape index of
+//                                                   an internal node and the
+//                                                   first particle of a leaf
+//                                                   (whose escape index is its
+//                                                   own + 1); the top bit of
+//                                                   count is set when the node
+//                                                   has a next sibling (escape
+//                                                   index < parent's)
 // hi + lo carries each FP64 coordinate to ~2^-48 relative, so offsets to the
 // target (also split) come out in FP32 to ~1e-7 relative without conversions.
 struct alignas(16) WalkNode {

@@ -177,8 +177,8 @@ __device__ void union_walk(const DeviceNode *__restrict__ nodes,
         const float4 A = walk[cur].a;
         const float4 B = walk[cur].b;
         const float4 D = walk[cur].d;
-        const uint32_t next = __float_as_uint(D.z);
         const uint32_t count = __float_as_uint(D.w) & kWalkCountMask;
+        const uint32_t next = count > 0u ? cur + 1u : __float_as_uint(D.z);
         bool open_leaf = false;
         float dx = 0.0f, dy = 0.0f, dz = 0.0f;
         if (cursor == cur) {
@@ -291,10 +291,9 @@ __device__ __forceinline__ void queue_leaf(WarpSpace &ws, uint32_t k, float3 c, 
 }
 
 // A leaf's first particle and size, checked against the particle count.
-__device__ __forceinline__ void leaf_range(const uint32_t *first_of, uint32_t v, uint32_t count,
-                                           uint32_t n, unsigned *status, uint32_t &first,
-                                           uint32_t &size) {
-    first = first_of[v];
+__device__ __forceinline__ void leaf_range(uint32_t link, uint32_t count, uint32_t n,
+                                           unsigned *status, uint32_t &first, uint32_t &size) {
+    first = link;
     size = count;
     if (first > n || size > n - first) {
         atomicOr(status, kStatusInvalid);
@@ -303,9 +302,54 @@ __device__ __forceinline__ void leaf_range(const uint32_t *first_of, uint32_t v,
     }
 }
 
+// Two staged cells (pair p) for this lane's target: m d / r^3 and, with QUAD,
+// the quadrupole term, added to the packed sums (zero outside a cell's mask).
+template <bool QUAD>
+__device__ __forceinline__ void cell_pair(const WarpSpace &ws, uint32_t p, float2 ntx, float2 nty,
+                                          float2 ntz, float2 eps2, uint32_t lane_bit, float2 &sx,
+                                          float2 &sy, float2 &sz) {
+    const float4 q0 = ws.cells[0][p], q1 = ws.cells[1][p];
+    const uint2 masks = *reinterpret_cast<const uint2 *>(&ws.cell_mask[2 * p]);
+    const float2 dx = __fadd2_rn(f2(q0.x, q0.y), ntx);
+    const float2 dy = __fadd2_rn(f2(q0.z, q0.w), nty);
+    const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
+    const float2 r2e = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
+    const float inv0 = rsqrt_approx(r2e.x);
+    const float inv1 = rsqrt_approx(r2e.y);
+    const float2 inv = f2((masks.x & lane_bit) != 0u ? inv0 : 0.0f,
+                          (masks.y & lane_bit) != 0u ? inv1 : 0.0f);
+    const float2 inv2 = __fmul2_rn(inv, inv);
+    // Monopole m d / r^3 (tree_walk.hpp:129-140).
+    float2 coef = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
+    if (QUAD) {
+        // Quadrupole -Q d / r^5 + 2.5 (d.Q d) d / r^7 (tree_walk.hpp:142-181),
+        // folded with the monopole: d (m / r^3 + 2.5 (d.Q d) / r^7) - Q d / r^5.
+        const float4 q2 = ws.cells[2][p], q3 = ws.cells[3][p], q4 = ws.cells[4][p];
+        const float2 xx = f2(q2.x, q2.y), xy = f2(q2.z, q2.w);
+        const float2 xz = f2(q3.x, q3.y), yy = f2(q3.z, q3.w);
+        const float2 yz = f2(q4.x, q4.y), zz = f2(q4.z, q4.w);
+        const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
+        const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
+        const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
+        // q = 2.5 Q d, quadratic = 2.5 d.Q d.
+        const float2 quadratic = __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
+        const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
+        coef = __ffma2_rn(quadratic, __fmul2_rn(inv5, inv2), coef);
+        const float2 ninv5 = __fmul2_rn(inv5, f2(-0.4f, -0.4f));
+        sx = __ffma2_rn(qx, ninv5, sx);
+        sy = __ffma2_rn(qy, ninv5, sy);
+        sz = __ffma2_rn(qz, ninv5, sz);
+    }
+    sx = __ffma2_rn(dx, coef, sx);
+    sy = __ffma2_rn(dy, coef, sy);
+    sz = __ffma2_rn(dz, coef, sz);
+}
+
 // Evaluates the staged cells: every lane sums every cell for its target (zero
-// outside the cell's mask), two cells per FP32x2 instruction. Each lane holds
-// its target relative to G, so the offset to a cell is one subtraction.
+// outside the cell's mask), two cells per FP32x2 instruction, four per loop
+// step (the batch is padded with neutral entries to a multiple of four).
+// Each lane holds its target relative to G, so the offset to a cell is one
+// subtraction.
 template <bool QUAD>
 __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count, float2 ntx, float2 nty,
                                             float2 ntz, float2 eps2, uint32_t lane_bit,
@@ -321,42 +365,7 @@ __device__ __forceinline__ void flush_cells(WarpSpace &ws, uint32_t count, float
     __syncwarp();
     float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
     for (uint32_t j = 0; j < count; j += 2) {
-        const uint32_t p = j >> 1;
-        const float4 q0 = ws.cells[0][p], q1 = ws.cells[1][p];
-        const uint2 masks = *reinterpret_cast<const uint2 *>(&ws.cell_mask[j]);
-        const float2 dx = __fadd2_rn(f2(q0.x, q0.y), ntx);
-        const float2 dy = __fadd2_rn(f2(q0.z, q0.w), nty);
-        const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
-        const float2 r2e = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, eps2)));
-        const float inv0 = rsqrt_approx(r2e.x);
-        const float inv1 = rsqrt_approx(r2e.y);
-        const float2 inv = f2((masks.x & lane_bit) != 0u ? inv0 : 0.0f,
-                              (masks.y & lane_bit) != 0u ? inv1 : 0.0f);
-        const float2 inv2 = __fmul2_rn(inv, inv);
-        // Monopole m d / r^3 (tree_walk.hpp:129-140).
-        float2 coef = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
-        if (QUAD) {
-            // Quadrupole -Q d / r^5 + 2.5 (d.Q d) d / r^7 (tree_walk.hpp:142-181),
-            // folded with the monopole: d (m / r^3 + 2.5 (d.Q d) / r^7) - Q d / r^5.
-            const float4 q2 = ws.cells[2][p], q3 = ws.cells[3][p], q4 = ws.cells[4][p];
-            const float2 xx = f2(q2.x, q2.y), xy = f2(q2.z, q2.w);
-            const float2 xz = f2(q3.x, q3.y), yy = f2(q3.z, q3.w);
-            const float2 yz = f2(q4.x, q4.y), zz = f2(q4.z, q4.w);
-            const float2 qx = __ffma2_rn(xx, dx, __ffma2_rn(xy, dy, __fmul2_rn(xz, dz)));
-            const float2 qy = __ffma2_rn(xy, dx, __ffma2_rn(yy, dy, __fmul2_rn(yz, dz)));
-            const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
-            // q = 2.5 Q d, quadratic = 2.5 d.Q d.
-            const float2 quadratic = __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
-            const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
-            coef = __ffma2_rn(quadratic, __fmul2_rn(inv5, inv2), coef);
-            const float2 ninv5 = __fmul2_rn(inv5, f2(-0.4f, -0.4f));
-            sx = __ffma2_rn(qx, ninv5, sx);
-            sy = __ffma2_rn(qy, ninv5, sy);
-            sz = __ffma2_rn(qz, ninv5, sz);
-        }
-        sx = __ffma2_rn(dx, coef, sx);
-        sy = __ffma2_rn(dy, coef, sy);
-        sz = __ffma2_rn(dz, coef, sz);
+        cell_pair<QUAD>(ws, j >> 1, ntx, nty, ntz, eps2, lane_bit, sx, sy, sz);
     }
     __syncwarp();
     acc_x += static_cast<double>(sx.x) + static_cast<double>(sx.y);
@@ -553,14 +562,14 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
         // opens it (open_mask), or each target decides for itself (mixed).
         bool sibling = false, mixed = false;
         uint32_t next = 0, count = 0, cell_mask = 0u, open_mask = 0u;
-        float4 A = make_float4(0.0f, 0.0f, 0.0f, 0.0f), B = A, D = A;
+        float4 A = make_float4(0.0f, 0.0f, 0.0f, 0.0f), B = A, C = A, D = A;
         if (has && item.x < node_count) {
             A = walk[item.x].a;
             B = walk[item.x].b;
             D = walk[item.x].d;
-            next = __float_as_uint(D.z);
             const uint32_t word = __float_as_uint(D.w);
             count = word & kWalkCountMask;
+            next = count > 0u ? item.x + 1u : __float_as_uint(D.z);
             sibling = (word & kWalkSiblingBit) != 0u;
             const float4 loh = ws.box[0], lol = ws.box[1], hih = ws.box[2], hil = ws.box[3];
             // Signed distances lo - c and c - hi per axis, from hi + lo parts.
@@ -638,7 +647,6 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
             const float4 Gh = ws.box[4], Gl = ws.box[5];
             const float3 c = centre_rel(A, B, Gh, Gl);
             if (cell) {
-                float4 C = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 if (QUAD) {
                     C = walk[item.x].c;
                 }
@@ -647,7 +655,7 @@ __global__ void __launch_bounds__(kWalkThreads, 8)
             }
             if (leaf) {
                 uint32_t first, lsize;
-                leaf_range(first_of, item.x, count, n, status, first, lsize);
+                leaf_range(__float_as_uint(D.z), count, n, status, first, lsize);
                 queue_leaf(ws, nleaf + __popc(bl & below), c, lsize, first, open_mask,
                            warp_first, warp_end);
             }
