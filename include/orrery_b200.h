@@ -153,7 +153,7 @@ int ob_tree_copy_order(ob_solver *solver, uint64_t *codes, uint32_t *indices, do
  * device memory only from their own fixed pool, or that must not grow or
  * fragment the device heap once running. (Like every entry point here it
  * makes CUDA calls, so it must not be called from a stream or host callback.)
- * Every intermediate buffer lives in one fixed device array of about 14 MB
+ * Every intermediate buffer lives in one fixed device array of about 17 MB
  * that each device holds from the library's loading until the process exits;
  * n above 1,048,576 is refused with OB_ERROR_CAPACITY. The first call on a
  * device looks up that array's device address, so make it before any stream

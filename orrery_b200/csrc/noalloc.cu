@@ -56,7 +56,7 @@ constexpr size_t kCubeOffset = kMetaOffset + kMetaBytes;
 constexpr size_t kCubeBytes = align256(sizeof(double) * 6 * kCubeBlocks);
 constexpr size_t kScratchBytes = kCubeOffset + kCubeBytes;
 
-// The fixed scratch (about 14 MB). Host code must not use this name as a
+// The fixed scratch (about 17 MB). Host code must not use this name as a
 // device address: its host-side value is a stand-in, and the device address
 // comes from cudaGetSymbolAddress below.
 static __device__ __align__(256) unsigned char g_order_scratch[kScratchBytes];

@@ -16,6 +16,9 @@
 // with warp match operations, publishes its per-digit counts, resolves its
 // global offsets by decoupled look-back over earlier tiles (every wait bounded)
 // and scatters through shared memory so the global writes are contiguous runs.
+#include <algorithm>
+#include <atomic>
+
 #include "common.cuh"
 #include "runtime.hpp"
 #include "tree_kernels.hpp"
@@ -233,10 +236,13 @@ __device__ __forceinline__ void store_volatile(uint32_t *p, uint32_t v) {
 
 constexpr uint32_t kWarps = kSortThreads / 32;
 
-__global__ void __launch_bounds__(kSortThreads)
+// One onesweep pass. CTAs are persistent: each takes tiles by atomic ticket
+// (so every tile's predecessors were taken by CTAs that are running or done,
+// which publish without waiting on later tiles) until the tiles run out.
+__global__ void __launch_bounds__(kSortThreads, 5)
     onesweep_kernel(const unsigned long long *__restrict__ keys_in,
                     const uint32_t *__restrict__ vals_in, unsigned long long *keys_out,
-                    uint32_t *vals_out, uint32_t n, uint32_t shift,
+                    uint32_t *vals_out, uint32_t n, uint32_t tiles, uint32_t shift,
                     const uint32_t *__restrict__ offsets, uint32_t *lookback, uint32_t *ticket,
                     unsigned *status, uint32_t poll_limit) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -249,114 +255,121 @@ __global__ void __launch_bounds__(kSortThreads)
 
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u, warp = tid >> 5;
-    if (tid == 0) {
-        *s_tile = atomicAdd(ticket, 1u);
-    }
-    for (uint32_t k = tid; k < kWarps * kRadix; k += kSortThreads) {
-        s_warp[k] = 0;
-    }
-    __syncthreads();
-    const uint32_t tile = *s_tile;
-    const uint32_t base = tile * kSortTile;
-
-    // Warp-striped load: the tile order of (warp, item, lane) is this order.
-    unsigned long long key[kSortItems];
-    uint32_t val[kSortItems], digit[kSortItems], rank[kSortItems];
     const uint32_t lt_mask = (1u << lane) - 1u;
     uint32_t *hist = s_warp + warp * kRadix;
-#pragma unroll
-    for (int it = 0; it < kSortItems; ++it) {
-        const uint32_t i = base + warp * (kSortItems * 32) + it * 32 + lane;
-        const bool valid = i < n;
-        key[it] = valid ? keys_in[i] : 0ull;
-        val[it] = valid ? vals_in[i] : 0u;
-        digit[it] = valid ? static_cast<uint32_t>((key[it] >> shift) & (kRadix - 1)) : kRadix;
-        // Stable warp-local rank: earlier items first, then lower lanes.
-        const uint32_t peers = __match_any_sync(0xffffffffu, digit[it]);
-        const uint32_t before = __popc(peers & lt_mask);
-        const uint32_t running = valid ? hist[digit[it]] : 0u;
-        __syncwarp();
-        if (valid && before == 0) {
-            hist[digit[it]] = running + __popc(peers);
+    while (true) {
+        if (tid == 0) {
+            *s_tile = atomicAdd(ticket, 1u);
         }
-        __syncwarp();
-        rank[it] = running + before;
-    }
-    __syncthreads();
+        for (uint32_t k = tid; k < kWarps * kRadix; k += kSortThreads) {
+            s_warp[k] = 0;
+        }
+        __syncthreads();
+        const uint32_t tile = *s_tile;
+        if (tile >= tiles) {
+            return; // uniform: every thread read the same ticket
+        }
+        const uint32_t base = tile * kSortTile;
 
-    // Thread t owns digit t: tile count, warp prefixes, publish, look back.
-    const uint32_t d = tid;
-    uint32_t count = 0;
-    for (uint32_t w = 0; w < kWarps; ++w) {
-        const uint32_t c = s_warp[w * kRadix + d];
-        s_warp[w * kRadix + d] = count;
-        count += c;
-    }
-    uint32_t *mine = lookback + static_cast<size_t>(tile) * kRadix + d;
-    if (tile == 0) {
-        store_volatile(mine, kFlagPrefix | count);
-    } else {
-        store_volatile(mine, kFlagAggregate | count);
-    }
-    uint32_t exclusive = 0;
-    bool ok = true;
-    if (tile > 0) {
-        int64_t j = static_cast<int64_t>(tile) - 1;
-        uint32_t polls = 0;
-        while (j >= 0) {
-            const uint32_t s = load_volatile(lookback + static_cast<size_t>(j) * kRadix + d);
-            const uint32_t flag = s & ~kCountMask;
-            if (flag == 0u) {
-                if (++polls > poll_limit) {
-                    atomicOr(status, kStatusTimeout);
-                    ok = false;
+        // Warp-striped load: the tile order of (warp, item, lane) is this order.
+        unsigned long long key[kSortItems];
+        uint32_t val[kSortItems], digit[kSortItems], rank[kSortItems];
+#pragma unroll
+        for (int it = 0; it < kSortItems; ++it) {
+            const uint32_t i = base + warp * (kSortItems * 32) + it * 32 + lane;
+            const bool valid = i < n;
+            key[it] = valid ? keys_in[i] : 0ull;
+            val[it] = valid ? vals_in[i] : 0u;
+            digit[it] = valid ? static_cast<uint32_t>((key[it] >> shift) & (kRadix - 1)) : kRadix;
+            // Stable warp-local rank: earlier items first, then lower lanes.
+            const uint32_t peers = __match_any_sync(0xffffffffu, digit[it]);
+            const uint32_t before = __popc(peers & lt_mask);
+            const uint32_t running = valid ? hist[digit[it]] : 0u;
+            __syncwarp();
+            if (valid && before == 0) {
+                hist[digit[it]] = running + __popc(peers);
+            }
+            __syncwarp();
+            rank[it] = running + before;
+        }
+        __syncthreads();
+
+        // Thread t owns digit t: tile count, warp prefixes, publish, look back.
+        const uint32_t d = tid;
+        uint32_t count = 0;
+        for (uint32_t w = 0; w < kWarps; ++w) {
+            const uint32_t c = s_warp[w * kRadix + d];
+            s_warp[w * kRadix + d] = count;
+            count += c;
+        }
+        uint32_t *mine = lookback + static_cast<size_t>(tile) * kRadix + d;
+        if (tile == 0) {
+            store_volatile(mine, kFlagPrefix | count);
+        } else {
+            store_volatile(mine, kFlagAggregate | count);
+        }
+        uint32_t exclusive = 0;
+        bool ok = true;
+        if (tile > 0) {
+            int64_t j = static_cast<int64_t>(tile) - 1;
+            uint32_t polls = 0;
+            while (j >= 0) {
+                const uint32_t s = load_volatile(lookback + static_cast<size_t>(j) * kRadix + d);
+                const uint32_t flag = s & ~kCountMask;
+                if (flag == 0u) {
+                    if (++polls > poll_limit) {
+                        atomicOr(status, kStatusTimeout);
+                        ok = false;
+                        break;
+                    }
+                    continue;
+                }
+                exclusive += s & kCountMask;
+                if (flag == kFlagPrefix) {
                     break;
                 }
-                continue;
+                --j;
             }
-            exclusive += s & kCountMask;
-            if (flag == kFlagPrefix) {
-                break;
-            }
-            --j;
+            __threadfence();
+            store_volatile(mine, kFlagPrefix | ((exclusive + count) & kCountMask));
         }
-        __threadfence();
-        store_volatile(mine, kFlagPrefix | ((exclusive + count) & kCountMask));
-    }
-    s_base[d] = offsets[d] + exclusive;
+        s_base[d] = offsets[d] + exclusive;
 
-    // Exclusive scan of the tile's digit counts gives each digit's run start.
-    s_start[d] = count;
-    __syncthreads();
-    for (uint32_t off = 1; off < kRadix; off <<= 1) {
-        const uint32_t v = d >= off ? s_start[d - off] : 0u;
+        // Exclusive scan of the tile's digit counts gives each digit's run start.
+        s_start[d] = count;
         __syncthreads();
-        s_start[d] += v;
+        for (uint32_t off = 1; off < kRadix; off <<= 1) {
+            const uint32_t v = d >= off ? s_start[d - off] : 0u;
+            __syncthreads();
+            s_start[d] += v;
+            __syncthreads();
+        }
+        s_start[d] -= count;
         __syncthreads();
-    }
-    s_start[d] -= count;
-    __syncthreads();
-    if (!__syncthreads_and(ok ? 1 : 0)) {
-        return;
-    }
+        if (!__syncthreads_and(ok ? 1 : 0)) {
+            return; // a timed-out tile stays unscattered; the CTA takes no more tiles
+        }
 
-    // Place keys in shared memory in digit order, then write contiguous runs.
+        // Place keys in shared memory in digit order, then write contiguous runs.
 #pragma unroll
-    for (int it = 0; it < kSortItems; ++it) {
-        if (digit[it] < kRadix) {
-            const uint32_t pos = s_start[digit[it]] + s_warp[warp * kRadix + digit[it]] + rank[it];
-            s_keys[pos] = key[it];
-            s_vals[pos] = val[it];
+        for (int it = 0; it < kSortItems; ++it) {
+            if (digit[it] < kRadix) {
+                const uint32_t pos =
+                    s_start[digit[it]] + s_warp[warp * kRadix + digit[it]] + rank[it];
+                s_keys[pos] = key[it];
+                s_vals[pos] = val[it];
+            }
         }
-    }
-    __syncthreads();
-    const uint32_t valid_in_tile = n > base ? min(kSortTile, n - base) : 0u;
-    for (uint32_t k = tid; k < valid_in_tile; k += kSortThreads) {
-        const unsigned long long kk = s_keys[k];
-        const uint32_t dd = static_cast<uint32_t>((kk >> shift) & (kRadix - 1));
-        const uint32_t dst = s_base[dd] + (k - s_start[dd]);
-        keys_out[dst] = kk;
-        vals_out[dst] = s_vals[k];
+        __syncthreads();
+        const uint32_t valid_in_tile = n > base ? min(kSortTile, n - base) : 0u;
+        for (uint32_t k = tid; k < valid_in_tile; k += kSortThreads) {
+            const unsigned long long kk = s_keys[k];
+            const uint32_t dd = static_cast<uint32_t>((kk >> shift) & (kRadix - 1));
+            const uint32_t dst = s_base[dd] + (k - s_start[dd]);
+            keys_out[dst] = kk;
+            vals_out[dst] = s_vals[k];
+        }
+        __syncthreads(); // the next tile reuses the shared arrays
     }
 }
 
@@ -497,8 +510,27 @@ cudaError_t launch_onesweep(const unsigned long long *keys_in, const uint32_t *v
     if (err != cudaSuccess) {
         return err;
     }
-    onesweep_kernel<<<sort_tiles(n), kSortThreads, onesweep_smem(), stream>>>(
-        keys_in, vals_in, keys_out, vals_out, n, static_cast<uint32_t>(kRadixBits * pass),
+    // Persistent CTAs: as many as fit on the device at once, at most one per tile.
+    static std::atomic<int> resident{0};
+    if (resident.load(std::memory_order_relaxed) == 0) {
+        int per_sm = 0, sms = 0, device = 0;
+        cudaError_t e = cudaGetDevice(&device);
+        if (e == cudaSuccess) {
+            e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        }
+        if (e == cudaSuccess) {
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_kernel,
+                                                              kSortThreads, onesweep_smem());
+        }
+        if (e != cudaSuccess) {
+            return e;
+        }
+        resident.store(std::max(1, per_sm) * std::max(1, sms), std::memory_order_relaxed);
+    }
+    const uint32_t tiles = sort_tiles(n);
+    const uint32_t grid = std::min(tiles, static_cast<uint32_t>(resident.load()));
+    onesweep_kernel<<<grid, kSortThreads, onesweep_smem(), stream>>>(
+        keys_in, vals_in, keys_out, vals_out, n, tiles, static_cast<uint32_t>(kRadixBits * pass),
         offsets + pass * kRadix, lookback, ticket, status, poll_limit);
     return cudaGetLastError();
 }

@@ -17,7 +17,7 @@ constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 constexpr int kRadixPasses = 8;
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
+constexpr int kSortItems = 8;
 constexpr uint32_t kSortTile = kSortThreads * kSortItems;
 
 // Bounding-cube reduction: blocks of the min/max pass (4 per SM); the
