@@ -529,7 +529,7 @@ int ob_probe_fp64(double *dfma_lane_per_s);
 int ob_test_lookback_timeout(uint64_t n, uint32_t poll_limit, int skip_first_tile);
 
 /* Bounds the FP32 tree walk's per-warp traversal stack of `solver` to `cap`
- * entries (0 restores the full 320) from its next evaluation on. A warp whose
+ * entries (0 restores the full 256) from its next evaluation on. A warp whose
  * stack fills discards its partial sums and finishes with the per-target
  * union walk (the fallback a valid tree rarely needs); a small cap forces it,
  * so tests can hold that path to the oracle. OB_ERROR_UNSUPPORTED for direct

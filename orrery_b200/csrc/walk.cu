@@ -38,8 +38,9 @@
 // batch and flushed into FP64 per-target sums.
 //
 // A round takes no more items than the stack has room to push back (each
-// pushes at most two), so the stack (320 entries per warp; the 2M two-disc
-// collision peaks near 280) only stops the traversal when completely full;
+// pushes at most two), so the stack (256 entries per warp; with this rule the
+// 2M two-disc collision rarely fills it) only stops the traversal when
+// completely full;
 // the warp then discards its partial sums and walks its targets with the
 // per-target union walk (union_walk below), which gives the same counts.
 //
@@ -70,7 +71,7 @@ constexpr uint32_t kFull = 0xffffffffu;
 // (capacity - size) items, so the stack cannot overflow while it has room;
 // cells and leaves are evaluated once more than capacity - 32 are queued.
 // Sized so that 8 CTAs of 4 warps fit in an SM's shared memory.
-constexpr uint32_t kStackCap = 320;
+constexpr uint32_t kStackCap = 256;
 constexpr uint32_t kCellCap = 48;
 constexpr uint32_t kLeafCap = 40;
 // Staged cell fields, as quads of packed pairs: quad f of pair p holds

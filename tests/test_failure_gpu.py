@@ -88,4 +88,4 @@ def test_the_stack_cap_is_refused_where_it_does_not_apply(b200):
     direct = b200.B200DirectSolver(0.01)
     assert lib.ob_test_set_walk_stack_cap(direct._handle, 8) == b200.ERROR_UNSUPPORTED
     tree = b200.B200TreeSolver(0.01, 0.5, 32, True)
-    assert lib.ob_test_set_walk_stack_cap(tree._handle, 321) == b200.ERROR_INVALID_ARGUMENT
+    assert lib.ob_test_set_walk_stack_cap(tree._handle, 257) == b200.ERROR_INVALID_ARGUMENT
