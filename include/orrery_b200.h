@@ -297,6 +297,18 @@ int ob_system_step_kernels(ob_system *system, int32_t integrator, double dt, uin
  * the chosen shape from the next step on (the step graph is captured again). */
 int ob_system_autotune(ob_system *system, ob_direct_shape *chosen, double *best_ms);
 
+/* Whole steps of a small system in one launch: with the FP32 direct field,
+ * softening and velocity Verlet or Yoshida-4, a system whose sources fit one
+ * CTA's shared memory (a few thousand particles) takes its steps -- kicks,
+ * drifts and every force evaluation -- in a single cooperative kernel instead
+ * of four launches per substep (on by default). The forces are the FP32
+ * direct kernel's arithmetic with its own summation order (within its
+ * bounds of the FP64 forces); the kicks and drifts are bit-identical.
+ * enable = 0 turns it off for this system; *active (may be NULL) tells
+ * whether the next velocity-Verlet step will use it. No reference
+ * counterpart (the reference launches per evaluation). */
+int ob_system_set_fused_steps(ob_system *system, int32_t enable, int32_t *active);
+
 int ob_system_counts(ob_system *system, ob_counts *counts);
 int ob_system_size(const ob_system *system, uint64_t *n);
 

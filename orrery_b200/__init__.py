@@ -197,6 +197,7 @@ def load_library():
     lib.ob_system_profile.argtypes = [vp, C.c_uint32]
     lib.ob_system_phase_times.argtypes = [vp, C.POINTER(Timings), C.POINTER(C.c_uint32)]
     lib.ob_system_step_kernels.argtypes = [vp, C.c_int32, C.c_double, C.POINTER(C.c_uint32)]
+    lib.ob_system_set_fused_steps.argtypes = [vp, C.c_int32, C.POINTER(C.c_int32)]
     lib.ob_batch_create.argtypes = [C.c_uint32, C.POINTER(C.c_uint64), _dp, C.POINTER(vp)]
     lib.ob_batch_destroy.argtypes = [vp]
     lib.ob_batch_destroy.restype = None
@@ -655,8 +656,17 @@ class DeviceSystem:
         _check(self._lib.ob_system_phase_times(self._handle, C.byref(t), C.byref(n)))
         return {k: getattr(t, k) for k, _ in Timings._fields_}, n.value
 
+    def set_fused_steps(self, enable: bool = True) -> bool:
+        """Allows (default) or forbids whole steps of a small FP32-direct system
+        in one launch; returns whether the next velocity-Verlet step uses it."""
+        active = C.c_int32()
+        _check(self._lib.ob_system_set_fused_steps(self._handle, 1 if enable else 0,
+                                                   C.byref(active)))
+        return bool(active.value)
+
     def step_kernels(self, dt: float, integrator: str = "vv") -> int:
-        """Kernel launches in one captured step."""
+        """Kernel launches one step call makes (a captured step's kernels, or one
+        launch for the fused small-system path, whatever the step count)."""
         k = C.c_uint32()
         _check(self._lib.ob_system_step_kernels(self._handle, _INTEGRATORS[integrator],
                                                 float(dt), C.byref(k)))

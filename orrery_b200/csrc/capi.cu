@@ -92,6 +92,10 @@ System::~System() {
     for (auto e : ring_) {
         cudaEventDestroy(e);
     }
+    for (auto &pair : fused_marks_) {
+        cudaEventDestroy(pair.first);
+        cudaEventDestroy(pair.second);
+    }
     if (stream_ != nullptr && owns_stream_) {
         cudaStreamDestroy(stream_);
     }
@@ -361,6 +365,12 @@ void System::profile(uint32_t steps) {
         cudaEventDestroy(e);
     }
     ring_.clear();
+    for (auto &pair : fused_marks_) {
+        cudaEventDestroy(pair.first);
+        cudaEventDestroy(pair.second);
+    }
+    fused_marks_.clear();
+    fused_mark_evals_.clear();
     ring_steps_ = steps;
     ring_used_ = 0;
     const size_t per_step = kMarksPerStep;
@@ -389,6 +399,15 @@ ob_timings System::phase_times(uint32_t &evaluations) {
             ++evaluations;
         }
     }
+    // Fused launches: the whole launch counts as force evaluation time (its
+    // kicks and drifts are a few microseconds of it), per evaluation.
+    for (size_t k = 0; k < fused_marks_.size(); ++k) {
+        float ms = 0;
+        check(cudaEventElapsedTime(&ms, fused_marks_[k].first, fused_marks_[k].second),
+              "phase timing");
+        t.traversal_ms += ms;
+        evaluations += static_cast<uint32_t>(fused_mark_evals_[k]);
+    }
     if (evaluations > 0) {
         t.ordering_ms /= evaluations;
         t.construction_ms /= evaluations;
@@ -397,10 +416,32 @@ ob_timings System::phase_times(uint32_t &evaluations) {
     return t;
 }
 
+bool System::set_fused_steps(bool enable) {
+    fused_enabled_ = enable;
+    return fused_for(OB_INTEGRATOR_VV);
+}
+
+bool System::fused_for(int integrator) {
+    const ob_solver_params &p = solver_->params();
+    if (!fused_enabled_ || (integrator != OB_INTEGRATOR_VV && integrator != OB_INTEGRATOR_YOSHIDA4) ||
+        p.kind != OB_SOLVER_DIRECT || p.precision != OB_PRECISION_FP32 ||
+        !(p.softening_squared > 0.0) || !(static_cast<float>(p.softening_squared) > 0.0f)) {
+        return false;
+    }
+    if (fused_fits_ < 0) {
+        fused_fits_ = fused_steps_fit(n_) ? 1 : 0;
+        cudaGetLastError();
+    }
+    return fused_fits_ == 1;
+}
+
 uint32_t System::step_kernels(int integrator, double dt) {
     require(integrator == OB_INTEGRATOR_VV || integrator == OB_INTEGRATOR_YOSHIDA4 ||
                 integrator == OB_INTEGRATOR_RK4,
             "unknown integrator");
+    if (fused_for(integrator)) {
+        return 1; // one launch per call, whatever the number of steps
+    }
     ensure_graph(integrator, dt);
     return graph_kernels_;
 }
@@ -411,6 +452,47 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
             "unknown integrator");
     require(std::isfinite(dt), "the timestep must be finite");
     if (steps == 0 || n_ == 0) {
+        solver_->account(steps * evaluations_per_step(integrator), n_);
+        return;
+    }
+    if (fused_for(integrator)) {
+        if (fused_buf_.size() == 0) {
+            fused_buf_.reserve(fused_scratch_floats4(n_));
+            fused_barrier_.reserve(2);
+            check(cudaMemset(fused_barrier_.data(), 0, 2 * sizeof(unsigned)),
+                  "clearing the grid barrier");
+        }
+        double h[3] = {dt, dt, dt};
+        int cycle = 1;
+        if (integrator == OB_INTEGRATOR_YOSHIDA4) {
+            double outer = 0.0, inner = 0.0;
+            yoshida_weights(outer, inner);
+            h[0] = outer * dt;
+            h[1] = inner * dt;
+            h[2] = outer * dt;
+            cycle = 3;
+        }
+        double *state[9];
+        for (int k = 0; k < 9; ++k) {
+            state[k] = array(kX + k);
+        }
+        const bool timed = fused_marks_.size() < ring_steps_;
+        std::pair<cudaEvent_t, cudaEvent_t> marks{nullptr, nullptr};
+        if (timed) {
+            check(cudaEventCreate(&marks.first), "creating an event");
+            check(cudaEventCreate(&marks.second), "creating an event");
+            fused_marks_.push_back(marks);
+            fused_mark_evals_.push_back(steps * static_cast<uint64_t>(cycle));
+            check(cudaEventRecord(marks.first, stream_), "timing the fused steps");
+        }
+        check(launch_fused_steps(state, array(kM), n_, steps, cycle, h,
+                                 static_cast<float>(solver_->params().softening_squared),
+                                 fused_buf_.data(), fused_barrier_.data(),
+                                 solver_->status_word(), stream_),
+              "fused integration steps");
+        if (timed) {
+            check(cudaEventRecord(marks.second, stream_), "timing the fused steps");
+        }
         solver_->account(steps * evaluations_per_step(integrator), n_);
         return;
     }
@@ -437,7 +519,7 @@ void System::step_host(int integrator, double dt, uint64_t steps, double *const 
     const double *in[9] = {io[0], io[1], io[2], io[3], io[4], io[5], io[6], io[7], io[8]};
     upload(kX, 9, in);
     upload(kM, 1, &m);
-    if (steps == 0 || n_ == 0) {
+    if (steps == 0 || n_ == 0 || fused_for(integrator)) {
         step_async(integrator, dt, steps);
         get_state(io);
         synchronize();
@@ -867,6 +949,16 @@ int ob_system_device_arrays(ob_system *system, void **arrays) {
         require(system != nullptr && arrays != nullptr, "NULL argument");
         for (int k = 0; k < 10; ++k) {
             arrays[k] = system->impl->size() == 0 ? nullptr : system->impl->array(k);
+        }
+    });
+}
+
+int ob_system_set_fused_steps(ob_system *system, int32_t enable, int32_t *active) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        const bool on = system->impl->set_fused_steps(enable != 0);
+        if (active != nullptr) {
+            *active = on ? 1 : 0;
         }
     });
 }

@@ -54,6 +54,8 @@ public:
 
     // Raises OB_ERROR_TIMEOUT if a kernel gave up on a bounded wait.
     void check_status(cudaStream_t stream);
+    // The device status word kernels of this solver's evaluations report to.
+    [[nodiscard]] unsigned *status_word() const noexcept { return status_.data(); }
 
     // Pair interactions the last direct evaluation computed, N(N-1).
     static uint64_t direct_pairs(uint64_t n) { return n > 1 ? n * (n - 1) : 0; }

@@ -8,6 +8,7 @@
 
 #include <cstdint>
 #include <memory>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -57,6 +58,12 @@ public:
 
     // Per-phase timing of graph replays (see ob_system_profile).
     void profile(uint32_t steps);
+
+    // Whole steps of a small FP32-direct system in one launch (fused.cu), used
+    // for velocity Verlet and Yoshida-4 where the system fits; on by default.
+    // Returns whether the next such step will use it.
+    bool set_fused_steps(bool enable);
+    bool fused_for(int integrator);
     ob_timings phase_times(uint32_t &evaluations);
     uint32_t step_kernels(int integrator, double dt);
 
@@ -101,6 +108,15 @@ private:
     std::vector<cudaEvent_t> marks_;
     std::vector<cudaGraphNode_t> mark_nodes_;
     static constexpr size_t kMarksPerStep = 16; // four per evaluation, RK4's four at most
+    // The fused small-system path: its position buffers and grid-barrier
+    // words, whether it is allowed and whether this system fits it (-1:
+    // not yet asked), and the event pairs timing its launches while profiling.
+    DeviceArray<float4> fused_buf_;
+    DeviceArray<unsigned> fused_barrier_;
+    bool fused_enabled_ = true;
+    int fused_fits_ = -1;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_marks_;
+    std::vector<uint64_t> fused_mark_evals_;
     std::vector<cudaEvent_t> ring_;
     uint32_t ring_steps_ = 0;     // capacity in steps
     uint32_t ring_used_ = 0;      // steps recorded
