@@ -459,8 +459,12 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
         if (fused_buf_.size() == 0) {
             fused_buf_.reserve(fused_scratch_floats4(n_));
             fused_barrier_.reserve(2);
-            check(cudaMemset(fused_barrier_.data(), 0, 2 * sizeof(unsigned)),
+            fused_barrier_reset_ = true;
+        }
+        if (fused_barrier_reset_) {
+            check(cudaMemsetAsync(fused_barrier_.data(), 0, 2 * sizeof(unsigned), stream_),
                   "clearing the grid barrier");
+            fused_barrier_reset_ = false;
         }
         double h[3] = {dt, dt, dt};
         int cycle = 1;
@@ -553,7 +557,14 @@ void System::step_host(int integrator, double dt, uint64_t steps, double *const 
 
 void System::synchronize() {
     check(cudaStreamSynchronize(stream_), "integrating");
-    solver_->check_status(stream_);
+    try {
+        solver_->check_status(stream_);
+    } catch (const Error &) {
+        // A fused launch that gave up on its grid barrier may have left the
+        // arrival count mid-way: clear it before the next fused launch.
+        fused_barrier_reset_ = true;
+        throw;
+    }
 }
 
 // Neumaier summation in index order, as core::CompensatedSum

@@ -114,6 +114,7 @@ private:
     DeviceArray<float4> fused_buf_;
     DeviceArray<unsigned> fused_barrier_;
     bool fused_enabled_ = true;
+    bool fused_barrier_reset_ = false; // clear the barrier words before the next fused launch
     int fused_fits_ = -1;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_marks_;
     std::vector<uint64_t> fused_mark_evals_;

@@ -320,8 +320,9 @@ __device__ __forceinline__ void cell_pair(const WarpSpace &ws, uint32_t p, float
     const float2 inv = f2((masks.x & lane_bit) != 0u ? inv0 : 0.0f,
                           (masks.y & lane_bit) != 0u ? inv1 : 0.0f);
     const float2 inv2 = __fmul2_rn(inv, inv);
+    const float2 inv3 = __fmul2_rn(inv2, inv);
     // Monopole m d / r^3 (tree_walk.hpp:129-140).
-    float2 coef = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), inv2);
+    float2 coef = __fmul2_rn(f2(q1.z, q1.w), inv3);
     if (QUAD) {
         // Quadrupole -Q d / r^5 + 2.5 (d.Q d) d / r^7 (tree_walk.hpp:142-181),
         // folded with the monopole: d (m / r^3 + 2.5 (d.Q d) / r^7) - Q d / r^5.
@@ -334,7 +335,7 @@ __device__ __forceinline__ void cell_pair(const WarpSpace &ws, uint32_t p, float
         const float2 qz = __ffma2_rn(xz, dx, __ffma2_rn(yz, dy, __fmul2_rn(zz, dz)));
         // q = 2.5 Q d, quadratic = 2.5 d.Q d.
         const float2 quadratic = __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
-        const float2 inv5 = __fmul2_rn(__fmul2_rn(inv2, inv2), inv);
+        const float2 inv5 = __fmul2_rn(inv3, inv2);
         coef = __ffma2_rn(quadratic, __fmul2_rn(inv5, inv2), coef);
         const float2 ninv5 = __fmul2_rn(inv5, f2(-0.4f, -0.4f));
         sx = __ffma2_rn(qx, ninv5, sx);
