@@ -428,11 +428,11 @@ bool System::fused_for(int integrator) {
         !(p.softening_squared > 0.0) || !(static_cast<float>(p.softening_squared) > 0.0f)) {
         return false;
     }
-    if (fused_fits_ < 0) {
-        fused_fits_ = fused_steps_fit(n_) ? 1 : 0;
+    if (fused_warps_ < 0) {
+        fused_warps_ = static_cast<int>(fused_steps_warps(n_));
         cudaGetLastError();
     }
-    return fused_fits_ == 1;
+    return fused_warps_ > 0;
 }
 
 uint32_t System::step_kernels(int integrator, double dt) {
@@ -492,7 +492,8 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
         check(launch_fused_steps(state, array(kM), n_, steps, cycle, h,
                                  static_cast<float>(solver_->params().softening_squared),
                                  fused_buf_.data(), fused_barrier_.data(),
-                                 solver_->status_word(), stream_),
+                                 solver_->status_word(), static_cast<uint32_t>(fused_warps_),
+                                 stream_),
               "fused integration steps");
         if (timed) {
             check(cudaEventRecord(marks.second, stream_), "timing the fused steps");

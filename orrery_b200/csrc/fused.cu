@@ -5,9 +5,10 @@
 // At a few thousand particles a step is four short launches (kick-drift,
 // source packing, forces, kick) whose launch gaps and thin force grid leave
 // most of the GPU idle. Here each CTA owns 32 targets (one per lane of each
-// warp) and keeps all N sources in shared memory; its sixteen warps each sum
-// one sixteenth of the sources for the same targets (the pair loop unrolled
-// so that independent pairs hide each other's latency). Per substep:
+// warp) and keeps all N sources in shared memory; its W warps (32 where the
+// grid fits one CTA per SM, else 16) each sum one W-th of the sources for the
+// same targets (the pair loop unrolled so that independent pairs hide each
+// other's latency). Per substep:
 //   A. each CTA kicks and drifts its own targets (the previous substep's
 //      closing kick first, as a separate rounding, then this substep's
 //      kick-drift: the same explicitly rounded FP64 operations, in the same
@@ -17,7 +18,7 @@
 //   C. each CTA loads all sources from buffer s % 2 into shared memory and
 //      evaluates its targets' accelerations: FP32 pair arithmetic two
 //      sources per packed FP32x2 instruction, each warp's slice summed in
-//      FP32, the sixteen slices added in FP64 in slice order.
+//      FP32, the W slices added in FP64 in slice order.
 // One barrier per substep suffices: a CTA can only write buffer (s + 2) % 2
 // after the barrier of substep s + 1, which every CTA reaches only after it
 // has finished loading buffer s % 2. After the last substep each CTA gives
@@ -40,10 +41,11 @@
 namespace ob {
 namespace {
 
-constexpr uint32_t kFusedWarps = 16;
-constexpr uint32_t kFusedThreads = kFusedWarps * 32;
 constexpr uint32_t kFusedTargets = 32; // per CTA: one per lane
-constexpr uint32_t kFusedGroup = 2 * kFusedWarps; // source padding: pairs per slice
+constexpr uint32_t kFusedMaxWarps = 32;
+// Source padding: a whole number of pairs per slice for 16 or 32 warps.
+constexpr uint32_t kFusedGroup = 2 * kFusedMaxWarps;
+constexpr size_t kFusedSmemCap = 200u * 1024u; // dynamic shared memory (sources)
 
 struct FusedArgs {
     double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
@@ -51,7 +53,7 @@ struct FusedArgs {
     float4 *buf0, *buf1; // FP32 x y z m per particle, double-buffered
     unsigned *barrier;   // [0] arrivals, [1] generation
     unsigned *status;
-    uint32_t n, padded;  // padded: a multiple of 2 * kFusedWarps
+    uint32_t n, padded;  // padded: a multiple of kFusedGroup
     uint32_t substeps;   // total substeps of the launch
     uint32_t cycle;      // substeps per step: 1 (velocity Verlet) or 3 (Yoshida-4)
     double h[3];         // substep timesteps of the cycle
@@ -97,10 +99,12 @@ __device__ __forceinline__ double kick(double v, double half, double a) {
     return __dadd_rn(v, __dmul_rn(half, a));
 }
 
-__global__ void __launch_bounds__(kFusedThreads)
+template <uint32_t WARPS>
+__global__ void __launch_bounds__(WARPS * 32)
     fused_steps_kernel(FusedArgs g) {
+    constexpr uint32_t kThreads = WARPS * 32;
     extern __shared__ __align__(16) float4 src[]; // pairs: (x0 x1 y0 y1) (z0 z1 m0 m1)
-    __shared__ double partial[kFusedWarps][3][kFusedTargets];
+    __shared__ double partial[WARPS][3][kFusedTargets];
     __shared__ unsigned generation_seen;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t first = blockIdx.x * kFusedTargets;
@@ -114,7 +118,7 @@ __global__ void __launch_bounds__(kFusedThreads)
     generation = generation_seen;
 
     const uint32_t pairs = g.padded / 2u;
-    const uint32_t slice = pairs / kFusedWarps; // pairs per warp
+    const uint32_t slice = pairs / WARPS; // pairs per warp
     const float2 e2 = f2(g.eps2, g.eps2);
     bool ok = true;
     for (uint32_t s = 0; s < g.substeps && ok; ++s) {
@@ -151,7 +155,7 @@ __global__ void __launch_bounds__(kFusedThreads)
             break;
         }
         // C. All sources into shared memory (zero-mass padding at the origin).
-        for (uint32_t p = threadIdx.x; p < pairs; p += kFusedThreads) {
+        for (uint32_t p = threadIdx.x; p < pairs; p += kThreads) {
             const uint32_t j = 2u * p;
             const float4 a = j < g.n ? __ldcg(&buf[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             const float4 b =
@@ -201,7 +205,7 @@ __global__ void __launch_bounds__(kFusedThreads)
         __syncthreads();
         if (warp == 0 && mine) {
             double a[3] = {0.0, 0.0, 0.0};
-            for (uint32_t w = 0; w < kFusedWarps; ++w) {
+            for (uint32_t w = 0; w < WARPS; ++w) {
                 for (int k = 0; k < 3; ++k) {
                     a[k] += partial[w][k][lane];
                 }
@@ -227,33 +231,41 @@ uint32_t fused_padded(uint32_t n) {
     return (n + kFusedGroup - 1u) / kFusedGroup * kFusedGroup;
 }
 
+// Whether a grid of `blocks` CTAs of the WARPS-warp kernel, with `smem` bytes
+// of sources, is resident at once (the cooperative launch requires it).
+template <uint32_t WARPS>
+bool fused_resident(uint64_t blocks, size_t smem, int sms) {
+    static std::atomic<uint64_t> configured{0};
+    const void *kernel = reinterpret_cast<const void *>(fused_steps_kernel<WARPS>);
+    int per_sm = 0;
+    if (set_smem_limit_once(kernel, static_cast<int>(kFusedSmemCap), configured) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, WARPS * 32, smem) !=
+            cudaSuccess) {
+        return false;
+    }
+    return blocks <= static_cast<uint64_t>(per_sm) * static_cast<uint64_t>(sms);
+}
+
 } // namespace
 
-bool fused_steps_fit(uint32_t n) {
+uint32_t fused_steps_warps(uint32_t n) {
     if (n < 2u) {
-        return false;
+        return 0u;
     }
-    const uint32_t padded = fused_padded(n);
-    const size_t smem = fused_smem(padded);
-    if (smem > 200u * 1024u) {
-        return false;
+    const size_t smem = fused_smem(fused_padded(n));
+    if (smem > kFusedSmemCap) {
+        return 0u;
     }
-    int device = 0, sms = 0, per_sm = 0;
+    int device = 0, sms = 0;
     if (cudaGetDevice(&device) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
-        return false;
-    }
-    static std::atomic<uint64_t> configured{0};
-    if (set_smem_limit_once(reinterpret_cast<const void *>(fused_steps_kernel),
-                            static_cast<int>(200u * 1024u), configured) != cudaSuccess) {
-        return false;
-    }
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_steps_kernel, kFusedThreads,
-                                                      smem) != cudaSuccess) {
-        return false;
+        return 0u;
     }
     const uint64_t blocks = (n + kFusedTargets - 1u) / kFusedTargets;
-    return blocks <= static_cast<uint64_t>(per_sm) * static_cast<uint64_t>(sms);
+    if (fused_resident<32>(blocks, smem, sms)) {
+        return 32u;
+    }
+    return fused_resident<16>(blocks, smem, sms) ? 16u : 0u;
 }
 
 size_t fused_scratch_floats4(uint32_t n) { return 2ull * fused_padded(n); }
@@ -261,9 +273,12 @@ size_t fused_scratch_floats4(uint32_t n) { return 2ull * fused_padded(n); }
 cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n,
                                uint64_t steps, int cycle, const double *h, float eps2,
                                float4 *scratch, unsigned *barrier, unsigned *status,
-                               cudaStream_t stream) {
+                               uint32_t warps, cudaStream_t stream) {
     if (n == 0 || steps == 0) {
         return cudaSuccess;
+    }
+    if (warps != 16u && warps != 32u) {
+        return cudaErrorInvalidValue;
     }
     FusedArgs g{};
     g.x = state[0];
@@ -294,8 +309,9 @@ cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n
     g.eps2 = eps2;
     const uint32_t blocks = (n + kFusedTargets - 1u) / kFusedTargets;
     void *args[] = {&g};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<const void *>(fused_steps_kernel),
-                                       dim3(blocks), dim3(kFusedThreads), args,
+    const void *kernel = warps == 32u ? reinterpret_cast<const void *>(fused_steps_kernel<32>)
+                                      : reinterpret_cast<const void *>(fused_steps_kernel<16>);
+    return cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(warps * 32u), args,
                                        fused_smem(g.padded), stream);
 }
 

@@ -6,6 +6,8 @@
     python -m orrery_b200.profile_driver batch       # 64 clusters (3 above 8192 particles)
                                                      # in chunked batched items
     python -m orrery_b200.profile_driver rk4         # two RK4 steps, Plummer 1,048,576
+    python -m orrery_b200.profile_driver fused       # FP32 direct system of 4096 particles:
+                                                     # single-launch velocity-Verlet steps
 
 Each runs a handful of launches of the kernels it names, on seeded synthetic
 inputs, and exits 0; a profiler then captures the launches it wants (for
@@ -64,6 +66,19 @@ def rk4() -> None:
     system.step(1e-4, 2, "rk4")
 
 
+def fused() -> None:
+    from . import DeviceSystem
+
+    n = 4096
+    d = ic.plummer_sphere(n, seed=7)
+    system = DeviceSystem(n, 0.01, precision="fp32")
+    if not system.set_fused_steps(True):
+        raise SystemExit("the single-launch steps do not apply to this system")
+    system.set_state(d["x"], d["y"], d["z"], d["vx"], d["vy"], d["vz"], d["m"])
+    for _ in range(4):
+        system.step(1e-3, 1, "vv")
+
+
 def main(argv: list[str]) -> None:
     from . import load_library
 
@@ -71,8 +86,8 @@ def main(argv: list[str]) -> None:
     what = argv[1] if len(argv) > 1 else ""
     if what == "tree":
         tree(int(argv[2]))
-    elif what in ("pack", "batch", "rk4"):
-        {"pack": pack, "batch": batch, "rk4": rk4}[what]()
+    elif what in ("pack", "batch", "rk4", "fused"):
+        {"pack": pack, "batch": batch, "rk4": rk4, "fused": fused}[what]()
     else:
         raise SystemExit(__doc__)
     print("ok", what)

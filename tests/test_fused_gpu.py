@@ -35,7 +35,9 @@ def _system(b200, d, eps=0.01, fused=True):
     return s, active
 
 
-@pytest.mark.parametrize("n", [2, 33, 1000, 4096])
+# 5500: more CTAs than SMs, so the launch takes the 16-warp kernel at two
+# CTAs per SM; the others take the 32-warp kernel.
+@pytest.mark.parametrize("n", [2, 33, 1000, 4096, 5500])
 @pytest.mark.parametrize("integrator,steps", [("vv", 10), ("yoshida4", 4)])
 def test_fused_steps_carry_forces_within_the_fp32_bounds(b200, restatement, n, integrator, steps):
     d = _plummer(n)
