@@ -1,5 +1,6 @@
 // The extern "C" boundary (include/orrery_b200.h) and the device-resident
 // system that integrates on the GPU.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <memory>
@@ -458,13 +459,15 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
     if (fused_for(integrator)) {
         if (fused_buf_.size() == 0) {
             fused_buf_.reserve(fused_scratch_floats4(n_));
-            fused_barrier_.reserve(2);
-            fused_barrier_reset_ = true;
+            fused_ready_.reserve(fused_ready_words(n_));
+            fused_ready_reset_ = true;
         }
-        if (fused_barrier_reset_) {
-            check(cudaMemsetAsync(fused_barrier_.data(), 0, 2 * sizeof(unsigned), stream_),
-                  "clearing the grid barrier");
-            fused_barrier_reset_ = false;
+        if (fused_ready_reset_) {
+            check(cudaMemsetAsync(fused_ready_.data(), 0,
+                                  fused_ready_words(n_) * sizeof(unsigned), stream_),
+                  "clearing the ready words");
+            fused_epoch_ = 0;
+            fused_ready_reset_ = false;
         }
         double h[3] = {dt, dt, dt};
         int cycle = 1;
@@ -489,12 +492,19 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
             fused_mark_evals_.push_back(steps * static_cast<uint64_t>(cycle));
             check(cudaEventRecord(marks.first, stream_), "timing the fused steps");
         }
-        check(launch_fused_steps(state, array(kM), n_, steps, cycle, h,
-                                 static_cast<float>(solver_->params().softening_squared),
-                                 fused_buf_.data(), fused_barrier_.data(),
-                                 solver_->status_word(), static_cast<uint32_t>(fused_warps_),
-                                 stream_),
-              "fused integration steps");
+        // At most 2^30 substeps per launch (ready words compare within 2^31).
+        const uint64_t per_launch = (uint64_t{1} << 30) / static_cast<uint64_t>(cycle);
+        for (uint64_t left = steps; left > 0;) {
+            const uint64_t chunk = std::min(left, per_launch);
+            check(launch_fused_steps(state, array(kM), n_, chunk, cycle, h,
+                                     static_cast<float>(solver_->params().softening_squared),
+                                     fused_buf_.data(), fused_ready_.data(), fused_epoch_,
+                                     solver_->status_word(),
+                                     static_cast<uint32_t>(fused_warps_), stream_),
+                  "fused integration steps");
+            fused_epoch_ += static_cast<uint32_t>(chunk * static_cast<uint64_t>(cycle));
+            left -= chunk;
+        }
         if (timed) {
             check(cudaEventRecord(marks.second, stream_), "timing the fused steps");
         }
@@ -561,9 +571,9 @@ void System::synchronize() {
     try {
         solver_->check_status(stream_);
     } catch (const Error &) {
-        // A fused launch that gave up on its grid barrier may have left the
-        // arrival count mid-way: clear it before the next fused launch.
-        fused_barrier_reset_ = true;
+        // A fused launch that gave up waiting may have left the ready words
+        // short of the host's substep count: clear both before the next one.
+        fused_ready_reset_ = true;
         throw;
     }
 }

@@ -8,29 +8,37 @@
 // warp) and keeps all N sources in shared memory; its W warps (32 where the
 // grid fits one CTA per SM, else 16) each sum one W-th of the sources for the
 // same targets (the pair loop unrolled so that independent pairs hide each
-// other's latency). Per substep:
-//   A. each CTA kicks and drifts its own targets (the previous substep's
+// other's latency). The FP64 state of the CTA's targets stays in shared
+// memory for the whole launch (read at the start, written back at the end).
+// Per substep:
+//   A. warp 0 kicks and drifts the CTA's targets (the previous substep's
 //      closing kick first, as a separate rounding, then this substep's
 //      kick-drift: the same explicitly rounded FP64 operations, in the same
-//      order, as kick_kernel and kick_drift_kernel) and writes their FP32
-//      positions and masses into buffer s % 2;
-//   B. a grid barrier: every position of the substep is written;
-//   C. each CTA loads all sources from buffer s % 2 into shared memory and
-//      evaluates its targets' accelerations: FP32 pair arithmetic two
-//      sources per packed FP32x2 instruction, each warp's slice summed in
-//      FP32, the W slices added in FP64 in slice order.
-// One barrier per substep suffices: a CTA can only write buffer (s + 2) % 2
-// after the barrier of substep s + 1, which every CTA reaches only after it
-// has finished loading buffer s % 2. After the last substep each CTA gives
-// its targets the closing kick.
+//      order, as kick_kernel and kick_drift_kernel), writes their FP32
+//      positions and masses into buffer s % 2 and then raises the CTA's
+//      ready word to this substep's number;
+//   B. every warp loads its share of the sources from buffer s % 2 into
+//      shared memory, each 32-source chunk once the ready word of the CTA
+//      that wrote it has reached this substep (no grid-wide barrier: a warp
+//      waits only for the chunks it loads);
+//   C. the CTA evaluates its targets' accelerations: FP32 pair arithmetic
+//      two sources per packed FP32x2 instruction, each warp's slice summed
+//      in FP32, the W slices added in FP64 in slice order by warp 0.
+// Double buffering is safe with per-CTA words: a CTA writes buffer s % 2
+// again only at substep s + 2, after its forces of substep s + 1, which need
+// every CTA's chunk of substep s + 1, which each CTA publishes only after it
+// has finished loading buffer s % 2. After the last substep warp 0 gives the
+// targets the closing kick and writes their state back.
 //
-// The grid barrier is a counter and a generation word in global memory; its
-// waits are bounded (kSpinLimit polls, then the timeout bit of the status
-// word and no further work), and the launch is cooperative, so every CTA is
-// resident. The pair arithmetic is that of the FP32 direct kernel (positions
-// rounded to FP32, softened, FP32 sums per slice, FP64 across slices); with
-// softening the target's own entry adds exactly zero unless m / eps^3 of the
-// target overflows FP32, in which case the warp skips it explicitly.
+// Ready words count substeps across launches (the host passes the count so
+// far, `epoch`, and clears the words together with it); waits are bounded
+// (kSpinLimit polls, then the timeout bit of the status word, and every CTA
+// stops after the substep it is in), and the launch is cooperative, so every
+// CTA is resident. The pair arithmetic is that of the FP32 direct kernel
+// (positions rounded to FP32, softened, FP32 sums per slice, FP64 across
+// slices); with softening the target's own entry adds exactly zero unless
+// m / eps^3 of the target overflows FP32, in which case the warp skips it
+// explicitly.
 #include <algorithm>
 #include <atomic>
 
@@ -46,16 +54,22 @@ constexpr uint32_t kFusedMaxWarps = 32;
 // Source padding: a whole number of pairs per slice for 16 or 32 warps.
 constexpr uint32_t kFusedGroup = 2 * kFusedMaxWarps;
 constexpr size_t kFusedSmemCap = 200u * 1024u; // dynamic shared memory (sources)
+// Every warp's chunks have their ready words polled by one lane each.
+static_assert(kFusedSmemCap / 16u / 32u / 16u <= 32u, "at most 32 chunks per warp");
+// Ready words one 128-byte line apart: polls of different CTAs' words then go
+// to different L2 lines instead of queueing on a few.
+constexpr uint32_t kReadyStride = 32;
 
 struct FusedArgs {
     double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
     const double *m;
     float4 *buf0, *buf1; // FP32 x y z m per particle, double-buffered
-    unsigned *barrier;   // [0] arrivals, [1] generation
+    unsigned *ready;     // per CTA (kReadyStride apart): substeps published, across launches
     unsigned *status;
     uint32_t n, padded;  // padded: a multiple of kFusedGroup
     uint32_t substeps;   // total substeps of the launch
     uint32_t cycle;      // substeps per step: 1 (velocity Verlet) or 3 (Yoshida-4)
+    uint32_t epoch;      // substeps published by earlier launches since the words were cleared
     double h[3];         // substep timesteps of the cycle
     double half[3];      // their halves, computed on the host as the unfused path does
     float eps2;
@@ -63,107 +77,134 @@ struct FusedArgs {
 
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
-// Waits until every CTA of the grid has arrived. Returns false when the wait
-// ran out (the timeout bit is then set).
-__device__ bool grid_barrier(unsigned *barrier, unsigned &generation, unsigned *status) {
-    __shared__ int ok;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        ok = 1;
-        const unsigned target = generation + 1u;
-        __threadfence();
-        const unsigned arrived = atomicAdd(&barrier[0], 1u);
-        if (arrived == gridDim.x - 1u) {
-            barrier[0] = 0u;
-            __threadfence();
-            atomicExch(&barrier[1], target);
-        } else {
-            uint32_t polls = 0;
-            while (*reinterpret_cast<volatile unsigned *>(&barrier[1]) != target) {
-                if (++polls > kSpinLimit) {
-                    atomicOr(status, kStatusTimeout);
-                    ok = 0;
-                    break;
-                }
-            }
-        }
-        __threadfence();
-        generation = target;
-    }
-    __syncthreads();
-    return ok != 0;
-}
-
 // Kick: v += half a (kick_kernel's rounding).
 __device__ __forceinline__ double kick(double v, double half, double a) {
     return __dadd_rn(v, __dmul_rn(half, a));
 }
 
+// Whether a ready word has reached `target` (the counts wrap at 2^32).
+__device__ __forceinline__ bool reached(unsigned word, unsigned target) {
+    return static_cast<int>(word - target) >= 0;
+}
+
+// A ready word, read with acquire semantics at GPU scope: this thread's later
+// loads see every write the publishing CTA made before raising it.
+__device__ __forceinline__ unsigned load_acquire(const unsigned *word) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(word) : "memory");
+    return v;
+}
+
+// Raises a ready word with release semantics at GPU scope.
+__device__ __forceinline__ void store_release(unsigned *word, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" : : "l"(word), "r"(v) : "memory");
+}
+
 template <uint32_t WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
     fused_steps_kernel(FusedArgs g) {
-    constexpr uint32_t kThreads = WARPS * 32;
     extern __shared__ __align__(16) float4 src[]; // pairs: (x0 x1 y0 y1) (z0 z1 m0 m1)
     __shared__ double partial[WARPS][3][kFusedTargets];
-    __shared__ unsigned generation_seen;
+    __shared__ double state[9][kFusedTargets]; // x y z vx vy vz ax ay az of the CTA's targets
+    __shared__ int stop;
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t first = blockIdx.x * kFusedTargets;
-    const uint32_t i = first + lane; // this lane's target in every warp
+    const uint32_t i = blockIdx.x * kFusedTargets + lane; // this lane's target in every warp
     const bool mine = i < g.n;
-    unsigned generation = 0;
+    double *const global_state[9] = {g.x, g.y, g.z, g.vx, g.vy, g.vz, g.ax, g.ay, g.az};
+    float mass = 0.0f;
+    if (warp == 0) {
+        for (int k = 0; k < 9; ++k) {
+            state[k][lane] = mine ? global_state[k][i] : 0.0;
+        }
+        mass = mine ? __double2float_rn(g.m[i]) : 0.0f;
+    }
     if (threadIdx.x == 0) {
-        generation_seen = *reinterpret_cast<volatile unsigned *>(&g.barrier[1]);
+        stop = 0;
     }
     __syncthreads();
-    generation = generation_seen;
-
-    const uint32_t pairs = g.padded / 2u;
-    const uint32_t slice = pairs / WARPS; // pairs per warp
+    const uint32_t blocks = gridDim.x;
+    const uint32_t chunks = g.padded / 32u; // 32-source chunks, padding included
+    const uint32_t slice = g.padded / 2u / WARPS; // pairs per warp
     const float2 e2 = f2(g.eps2, g.eps2);
-    bool ok = true;
-    for (uint32_t s = 0; s < g.substeps && ok; ++s) {
+    uint32_t s = 0;
+    for (; s < g.substeps; ++s) {
         const uint32_t c = s % g.cycle;
+        const unsigned target = g.epoch + s + 1u;
         float4 *buf = (s & 1u) != 0u ? g.buf1 : g.buf0;
-        // A. Kick and drift this CTA's targets (warp 0), write their FP32 copy.
-        if (warp == 0 && mine) {
-            double vx = g.vx[i], vy = g.vy[i], vz = g.vz[i];
-            const double ax = g.ax[i], ay = g.ay[i], az = g.az[i];
-            if (s > 0) {
-                const double hp = g.half[(s - 1u) % g.cycle];
-                vx = kick(vx, hp, ax);
-                vy = kick(vy, hp, ay);
-                vz = kick(vz, hp, az);
+        // A. Kick and drift this CTA's targets, publish their FP32 copy.
+        if (warp == 0) {
+            if (mine) {
+                double vx = state[3][lane], vy = state[4][lane], vz = state[5][lane];
+                const double ax = state[6][lane], ay = state[7][lane], az = state[8][lane];
+                if (s > 0) {
+                    const double hp = g.half[(s - 1u) % g.cycle];
+                    vx = kick(vx, hp, ax);
+                    vy = kick(vy, hp, ay);
+                    vz = kick(vz, hp, az);
+                }
+                vx = kick(vx, g.half[c], ax);
+                vy = kick(vy, g.half[c], ay);
+                vz = kick(vz, g.half[c], az);
+                const double x = __dadd_rn(state[0][lane], __dmul_rn(g.h[c], vx));
+                const double y = __dadd_rn(state[1][lane], __dmul_rn(g.h[c], vy));
+                const double z = __dadd_rn(state[2][lane], __dmul_rn(g.h[c], vz));
+                state[0][lane] = x;
+                state[1][lane] = y;
+                state[2][lane] = z;
+                state[3][lane] = vx;
+                state[4][lane] = vy;
+                state[5][lane] = vz;
+                buf[i] = make_float4(__double2float_rn(x), __double2float_rn(y),
+                                     __double2float_rn(z), mass);
             }
-            vx = kick(vx, g.half[c], ax);
-            vy = kick(vy, g.half[c], ay);
-            vz = kick(vz, g.half[c], az);
-            const double x = __dadd_rn(g.x[i], __dmul_rn(g.h[c], vx));
-            const double y = __dadd_rn(g.y[i], __dmul_rn(g.h[c], vy));
-            const double z = __dadd_rn(g.z[i], __dmul_rn(g.h[c], vz));
-            g.vx[i] = vx;
-            g.vy[i] = vy;
-            g.vz[i] = vz;
-            g.x[i] = x;
-            g.y[i] = y;
-            g.z[i] = z;
-            buf[i] = make_float4(__double2float_rn(x), __double2float_rn(y),
-                                 __double2float_rn(z), __double2float_rn(g.m[i]));
+            __threadfence();
+            __syncwarp();
+            if (lane == 0) {
+                store_release(&g.ready[blockIdx.x * kReadyStride], target);
+            }
         }
-        // B. Every position of this substep is written.
-        ok = grid_barrier(g.barrier, generation, g.status);
-        if (!ok) {
-            break;
+        // B. Sources into shared memory, chunk q = sources 32q .. 32q + 31
+        // (zero-mass padding at the origin past N), once the CTA that wrote
+        // each chunk has published it. Warp w loads chunks w, w + W, ...;
+        // lane k polls the ready word of the warp's k-th chunk (at most 32),
+        // and the warp barrier after the poll orders every lane's loads
+        // after the acquiring reads.
+        {
+            const uint32_t q = warp + WARPS * lane;
+            const bool polling = q < blocks && q < chunks;
+            for (uint32_t polls = 0;; ++polls) {
+                const bool behind =
+                    polling && !reached(load_acquire(&g.ready[q * kReadyStride]), target);
+                if (!__any_sync(0xffffffffu, behind)) {
+                    break;
+                }
+                if (polls >= kSpinLimit) {
+                    if (lane == 0) {
+                        atomicOr(g.status, kStatusTimeout);
+                        stop = 1;
+                    }
+                    break;
+                }
+            }
+            __syncwarp();
         }
-        // C. All sources into shared memory (zero-mass padding at the origin).
-        for (uint32_t p = threadIdx.x; p < pairs; p += kThreads) {
-            const uint32_t j = 2u * p;
+#pragma unroll 4
+        for (uint32_t q = warp; q < chunks; q += WARPS) {
+            const uint32_t j = 32u * q + lane;
             const float4 a = j < g.n ? __ldcg(&buf[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            const float4 b =
-                j + 1u < g.n ? __ldcg(&buf[j + 1u]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            src[2u * p] = make_float4(a.x, b.x, a.y, b.y);
-            src[2u * p + 1u] = make_float4(a.z, b.z, a.w, b.w);
+            // Slot j % 2 of pair j / 2: (x0 x1 y0 y1) (z0 z1 m0 m1).
+            float *lo = reinterpret_cast<float *>(&src[2u * (j >> 1)]) + (j & 1u);
+            float *hi = reinterpret_cast<float *>(&src[2u * (j >> 1) + 1u]) + (j & 1u);
+            lo[0] = a.x;
+            lo[2] = a.y;
+            hi[0] = a.z;
+            hi[2] = a.w;
         }
         __syncthreads();
+        if (stop != 0) {
+            break; // every thread reads the same word after the barrier
+        }
+        // C. This CTA's targets against every source.
         float tx = 0.0f, ty = 0.0f, tz = 0.0f, tm = 0.0f;
         if (mine) {
             const float4 q0 = src[2u * (i >> 1)], q1 = src[2u * (i >> 1) + 1u];
@@ -202,26 +243,34 @@ __global__ void __launch_bounds__(WARPS * 32)
         partial[warp][0][lane] = static_cast<double>(sx.x) + static_cast<double>(sx.y);
         partial[warp][1][lane] = static_cast<double>(sy.x) + static_cast<double>(sy.y);
         partial[warp][2][lane] = static_cast<double>(sz.x) + static_cast<double>(sz.y);
+        // The sources are read and the partials written: warp 0 adds the
+        // slices while the other warps go on to the next substep's loads,
+        // which wait for warp 0's next publication.
         __syncthreads();
-        if (warp == 0 && mine) {
+        if (warp == 0) {
             double a[3] = {0.0, 0.0, 0.0};
             for (uint32_t w = 0; w < WARPS; ++w) {
                 for (int k = 0; k < 3; ++k) {
                     a[k] += partial[w][k][lane];
                 }
             }
-            g.ax[i] = a[0];
-            g.ay[i] = a[1];
-            g.az[i] = a[2];
+            state[6][lane] = a[0];
+            state[7][lane] = a[1];
+            state[8][lane] = a[2];
         }
-        // The next substep reuses the shared arrays only after its barrier.
     }
-    // The closing kick of the last substep.
-    if (ok && warp == 0 && mine && g.substeps > 0) {
-        const double hp = g.half[(g.substeps - 1u) % g.cycle];
-        g.vx[i] = kick(g.vx[i], hp, g.ax[i]);
-        g.vy[i] = kick(g.vy[i], hp, g.ay[i]);
-        g.vz[i] = kick(g.vz[i], hp, g.az[i]);
+    // The closing kick of the last substep, and the state back to HBM (as
+    // far as it got when a wait ran out).
+    if (warp == 0 && mine) {
+        if (s == g.substeps && s > 0) {
+            const double hp = g.half[(s - 1u) % g.cycle];
+            state[3][lane] = kick(state[3][lane], hp, state[6][lane]);
+            state[4][lane] = kick(state[4][lane], hp, state[7][lane]);
+            state[5][lane] = kick(state[5][lane], hp, state[8][lane]);
+        }
+        for (int k = 0; k < 9; ++k) {
+            global_state[k][i] = state[k][lane];
+        }
     }
 }
 
@@ -248,6 +297,10 @@ bool fused_resident(uint64_t blocks, size_t smem, int sms) {
 
 } // namespace
 
+uint32_t fused_blocks(uint32_t n) { return (n + kFusedTargets - 1u) / kFusedTargets; }
+
+size_t fused_ready_words(uint32_t n) { return static_cast<size_t>(fused_blocks(n)) * kReadyStride; }
+
 uint32_t fused_steps_warps(uint32_t n) {
     if (n < 2u) {
         return 0u;
@@ -261,7 +314,7 @@ uint32_t fused_steps_warps(uint32_t n) {
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
         return 0u;
     }
-    const uint64_t blocks = (n + kFusedTargets - 1u) / kFusedTargets;
+    const uint64_t blocks = fused_blocks(n);
     if (fused_resident<32>(blocks, smem, sms)) {
         return 32u;
     }
@@ -272,13 +325,16 @@ size_t fused_scratch_floats4(uint32_t n) { return 2ull * fused_padded(n); }
 
 cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n,
                                uint64_t steps, int cycle, const double *h, float eps2,
-                               float4 *scratch, unsigned *barrier, unsigned *status,
-                               uint32_t warps, cudaStream_t stream) {
+                               float4 *scratch, unsigned *ready, uint32_t epoch,
+                               unsigned *status, uint32_t warps, cudaStream_t stream) {
     if (n == 0 || steps == 0) {
         return cudaSuccess;
     }
     if (warps != 16u && warps != 32u) {
         return cudaErrorInvalidValue;
+    }
+    if (steps * static_cast<uint64_t>(cycle) > 0x7fffffffull) {
+        return cudaErrorInvalidValue; // ready words compare within 2^31 substeps
     }
     FusedArgs g{};
     g.x = state[0];
@@ -294,24 +350,21 @@ cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n
     g.padded = fused_padded(n);
     g.buf0 = scratch;
     g.buf1 = scratch + g.padded;
-    g.barrier = barrier;
+    g.ready = ready;
     g.status = status;
     g.n = n;
     g.cycle = static_cast<uint32_t>(cycle);
-    if (steps * static_cast<uint64_t>(cycle) > 0xffffffffull) {
-        return cudaErrorInvalidValue;
-    }
+    g.epoch = epoch;
     g.substeps = static_cast<uint32_t>(steps * static_cast<uint64_t>(cycle));
     for (int k = 0; k < cycle && k < 3; ++k) {
         g.h[k] = h[k];
         g.half[k] = h[k] / 2.0; // as enqueue_substep computes it
     }
     g.eps2 = eps2;
-    const uint32_t blocks = (n + kFusedTargets - 1u) / kFusedTargets;
     void *args[] = {&g};
     const void *kernel = warps == 32u ? reinterpret_cast<const void *>(fused_steps_kernel<32>)
                                       : reinterpret_cast<const void *>(fused_steps_kernel<16>);
-    return cudaLaunchCooperativeKernel(kernel, dim3(blocks), dim3(warps * 32u), args,
+    return cudaLaunchCooperativeKernel(kernel, dim3(fused_blocks(n)), dim3(warps * 32u), args,
                                        fused_smem(g.padded), stream);
 }
 

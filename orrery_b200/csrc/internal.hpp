@@ -42,14 +42,17 @@ cudaError_t launch_direct_f32(const float4 *sources, uint32_t n, uint32_t padded
 // (velocity Verlet: 1, Yoshida-4: 3), state = x y z vx vy vz ax ay az.
 // fused_steps_warps(n) gives the warps per CTA of a grid that is resident at
 // once (32 or 16), or 0 when the system does not fit; the caller passes it to
-// the launch. `scratch` holds fused_scratch_floats4(n) float4 and `barrier`
-// two words zeroed once.
+// the launch. `scratch` holds fused_scratch_floats4(n) float4; `ready` holds
+// fused_ready_words(n) words, zeroed together with the caller's substep count
+// `epoch`, which then grows by steps * cycle per launch.
 uint32_t fused_steps_warps(uint32_t n);
+uint32_t fused_blocks(uint32_t n);
+size_t fused_ready_words(uint32_t n);
 size_t fused_scratch_floats4(uint32_t n);
 cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n,
                                uint64_t steps, int cycle, const double *h, float eps2,
-                               float4 *scratch, unsigned *barrier, unsigned *status,
-                               uint32_t warps, cudaStream_t stream);
+                               float4 *scratch, unsigned *ready, uint32_t epoch,
+                               unsigned *status, uint32_t warps, cudaStream_t stream);
 
 // Precision form: hi/lo split positions, Kahan FP32 partials, FP64 tiles.
 cudaError_t launch_direct_split(const float4 *hi, const float4 *lo, uint32_t n, uint32_t padded,

@@ -108,14 +108,15 @@ private:
     std::vector<cudaEvent_t> marks_;
     std::vector<cudaGraphNode_t> mark_nodes_;
     static constexpr size_t kMarksPerStep = 16; // four per evaluation, RK4's four at most
-    // The fused small-system path: its position buffers and grid-barrier
-    // words, whether it is allowed, the warps per CTA of its launch (0: this
-    // system does not fit it; -1: not yet asked), and the event pairs timing
-    // its launches while profiling.
+    // The fused small-system path: its position buffers and ready words,
+    // whether it is allowed, the warps per CTA of its launch (0: this system
+    // does not fit it; -1: not yet asked), and the event pairs timing its
+    // launches while profiling.
     DeviceArray<float4> fused_buf_;
-    DeviceArray<unsigned> fused_barrier_;
+    DeviceArray<unsigned> fused_ready_; // per CTA: substeps published (fused.cu)
+    uint32_t fused_epoch_ = 0;          // substeps launched since the words were cleared
     bool fused_enabled_ = true;
-    bool fused_barrier_reset_ = false; // clear the barrier words before the next fused launch
+    bool fused_ready_reset_ = false;    // clear the ready words before the next fused launch
     int fused_warps_ = -1;
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_marks_;
     std::vector<uint64_t> fused_mark_evals_;
