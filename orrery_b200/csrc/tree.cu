@@ -37,16 +37,18 @@ namespace {
 constexpr uint32_t kLevels = 21;
 constexpr uint32_t kThreads = 256;
 
-__device__ __forceinline__ int common_levels(const unsigned long long *codes, uint32_t b) {
-    if (b == 0) {
-        return -1;
-    }
-    const unsigned long long x = codes[b] ^ codes[b - 1];
+// Leading octal digits (levels) that codes a and b share; kLevels when equal.
+__device__ __forceinline__ int shared_levels(unsigned long long a, unsigned long long b) {
+    const unsigned long long x = a ^ b;
     if (x == 0ull) {
         return static_cast<int>(kLevels);
     }
     const int high = 63 - __clzll(static_cast<long long>(x));
     return 20 - high / 3;
+}
+
+__device__ __forceinline__ int common_levels(const unsigned long long *codes, uint32_t b) {
+    return b == 0 ? -1 : shared_levels(codes[b], codes[b - 1]);
 }
 
 __device__ __forceinline__ unsigned long long prefix(unsigned long long code, uint32_t level) {
@@ -106,7 +108,45 @@ __device__ uint32_t cell_start(const unsigned long long *codes, uint32_t i, uint
     return hi;
 }
 
+// max(first index of the level-`level` cell holding i, i - cap): a binary
+// search over the cap + 1 codes up to i (the cell is a contiguous run of the
+// sorted codes).
+__device__ uint32_t clipped_start(const unsigned long long *codes, uint32_t i, uint32_t level,
+                                  uint32_t cap) {
+    const unsigned long long code = codes[i];
+    uint32_t lo = i > cap ? i - cap : 0u, hi = i; // codes[hi] is inside
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (shared_levels(codes[mid], code) >= static_cast<int>(level)) {
+            hi = mid;
+        } else {
+            lo = mid + 1u;
+        }
+    }
+    return lo;
+}
+
+// min(end of the level-`level` cell whose first particle is b, b + cap + 1, n):
+// the exact end when the cell holds at most cap particles.
+__device__ uint32_t clipped_end(const unsigned long long *codes, uint32_t n, uint32_t b,
+                                uint32_t level, uint32_t cap) {
+    const unsigned long long code = codes[b];
+    uint32_t lo = b + 1u, hi = min(b + cap + 1u, n); // the end lies in [lo, hi]
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2u;
+        if (shared_levels(codes[mid], code) >= static_cast<int>(level)) {
+            lo = mid + 1u;
+        } else {
+            hi = mid;
+        }
+    }
+    return lo;
+}
+
 // The run of node levels starting at particle b: [lo, hi], or lo > hi for none.
+// A level-L cell whose first particle is f holds more than cap particles
+// exactly when codes[f + cap] exists and shares L levels with codes[f], so
+// each size test is one probe rather than a search for the cell's end.
 __device__ void node_run(const unsigned long long *codes, uint32_t n, uint32_t cap, uint32_t b,
                          int &c, uint32_t &lo, uint32_t &hi) {
     c = common_levels(codes, b);
@@ -116,10 +156,12 @@ __device__ void node_run(const unsigned long long *codes, uint32_t n, uint32_t c
             hi = 0;
             return;
         }
+        // The enclosing level-c cell holds b - 1 and b and is split when it
+        // holds more than cap particles; from a start clipped to b - 1 - cap
+        // the probe at start + cap = b - 1 lies inside, as it should.
         const uint32_t level = static_cast<uint32_t>(c);
-        const uint32_t start = cell_start(codes, b - 1, level);
-        const uint32_t end = cell_end(codes, n, b, level);
-        if (end - start <= cap) {
+        const uint32_t start = clipped_start(codes, b - 1, level, cap);
+        if (!(start + cap < n && shared_levels(codes[start], codes[start + cap]) >= c)) {
             lo = 1;
             hi = 0;
             return;
@@ -128,15 +170,15 @@ __device__ void node_run(const unsigned long long *codes, uint32_t n, uint32_t c
     } else {
         lo = 0;
     }
-    uint32_t level = lo;
-    while (true) {
-        const uint32_t end = cell_end(codes, n, b, level);
-        if (end - b <= cap || level >= kLevels) {
-            break;
-        }
-        ++level;
+    // The cells starting at b hold more than cap particles at the levels up
+    // to shared_levels(codes[b], codes[b + cap]); the run ends at the first
+    // level past them (or at the deepest level).
+    if (b + cap >= n) {
+        hi = lo;
+    } else {
+        const uint32_t split = static_cast<uint32_t>(shared_levels(codes[b], codes[b + cap]));
+        hi = max(lo, min(split + 1u, kLevels));
     }
-    hi = level;
 }
 
 __global__ void __launch_bounds__(kThreads)
@@ -153,8 +195,8 @@ __global__ void __launch_bounds__(kThreads)
 __global__ void __launch_bounds__(kThreads)
     layout_write_kernel(const unsigned long long *__restrict__ codes, uint32_t n, uint32_t cap,
                         const uint32_t *__restrict__ offsets, uint32_t capacity,
-                        DeviceNode *nodes, uint32_t *children, TreeMeta *meta,
-                        unsigned *status) {
+                        DeviceNode *nodes, uint32_t *children, uint32_t *child_slots,
+                        TreeMeta *meta, unsigned *status) {
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const uint32_t total = offsets[n];
         meta->node_count = total <= capacity ? total : 0u;
@@ -188,8 +230,10 @@ __global__ void __launch_bounds__(kThreads)
             parent = offsets[start] + (level - first_level);
         }
         for (uint32_t level = lo; level <= hi; ++level, ++index) {
-            const uint32_t end = cell_end(codes, n, b, level);
             const bool leaf = level == hi;
+            // A leaf above the deepest level holds at most cap particles.
+            const uint32_t end = leaf && level < kLevels ? clipped_end(codes, n, b, level, cap)
+                                                         : cell_end(codes, n, b, level);
             DeviceNode node;
             node.com_x = node.com_y = node.com_z = 0.0;
             node.r2 = 0.0;
@@ -202,7 +246,14 @@ __global__ void __launch_bounds__(kThreads)
             node.pad = 0;
             nodes[index] = node;
             if (parent != index) {
-                atomicAdd(&children[parent], 1u);
+                // A cell has at most eight children; their slots are filled
+                // in arrival order and sorted by the moments pass.
+                const uint32_t slot = atomicAdd(&children[parent], 1u);
+                if (slot < kMaxChildren) {
+                    child_slots[static_cast<size_t>(parent) * kMaxChildren + slot] = index;
+                } else {
+                    atomicOr(status, kStatusInvalid);
+                }
             }
             parent = index;
             if (leaf) {
@@ -224,7 +275,9 @@ __global__ void __launch_bounds__(kThreads)
 
 // Geometric centre and edge of the cell at `level` holding `code`, by the
 // reference's recursion: child centre = centre +- size/4 per axis, child size
-// = size/2 (octree.cpp:41-47, 305-310).
+// = size/2 (octree.cpp:41-47, 305-310). Division by 4 or 2 is multiplication
+// by the exact reciprocal (both give the correctly rounded quotient), so the
+// divisions are written as one multiplication each.
 __device__ void cell_geometry(const TreeMeta *meta, unsigned long long code, uint32_t level,
                               double c[3], double &size) {
     c[0] = meta->root_centre[0];
@@ -233,11 +286,11 @@ __device__ void cell_geometry(const TreeMeta *meta, unsigned long long code, uin
     size = meta->size;
     for (uint32_t l = 1; l <= level; ++l) {
         const uint32_t octant = static_cast<uint32_t>((code >> (3u * (kLevels - l))) & 7u);
-        const double quarter = __ddiv_rn(size, 4.0);
+        const double quarter = __dmul_rn(size, 0.25);
         c[0] = __dadd_rn(c[0], (octant & 4u) ? quarter : -quarter);
         c[1] = __dadd_rn(c[1], (octant & 2u) ? quarter : -quarter);
         c[2] = __dadd_rn(c[2], (octant & 1u) ? quarter : -quarter);
-        size = __ddiv_rn(size, 2.0);
+        size = __dmul_rn(size, 0.5);
     }
 }
 
@@ -273,12 +326,17 @@ __device__ double acceptance(const TreeMeta *meta, unsigned long long code, uint
     return __dmul_rn(radius, radius);
 }
 
-// Escape index of a child; an index that does not move forward (never
-// produced by the layout) ends the loop instead of repeating forever.
-__device__ __forceinline__ uint32_t next_child(const DeviceNode *nodes, uint32_t child,
-                                               uint32_t stop) {
-    const uint32_t next = __ldcg(&nodes[child].next);
-    return next > child ? next : stop;
+// Sorts eight values in registers (Batcher's odd-even merge network).
+__device__ __forceinline__ void sort8(uint32_t (&v)[8]) {
+    constexpr int kPairs[19][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3}, {4, 6},
+                                   {5, 7}, {1, 2}, {5, 6}, {0, 4}, {1, 5}, {2, 6}, {3, 7},
+                                   {2, 4}, {3, 5}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+    for (int p = 0; p < 19; ++p) {
+        const uint32_t a = v[kPairs[p][0]], b = v[kPairs[p][1]];
+        v[kPairs[p][0]] = min(a, b);
+        v[kPairs[p][1]] = max(a, b);
+    }
 }
 
 // Writes the walk's compact record of node k (see WalkNode). `sibling`: the
@@ -315,7 +373,8 @@ __device__ void store_walk_node(WalkNode *walk, uint32_t *first_of, uint32_t k,
 __global__ void __launch_bounds__(kThreads)
     moments_kernel(const double *__restrict__ sorted, const unsigned long long *__restrict__ codes,
                    uint32_t n, DeviceNode *nodes, DeviceQuadrupole *quads, WalkNode *walk,
-                   uint32_t *first_of, const uint32_t *__restrict__ children, uint32_t *arrived,
+                   uint32_t *first_of, const uint32_t *__restrict__ children,
+                   const uint32_t *__restrict__ child_slots, uint32_t *arrived,
                    float4 *leaf_rel, TreeMeta *meta, double theta) {
     const double *X = sorted;
     const double *Y = sorted + n;
@@ -392,22 +451,36 @@ __global__ void __launch_bounds__(kThreads)
             }
             __threadfence();
             const uint32_t stop = __ldcg(&nodes[parent].next);
+            // The parent's children in index (octant) order: its slots,
+            // sorted, so that their loads need no walk along escape indices.
+            const uint32_t kids = min(children[parent], kMaxChildren);
+            const uint4 *slots =
+                reinterpret_cast<const uint4 *>(child_slots + static_cast<size_t>(parent) *
+                                                                  kMaxChildren);
+            const uint4 s0 = __ldcg(slots), s1 = __ldcg(slots + 1);
+            uint32_t kid[kMaxChildren] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
+#pragma unroll
+            for (uint32_t k = 0; k < kMaxChildren; ++k) {
+                kid[k] = k < kids && kid[k] < count_nodes ? kid[k] : 0xffffffffu;
+            }
+            sort8(kid);
             double pm = 0.0, px = 0.0, py = 0.0, pz = 0.0, mx = 0.0, my = 0.0, mz = 0.0;
-            uint32_t kids = 0;
-            for (uint32_t child = parent + 1; child < stop;
-                 child = next_child(nodes, child, stop)) {
-                const double cm = __ldcg(&nodes[child].mass);
-                const double ccx = __ldcg(&nodes[child].com_x);
-                const double ccy = __ldcg(&nodes[child].com_y);
-                const double ccz = __ldcg(&nodes[child].com_z);
-                pm = __dadd_rn(pm, cm);
-                px = __dadd_rn(px, __dmul_rn(ccx, cm));
-                py = __dadd_rn(py, __dmul_rn(ccy, cm));
-                pz = __dadd_rn(pz, __dmul_rn(ccz, cm));
-                mx = __dadd_rn(mx, ccx);
-                my = __dadd_rn(my, ccy);
-                mz = __dadd_rn(mz, ccz);
-                ++kids;
+#pragma unroll
+            for (uint32_t k = 0; k < kMaxChildren; ++k) {
+                if (kid[k] != 0xffffffffu) {
+                    const uint32_t child = kid[k];
+                    const double cm = __ldcg(&nodes[child].mass);
+                    const double ccx = __ldcg(&nodes[child].com_x);
+                    const double ccy = __ldcg(&nodes[child].com_y);
+                    const double ccz = __ldcg(&nodes[child].com_z);
+                    pm = __dadd_rn(pm, cm);
+                    px = __dadd_rn(px, __dmul_rn(ccx, cm));
+                    py = __dadd_rn(py, __dmul_rn(ccy, cm));
+                    pz = __dadd_rn(pz, __dmul_rn(ccz, cm));
+                    mx = __dadd_rn(mx, ccx);
+                    my = __dadd_rn(my, ccy);
+                    mz = __dadd_rn(mz, ccz);
+                }
             }
             double gx, gy, gz;
             if (pm > 0.0) {
@@ -422,18 +495,21 @@ __global__ void __launch_bounds__(kThreads)
             }
             if (with_quads) {
                 DeviceQuadrupole moment{0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-                for (uint32_t child = parent + 1; child < stop;
-                     child = next_child(nodes, child, stop)) {
-                    moment.xx = __dadd_rn(moment.xx, __ldcg(&quads[child].xx));
-                    moment.xy = __dadd_rn(moment.xy, __ldcg(&quads[child].xy));
-                    moment.xz = __dadd_rn(moment.xz, __ldcg(&quads[child].xz));
-                    moment.yy = __dadd_rn(moment.yy, __ldcg(&quads[child].yy));
-                    moment.yz = __dadd_rn(moment.yz, __ldcg(&quads[child].yz));
-                    moment.zz = __dadd_rn(moment.zz, __ldcg(&quads[child].zz));
-                    add_displaced(moment, __ldcg(&nodes[child].mass),
-                                  __dsub_rn(__ldcg(&nodes[child].com_x), gx),
-                                  __dsub_rn(__ldcg(&nodes[child].com_y), gy),
-                                  __dsub_rn(__ldcg(&nodes[child].com_z), gz));
+#pragma unroll
+                for (uint32_t k = 0; k < kMaxChildren; ++k) {
+                    if (kid[k] != 0xffffffffu) {
+                        const uint32_t child = kid[k];
+                        moment.xx = __dadd_rn(moment.xx, __ldcg(&quads[child].xx));
+                        moment.xy = __dadd_rn(moment.xy, __ldcg(&quads[child].xy));
+                        moment.xz = __dadd_rn(moment.xz, __ldcg(&quads[child].xz));
+                        moment.yy = __dadd_rn(moment.yy, __ldcg(&quads[child].yy));
+                        moment.yz = __dadd_rn(moment.yz, __ldcg(&quads[child].yz));
+                        moment.zz = __dadd_rn(moment.zz, __ldcg(&quads[child].zz));
+                        add_displaced(moment, __ldcg(&nodes[child].mass),
+                                      __dsub_rn(__ldcg(&nodes[child].com_x), gx),
+                                      __dsub_rn(__ldcg(&nodes[child].com_y), gy),
+                                      __dsub_rn(__ldcg(&nodes[child].com_z), gz));
+                    }
                 }
                 quads[parent] = moment;
             }
@@ -476,22 +552,26 @@ cudaError_t launch_layout_count(const unsigned long long *codes, uint32_t n, uin
 
 cudaError_t launch_layout_write(const unsigned long long *codes, uint32_t n, uint32_t leaf_cap,
                                 const uint32_t *offsets, uint32_t node_capacity,
-                                DeviceNode *nodes, uint32_t *children, TreeMeta *meta,
-                                unsigned *status, cudaStream_t stream) {
+                                DeviceNode *nodes, uint32_t *children, uint32_t *child_slots,
+                                TreeMeta *meta, unsigned *status, cudaStream_t stream) {
     layout_write_kernel<<<grid_for(n), kThreads, 0, stream>>>(codes, n, leaf_cap, offsets,
                                                              node_capacity, nodes, children,
-                                                             meta, status);
+                                                             child_slots, meta, status);
     return cudaGetLastError();
 }
 
 cudaError_t launch_moments(const double *sorted, const unsigned long long *codes, uint32_t n,
                            DeviceNode *nodes, DeviceQuadrupole *quads, WalkNode *walk_nodes,
-                           uint32_t *first_of, const uint32_t *children, uint32_t *arrived,
-                           float4 *leaf_rel, TreeMeta *meta, double opening_angle,
-                           uint32_t node_capacity, cudaStream_t stream) {
+                           uint32_t *first_of, const uint32_t *children,
+                           const uint32_t *child_slots, uint32_t *arrived, float4 *leaf_rel,
+                           TreeMeta *meta, double opening_angle, uint32_t node_capacity,
+                           cudaStream_t stream) {
+    if (reinterpret_cast<uintptr_t>(child_slots) % 16u != 0u) {
+        return cudaErrorMisalignedAddress; // the climb reads a node's slots as two uint4
+    }
     moments_kernel<<<grid_for(node_capacity), kThreads, 0, stream>>>(
-        sorted, codes, n, nodes, quads, walk_nodes, first_of, children, arrived, leaf_rel, meta,
-        opening_angle);
+        sorted, codes, n, nodes, quads, walk_nodes, first_of, children, child_slots, arrived,
+        leaf_rel, meta, opening_angle);
     return cudaGetLastError();
 }
 
@@ -547,7 +627,10 @@ void TreePipeline::reserve(uint32_t n) {
         }
         walk_nodes_.reserve(want);
         first_of_.reserve(want);
-        level_lists_.reserve(2ull * want); // children counts, then arrivals
+        // kMaxChildren child slots per node (first, so that a node's slots
+        // start on a 16-byte boundary for their vector loads), then child
+        // counts and arrival counts.
+        level_lists_.reserve((kMaxChildren + 2ull) * want);
         node_capacity_ = want;
     }
 }
@@ -573,8 +656,8 @@ void TreePipeline::evaluate(uint32_t n, const double *x, const double *y, const 
           "clearing look-back words");
     check(cudaMemsetAsync(tile_counter_.data(), 0, sizeof(uint32_t) * kRadixPasses, stream),
           "clearing tile tickets");
-    check(cudaMemsetAsync(level_lists_.data(), 0, sizeof(uint32_t) * 2ull * node_capacity_,
-                          stream),
+    check(cudaMemsetAsync(level_lists_.data() + kMaxChildren * static_cast<size_t>(node_capacity_),
+                          0, sizeof(uint32_t) * 2ull * node_capacity_, stream),
           "clearing child counts");
 
     // Ordering: cube, codes + histograms, eight onesweep passes, gather.
@@ -604,15 +687,16 @@ void TreePipeline::evaluate(uint32_t n, const double *x, const double *y, const 
     uint32_t *offsets = node_start_.data() + n;
     check(launch_layout_count(codes, n, cap, counts, stream), "node counts");
     check(launch_exclusive_scan(counts, offsets, n, scan_partials_.data(), stream), "node scan");
-    uint32_t *children = level_lists_.data();
-    uint32_t *arrived = level_lists_.data() + node_capacity_;
+    uint32_t *child_slots = level_lists_.data();
+    uint32_t *children = child_slots + kMaxChildren * static_cast<size_t>(node_capacity_);
+    uint32_t *arrived = children + node_capacity_;
     check(launch_layout_write(codes, n, cap, offsets, node_capacity_, nodes_.data(), children,
-                              meta_.data(), status, stream),
+                              child_slots, meta_.data(), status, stream),
           "node layout");
     check(launch_moments(sorted_.data(), codes, n, nodes_.data(),
                          params_.quadrupole ? quads_.data() : nullptr, walk_nodes_.data(),
-                         first_of_.data(), children, arrived, leaf_rel_.data(), meta_.data(),
-                         params_.opening_angle, node_capacity_, stream),
+                         first_of_.data(), children, child_slots, arrived, leaf_rel_.data(),
+                         meta_.data(), params_.opening_angle, node_capacity_, stream),
           "moments");
     record(built, stream, external);
 

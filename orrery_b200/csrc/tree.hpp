@@ -138,7 +138,7 @@ private:
     DeviceArray<DeviceQuadrupole> quads_;        // FP64 moments (parity, upward pass)
     DeviceArray<WalkNode> walk_nodes_;           // compact FP32 node records the walk reads
     DeviceArray<uint32_t> first_of_;             // first particle of each node (leaves)
-    DeviceArray<uint32_t> level_lists_;          // child counts, then arrival counts
+    DeviceArray<uint32_t> level_lists_;          // child slots, child counts, arrival counts
     DeviceArray<TreeMeta> meta_;
     DeviceArray<double> reduce_;                 // cube min/max partials
     DeviceArray<unsigned long long> counters_;   // pair and cell counts (accumulating)

@@ -75,20 +75,23 @@ cudaError_t launch_exclusive_scan(const uint32_t *in, uint32_t *out, uint32_t n,
 cudaError_t launch_layout_count(const unsigned long long *codes, uint32_t n, uint32_t leaf_cap,
                                 uint32_t *counts, cudaStream_t stream);
 
-// Writes the node records (escape, first, count, level, parent) and counts
-// each internal node's children. `offsets` is the exclusive scan of counts.
+// Writes the node records (escape, first, count, level, parent), counts each
+// internal node's children and lists them (in arrival order) in its
+// kMaxChildren slots of child_slots. `offsets` is the exclusive scan of counts.
+constexpr uint32_t kMaxChildren = 8;
 cudaError_t launch_layout_write(const unsigned long long *codes, uint32_t n, uint32_t leaf_cap,
                                 const uint32_t *offsets, uint32_t node_capacity,
-                                DeviceNode *nodes, uint32_t *children, TreeMeta *meta,
-                                unsigned *status, cudaStream_t stream);
+                                DeviceNode *nodes, uint32_t *children, uint32_t *child_slots,
+                                TreeMeta *meta, unsigned *status, cudaStream_t stream);
 
 // Moments bottom-up (mass, centre of mass, quadrupole, acceptance radius) and
 // the leaf-relative FP32 source positions the walk reads.
 cudaError_t launch_moments(const double *sorted, const unsigned long long *codes, uint32_t n,
                            DeviceNode *nodes, DeviceQuadrupole *quads, WalkNode *walk_nodes,
-                           uint32_t *first_of, const uint32_t *children, uint32_t *arrived,
-                           float4 *leaf_rel, TreeMeta *meta, double opening_angle,
-                           uint32_t node_capacity, cudaStream_t stream);
+                           uint32_t *first_of, const uint32_t *children,
+                           const uint32_t *child_slots, uint32_t *arrived, float4 *leaf_rel,
+                           TreeMeta *meta, double opening_angle, uint32_t node_capacity,
+                           cudaStream_t stream);
 
 // ------------------------------------------------------------------- walk
 
