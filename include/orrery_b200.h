@@ -548,6 +548,15 @@ int ob_test_lookback_timeout(uint64_t n, uint32_t poll_limit, int skip_first_til
  * or FP64 solvers. No reference counterpart. */
 int ob_test_set_walk_stack_cap(ob_solver *solver, uint32_t cap);
 
+/* Arms the next fused launch of `system` (ob_system_set_fused_steps) for a
+ * test of its bounded wait: that launch polls each ready word at most
+ * `poll_limit` times and its first CTA never publishes its positions, so the
+ * other CTAs' waits run out, the launch sets its timeout bit and the step
+ * returns OB_ERROR_TIMEOUT, the device staying usable; the launch after it
+ * clears the ready words and steps normally. OB_ERROR_UNSUPPORTED when the
+ * system does not take fused steps. No reference counterpart. */
+int ob_test_fused_timeout(ob_system *system, uint32_t poll_limit);
+
 #ifdef __cplusplus
 }
 #endif

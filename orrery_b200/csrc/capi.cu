@@ -422,6 +422,14 @@ bool System::set_fused_steps(bool enable) {
     return fused_for(OB_INTEGRATOR_VV);
 }
 
+bool System::arm_fused_timeout(uint32_t poll_limit) {
+    if (!fused_for(OB_INTEGRATOR_VV)) {
+        return false;
+    }
+    fused_test_polls_ = poll_limit;
+    return true;
+}
+
 bool System::fused_for(int integrator) {
     const ob_solver_params &p = solver_->params();
     if (!fused_enabled_ || (integrator != OB_INTEGRATOR_VV && integrator != OB_INTEGRATOR_YOSHIDA4) ||
@@ -496,11 +504,14 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
         const uint64_t per_launch = (uint64_t{1} << 30) / static_cast<uint64_t>(cycle);
         for (uint64_t left = steps; left > 0;) {
             const uint64_t chunk = std::min(left, per_launch);
+            const uint32_t polls = fused_test_polls_;
+            fused_test_polls_ = 0;
             check(launch_fused_steps(state, array(kM), n_, chunk, cycle, h,
                                      static_cast<float>(solver_->params().softening_squared),
                                      fused_buf_.data(), fused_ready_.data(), fused_epoch_,
                                      solver_->status_word(),
-                                     static_cast<uint32_t>(fused_warps_), stream_),
+                                     static_cast<uint32_t>(fused_warps_), stream_, polls,
+                                     polls != 0 ? 0u : ~0u),
                   "fused integration steps");
             fused_epoch_ += static_cast<uint32_t>(chunk * static_cast<uint64_t>(cycle));
             left -= chunk;
@@ -981,6 +992,16 @@ int ob_system_set_fused_steps(ob_system *system, int32_t enable, int32_t *active
         const bool on = system->impl->set_fused_steps(enable != 0);
         if (active != nullptr) {
             *active = on ? 1 : 0;
+        }
+    });
+}
+
+int ob_test_fused_timeout(ob_system *system, uint32_t poll_limit) {
+    return guarded([&] {
+        require(system != nullptr, "system is NULL");
+        require(poll_limit > 0, "the poll limit must be positive");
+        if (!system->impl->arm_fused_timeout(poll_limit)) {
+            throw ob::Error(OB_ERROR_UNSUPPORTED, "the system does not take fused steps");
         }
     });
 }

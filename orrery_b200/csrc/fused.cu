@@ -32,8 +32,8 @@
 //
 // Ready words count substeps across launches (the host passes the count so
 // far, `epoch`, and clears the words together with it); waits are bounded
-// (kSpinLimit polls, then the timeout bit of the status word, and every CTA
-// stops after the substep it is in), and the launch is cooperative, so every
+// (kSpinLimit polls, or fewer where a test asks, then the timeout bit of the
+// status word, and every CTA stops after the substep it is in), and the launch is cooperative, so every
 // CTA is resident. The pair arithmetic is that of the FP32 direct kernel
 // (positions rounded to FP32, softened, FP32 sums per slice, FP64 across
 // slices); with softening the target's own entry adds exactly zero unless
@@ -70,6 +70,8 @@ struct FusedArgs {
     uint32_t substeps;   // total substeps of the launch
     uint32_t cycle;      // substeps per step: 1 (velocity Verlet) or 3 (Yoshida-4)
     uint32_t epoch;      // substeps published by earlier launches since the words were cleared
+    uint32_t poll_limit; // polls of a ready word before the wait gives up (kSpinLimit)
+    uint32_t silent_cta; // a CTA that never publishes (tests of the bounded wait), or ~0
     double h[3];         // substep timesteps of the cycle
     double half[3];      // their halves, computed on the host as the unfused path does
     float eps2;
@@ -159,7 +161,7 @@ __global__ void __launch_bounds__(WARPS * 32)
             }
             __threadfence();
             __syncwarp();
-            if (lane == 0) {
+            if (lane == 0 && blockIdx.x != g.silent_cta) {
                 store_release(&g.ready[blockIdx.x * kReadyStride], target);
             }
         }
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(WARPS * 32)
                 if (!__any_sync(0xffffffffu, behind)) {
                     break;
                 }
-                if (polls >= kSpinLimit) {
+                if (polls >= g.poll_limit) {
                     if (lane == 0) {
                         atomicOr(g.status, kStatusTimeout);
                         stop = 1;
@@ -326,7 +328,8 @@ size_t fused_scratch_floats4(uint32_t n) { return 2ull * fused_padded(n); }
 cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n,
                                uint64_t steps, int cycle, const double *h, float eps2,
                                float4 *scratch, unsigned *ready, uint32_t epoch,
-                               unsigned *status, uint32_t warps, cudaStream_t stream) {
+                               unsigned *status, uint32_t warps, cudaStream_t stream,
+                               uint32_t poll_limit, uint32_t silent_cta) {
     if (n == 0 || steps == 0) {
         return cudaSuccess;
     }
@@ -355,6 +358,8 @@ cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n
     g.n = n;
     g.cycle = static_cast<uint32_t>(cycle);
     g.epoch = epoch;
+    g.poll_limit = poll_limit == 0u ? kSpinLimit : poll_limit;
+    g.silent_cta = silent_cta;
     g.substeps = static_cast<uint32_t>(steps * static_cast<uint64_t>(cycle));
     for (int k = 0; k < cycle && k < 3; ++k) {
         g.h[k] = h[k];

@@ -44,7 +44,9 @@ cudaError_t launch_direct_f32(const float4 *sources, uint32_t n, uint32_t padded
 // once (32 or 16), or 0 when the system does not fit; the caller passes it to
 // the launch. `scratch` holds fused_scratch_floats4(n) float4; `ready` holds
 // fused_ready_words(n) words, zeroed together with the caller's substep count
-// `epoch`, which then grows by steps * cycle per launch.
+// `epoch`, which then grows by steps * cycle per launch. poll_limit (0: the
+// library's limit) and silent_cta (a CTA that never publishes; ~0 for none)
+// exist for tests of the bounded wait.
 uint32_t fused_steps_warps(uint32_t n);
 uint32_t fused_blocks(uint32_t n);
 size_t fused_ready_words(uint32_t n);
@@ -52,7 +54,8 @@ size_t fused_scratch_floats4(uint32_t n);
 cudaError_t launch_fused_steps(double *const *state, const double *m, uint32_t n,
                                uint64_t steps, int cycle, const double *h, float eps2,
                                float4 *scratch, unsigned *ready, uint32_t epoch,
-                               unsigned *status, uint32_t warps, cudaStream_t stream);
+                               unsigned *status, uint32_t warps, cudaStream_t stream,
+                               uint32_t poll_limit = 0, uint32_t silent_cta = ~0u);
 
 // Precision form: hi/lo split positions, Kahan FP32 partials, FP64 tiles.
 cudaError_t launch_direct_split(const float4 *hi, const float4 *lo, uint32_t n, uint32_t padded,

@@ -63,6 +63,10 @@ public:
     // for velocity Verlet and Yoshida-4 where the system fits; on by default.
     // Returns whether the next such step will use it.
     bool set_fused_steps(bool enable);
+    // Tests of the fused launch's bounded wait: the next fused launch polls at
+    // most `poll_limit` times and its CTA 0 never publishes. Returns whether
+    // the system takes fused steps.
+    bool arm_fused_timeout(uint32_t poll_limit);
     bool fused_for(int integrator);
     ob_timings phase_times(uint32_t &evaluations);
     uint32_t step_kernels(int integrator, double dt);
@@ -118,6 +122,7 @@ private:
     bool fused_enabled_ = true;
     bool fused_ready_reset_ = false;    // clear the ready words before the next fused launch
     int fused_warps_ = -1;
+    uint32_t fused_test_polls_ = 0; // nonzero: the next fused launch's test wait (above)
     std::vector<std::pair<cudaEvent_t, cudaEvent_t>> fused_marks_;
     std::vector<uint64_t> fused_mark_evals_;
     std::vector<cudaEvent_t> ring_;

@@ -89,3 +89,45 @@ def test_the_stack_cap_is_refused_where_it_does_not_apply(b200):
     assert lib.ob_test_set_walk_stack_cap(direct._handle, 8) == b200.ERROR_UNSUPPORTED
     tree = b200.B200TreeSolver(0.01, 0.5, 32, True)
     assert lib.ob_test_set_walk_stack_cap(tree._handle, 257) == b200.ERROR_INVALID_ARGUMENT
+
+
+def test_a_fused_launch_whose_ready_word_never_comes_times_out(b200):
+    # The fused small-system launch waits for each CTA's ready word; with one
+    # CTA silent and a poll limit of a thousand the waits run out, the step
+    # reports OB_ERROR_TIMEOUT, and the next launch (ready words cleared)
+    # steps exactly as a fresh system does.
+    from orrery_b200 import initial_conditions as ic
+    lib = b200.load_library()
+    lib.ob_test_fused_timeout.argtypes = [C.c_void_p, C.c_uint32]
+    lib.ob_test_fused_timeout.restype = C.c_int
+    d = ic.plummer_sphere(2048, seed=12)
+    keys = ("x", "y", "z", "vx", "vy", "vz", "m")
+
+    def fresh():
+        s = b200.DeviceSystem(2048, 0.01, precision="fp32")
+        assert s.set_fused_steps(True)
+        s.set_state(*(d[k] for k in keys))
+        return s
+
+    s = fresh()
+    assert lib.ob_test_fused_timeout(s._handle, 1000) == b200.OK
+    with pytest.raises(b200.OrreryError) as err:
+        s.step(1e-3, 3, "vv")
+    assert err.value.code == b200.ERROR_TIMEOUT
+    s.set_state(*(d[k] for k in keys))
+    s.step(1e-3, 5, "vv")
+    reference = fresh()
+    reference.step(1e-3, 5, "vv")
+    a, b = s.state(), reference.state()
+    for k in ("x", "y", "z", "vx", "vy", "vz", "ax", "ay", "az"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_the_fused_timeout_entry_checks_its_arguments(b200):
+    lib = b200.load_library()
+    lib.ob_test_fused_timeout.argtypes = [C.c_void_p, C.c_uint32]
+    lib.ob_test_fused_timeout.restype = C.c_int
+    big = b200.DeviceSystem(100_000, 0.01, precision="fp32")
+    assert lib.ob_test_fused_timeout(big._handle, 10) == b200.ERROR_UNSUPPORTED
+    small = b200.DeviceSystem(512, 0.01, precision="fp32")
+    assert lib.ob_test_fused_timeout(small._handle, 0) == b200.ERROR_INVALID_ARGUMENT
