@@ -102,6 +102,33 @@ __device__ __forceinline__ void store_release(unsigned *word, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" : : "l"(word), "r"(v) : "memory");
 }
 
+// Pairs [p0, p1) of the staged sources against the lane's target (offset
+// -t): FP32 terms two sources per packed instruction, added to the slice
+// sums. SKIP_SELF zeroes the target's own term by index.
+template <bool SKIP_SELF>
+__device__ __forceinline__ void pair_slice(const float4 *src, uint32_t p0, uint32_t p1,
+                                           uint32_t i, float2 ntx, float2 nty, float2 ntz,
+                                           float2 e2, float2 &sx, float2 &sy, float2 &sz) {
+#pragma unroll 4
+    for (uint32_t p = p0; p < p1; ++p) {
+        const float4 q0 = src[2u * p], q1 = src[2u * p + 1u];
+        const float2 dx = __fadd2_rn(f2(q0.x, q0.y), ntx);
+        const float2 dy = __fadd2_rn(f2(q0.z, q0.w), nty);
+        const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
+        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, e2)));
+        float inv0 = rsqrt_approx(r2.x), inv1 = rsqrt_approx(r2.y);
+        if (SKIP_SELF) {
+            inv0 = 2u * p == i ? 0.0f : inv0;
+            inv1 = 2u * p + 1u == i ? 0.0f : inv1;
+        }
+        const float2 inv = f2(inv0, inv1);
+        const float2 f = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), __fmul2_rn(inv, inv));
+        sx = __ffma2_rn(f, dx, sx);
+        sy = __ffma2_rn(f, dy, sy);
+        sz = __ffma2_rn(f, dz, sz);
+    }
+}
+
 template <uint32_t WARPS>
 __global__ void __launch_bounds__(WARPS * 32)
     fused_steps_kernel(FusedArgs g) {
@@ -224,23 +251,11 @@ __global__ void __launch_bounds__(WARPS * 32)
         const float2 ntx = f2(-tx, -tx), nty = f2(-ty, -ty), ntz = f2(-tz, -tz);
         float2 sx = f2(0.0f, 0.0f), sy = sx, sz = sx;
         const uint32_t p0 = warp * slice, p1 = p0 + slice;
-#pragma unroll 4
-        for (uint32_t p = p0; p < p1; ++p) {
-            const float4 q0 = src[2u * p], q1 = src[2u * p + 1u];
-            const float2 dx = __fadd2_rn(f2(q0.x, q0.y), ntx);
-            const float2 dy = __fadd2_rn(f2(q0.z, q0.w), nty);
-            const float2 dz = __fadd2_rn(f2(q1.x, q1.y), ntz);
-            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __ffma2_rn(dx, dx, e2)));
-            float inv0 = rsqrt_approx(r2.x), inv1 = rsqrt_approx(r2.y);
-            if (skip_self) {
-                inv0 = 2u * p == i ? 0.0f : inv0;
-                inv1 = 2u * p + 1u == i ? 0.0f : inv1;
-            }
-            const float2 inv = f2(inv0, inv1);
-            const float2 f = __fmul2_rn(__fmul2_rn(f2(q1.z, q1.w), inv), __fmul2_rn(inv, inv));
-            sx = __ffma2_rn(f, dx, sx);
-            sy = __ffma2_rn(f, dy, sy);
-            sz = __ffma2_rn(f, dz, sz);
+        // The warp-uniform choice is made once, outside the pair loop.
+        if (skip_self) {
+            pair_slice<true>(src, p0, p1, i, ntx, nty, ntz, e2, sx, sy, sz);
+        } else {
+            pair_slice<false>(src, p0, p1, i, ntx, nty, ntz, e2, sx, sy, sz);
         }
         partial[warp][0][lane] = static_cast<double>(sx.x) + static_cast<double>(sx.y);
         partial[warp][1][lane] = static_cast<double>(sy.x) + static_cast<double>(sy.y);
