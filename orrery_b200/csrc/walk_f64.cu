@@ -105,16 +105,18 @@ __global__ void __launch_bounds__(kWalk64Threads)
             const double d2 = norm2(ox, oy, oz);
             uint32_t following;
             if (d2 >= cell.r2) {
+                // The monopole and quadrupole terms each take the softened
+                // inverse distance and its square of the same d2 (two calls
+                // in the reference, equal to the last bit): taken once here.
                 const double inv = inverse_distance(d2, eps2);
-                const double factor = __dmul_rn(cell.mass, __dmul_rn(__dmul_rn(inv, inv), inv));
+                const double inv2 = __dmul_rn(inv, inv);
+                const double factor = __dmul_rn(cell.mass, __dmul_rn(inv2, inv));
                 acc_x = __dadd_rn(acc_x, __dmul_rn(ox, factor));
                 acc_y = __dadd_rn(acc_y, __dmul_rn(oy, factor));
                 acc_z = __dadd_rn(acc_z, __dmul_rn(oz, factor));
                 if (quads != nullptr) {
                     const DeviceQuadrupole q = quads[cur];
-                    const double inverse = inverse_distance(d2, eps2);
-                    const double inv2 = __dmul_rn(inverse, inverse);
-                    const double inv5 = __dmul_rn(__dmul_rn(inv2, inv2), inverse);
+                    const double inv5 = __dmul_rn(__dmul_rn(inv2, inv2), inv);
                     const double inv7 = __dmul_rn(inv5, inv2);
                     // Q d with the symmetric tensor's six components.
                     const double cx = dot3(q.xx, q.xy, q.xz, ox, oy, oz);
