@@ -467,6 +467,9 @@ void System::step_async(int integrator, double dt, uint64_t steps) {
     if (fused_for(integrator)) {
         if (fused_buf_.size() == 0) {
             fused_buf_.reserve(fused_scratch_floats4(n_));
+            // The padding past N is copied as it is and never written.
+            check(cudaMemsetAsync(fused_buf_.data(), 0, fused_buf_.bytes(), stream_),
+                  "clearing the fused source buffers");
             fused_ready_.reserve(fused_ready_words(n_));
             fused_ready_reset_ = true;
         }

@@ -15,12 +15,14 @@
 //      closing kick first, as a separate rounding, then this substep's
 //      kick-drift: the same explicitly rounded FP64 operations, in the same
 //      order, as kick_kernel and kick_drift_kernel), writes their FP32
-//      positions and masses into buffer s % 2 and then raises the CTA's
-//      ready word to this substep's number;
-//   B. every warp loads its share of the sources from buffer s % 2 into
-//      shared memory, each 32-source chunk once the ready word of the CTA
-//      that wrote it has reached this substep (no grid-wide barrier: a warp
-//      waits only for the chunks it loads);
+//      positions and masses into buffer s % 2 (already in the pair layout
+//      the pair loop reads) and then raises the CTA's ready word to this
+//      substep's number;
+//   B. every warp copies its share of the sources from buffer s % 2 into
+//      shared memory, each 32-source chunk by one bulk copy once the ready
+//      word of the CTA that wrote it has reached this substep (no grid-wide
+//      barrier: a warp waits only for the chunks it copies; the CTA waits on
+//      an mbarrier for the bytes of all of them);
 //   C. the CTA evaluates its targets' accelerations: FP32 pair arithmetic
 //      two sources per packed FP32x2 instruction, each warp's slice summed
 //      in FP32, the W slices added in FP64 in slice order by warp 0.
@@ -63,7 +65,7 @@ constexpr uint32_t kReadyStride = 32;
 struct FusedArgs {
     double *x, *y, *z, *vx, *vy, *vz, *ax, *ay, *az;
     const double *m;
-    float4 *buf0, *buf1; // FP32 x y z m per particle, double-buffered
+    float4 *buf0, *buf1; // FP32 sources in pairs (x0 x1 y0 y1) (z0 z1 m0 m1), double-buffered
     unsigned *ready;     // per CTA (kReadyStride apart): substeps published, across launches
     unsigned *status;
     uint32_t n, padded;  // padded: a multiple of kFusedGroup
@@ -136,6 +138,7 @@ __global__ void __launch_bounds__(WARPS * 32)
     __shared__ double partial[WARPS][3][kFusedTargets];
     __shared__ double state[9][kFusedTargets]; // x y z vx vy vz ax ay az of the CTA's targets
     __shared__ int stop;
+    __shared__ __align__(8) uint64_t loaded; // the substep's source chunks have landed
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t i = blockIdx.x * kFusedTargets + lane; // this lane's target in every warp
     const bool mine = i < g.n;
@@ -149,6 +152,8 @@ __global__ void __launch_bounds__(WARPS * 32)
     }
     if (threadIdx.x == 0) {
         stop = 0;
+        mbar_init(&loaded, 1);
+        fence_barrier_init();
     }
     __syncthreads();
     const uint32_t blocks = gridDim.x;
@@ -183,9 +188,16 @@ __global__ void __launch_bounds__(WARPS * 32)
                 state[3][lane] = vx;
                 state[4][lane] = vy;
                 state[5][lane] = vz;
-                buf[i] = make_float4(__double2float_rn(x), __double2float_rn(y),
-                                     __double2float_rn(z), mass);
+                // Slot i % 2 of pair i / 2: (x0 x1 y0 y1) (z0 z1 m0 m1), the
+                // layout the pair loop reads, so that chunks copy as they are.
+                float *lo = reinterpret_cast<float *>(&buf[2u * (i >> 1)]) + (i & 1u);
+                float *hi = reinterpret_cast<float *>(&buf[2u * (i >> 1) + 1u]) + (i & 1u);
+                lo[0] = __double2float_rn(x);
+                lo[2] = __double2float_rn(y);
+                hi[0] = __double2float_rn(z);
+                hi[2] = mass;
             }
+            asm volatile("fence.proxy.async.global;" ::: "memory");
             __threadfence();
             __syncwarp();
             if (lane == 0 && blockIdx.x != g.silent_cta) {
@@ -193,14 +205,21 @@ __global__ void __launch_bounds__(WARPS * 32)
             }
         }
         // B. Sources into shared memory, chunk q = sources 32q .. 32q + 31
-        // (zero-mass padding at the origin past N), once the CTA that wrote
-        // each chunk has published it. Warp w loads chunks w, w + W, ...;
-        // lane k polls the ready word of the warp's k-th chunk (at most 32),
-        // and the warp barrier after the poll orders every lane's loads
-        // after the acquiring reads.
+        // (512 bytes; zero-mass padding at the origin past N, zeroed once on
+        // the host and never written), once the CTA that wrote each chunk has
+        // published it. Warp w copies chunks w, w + W, ...: lane k polls the
+        // ready word of the warp's k-th chunk (at most 32) and then starts
+        // its bulk copy, completing on `loaded`, whose byte count thread 0
+        // posts for the substep. A chunk whose wait ran out is copied all
+        // the same, so that the barrier completes and no copy is left in
+        // flight; the substep is then abandoned.
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(&loaded, g.padded * 16u);
+        }
         {
             const uint32_t q = warp + WARPS * lane;
-            const bool polling = q < blocks && q < chunks;
+            const bool copies = q < chunks;
+            const bool polling = copies && q < blocks;
             for (uint32_t polls = 0;; ++polls) {
                 const bool behind =
                     polling && !reached(load_acquire(&g.ready[q * kReadyStride]), target);
@@ -215,19 +234,17 @@ __global__ void __launch_bounds__(WARPS * 32)
                     break;
                 }
             }
-            __syncwarp();
+            if (copies) {
+                // The chunk's generic-proxy writes (acquired above) before
+                // the async-proxy read; this CTA's reads of the previous
+                // substep's sources before the async-proxy write.
+                asm volatile("fence.proxy.async.global;" ::: "memory");
+                fence_proxy_async_shared();
+                bulk_copy_g2s(&src[32u * q], &buf[32u * q], 512u, &loaded);
+            }
         }
-#pragma unroll 4
-        for (uint32_t q = warp; q < chunks; q += WARPS) {
-            const uint32_t j = 32u * q + lane;
-            const float4 a = j < g.n ? __ldcg(&buf[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            // Slot j % 2 of pair j / 2: (x0 x1 y0 y1) (z0 z1 m0 m1).
-            float *lo = reinterpret_cast<float *>(&src[2u * (j >> 1)]) + (j & 1u);
-            float *hi = reinterpret_cast<float *>(&src[2u * (j >> 1) + 1u]) + (j & 1u);
-            lo[0] = a.x;
-            lo[2] = a.y;
-            hi[0] = a.z;
-            hi[2] = a.w;
+        if (!mbar_wait_bounded(&loaded, s & 1u, g.status)) {
+            stop = 1;
         }
         __syncthreads();
         if (stop != 0) {

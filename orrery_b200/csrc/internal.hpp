@@ -42,7 +42,8 @@ cudaError_t launch_direct_f32(const float4 *sources, uint32_t n, uint32_t padded
 // (velocity Verlet: 1, Yoshida-4: 3), state = x y z vx vy vz ax ay az.
 // fused_steps_warps(n) gives the warps per CTA of a grid that is resident at
 // once (32 or 16), or 0 when the system does not fit; the caller passes it to
-// the launch. `scratch` holds fused_scratch_floats4(n) float4; `ready` holds
+// the launch. `scratch` holds fused_scratch_floats4(n) float4, zeroed once
+// (the padding past n is read, never written); `ready` holds
 // fused_ready_words(n) words, zeroed together with the caller's substep count
 // `epoch`, which then grows by steps * cycle per launch. poll_limit (0: the
 // library's limit) and silent_cta (a CTA that never publishes; ~0 for none)
