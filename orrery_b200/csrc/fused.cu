@@ -28,15 +28,15 @@
 //      in FP32, the W slices added in FP64 in slice order by warp 0.
 // Double buffering is safe with per-CTA words: a CTA writes buffer s % 2
 // again only at substep s + 2, after its forces of substep s + 1, which need
-// every CTA's chunk of substep s + 1, which each CTA publishes only after it
-// has finished loading buffer s % 2. After the last substep warp 0 gives the
+// every CTA's chunk of substep s + 1, which each CTA publishes only after its
+// copies of buffer s % 2 have landed. After the last substep warp 0 gives the
 // targets the closing kick and writes their state back.
 //
 // Ready words count substeps across launches (the host passes the count so
 // far, `epoch`, and clears the words together with it); waits are bounded
 // (kSpinLimit polls, or fewer where a test asks, then the timeout bit of the
-// status word, and every CTA stops after the substep it is in), and the launch is cooperative, so every
-// CTA is resident. The pair arithmetic is that of the FP32 direct kernel
+// status word, and every CTA stops after the substep it is in), and the
+// launch is cooperative, so every CTA is resident. The pair arithmetic is that of the FP32 direct kernel
 // (positions rounded to FP32, softened, FP32 sums per slice, FP64 across
 // slices); with softening the target's own entry adds exactly zero unless
 // m / eps^3 of the target overflows FP32, in which case the warp skips it
