@@ -89,6 +89,22 @@ def test_fused_steps_split_across_calls_equal_one_call(b200):
     assert all(np.array_equal(sa[k], sb[k]) for k in KEYS)
 
 
+def test_fused_host_steps_equal_resident_steps(b200):
+    # Integrator::step over host arrays (upload, one fused launch, download)
+    # is the resident fused step, bit for bit.
+    d = _plummer(2048, seed=9)
+    a, on_a = _system(b200, d)
+    b, on_b = _system(b200, d)
+    assert on_a and on_b
+    a.step(1e-3, 3, "vv")
+    host = b.state()
+    host["m"] = np.ascontiguousarray(d["m"], dtype=np.float64)
+    for _ in range(3):
+        b.step_host(host, 1e-3, 1, "vv")
+    sa = a.state()
+    assert all(np.array_equal(sa[k], host[k]) for k in KEYS)
+
+
 def test_a_heavy_target_skips_itself(b200, restatement):
     # m / eps^3 above the FP32 range (1e30 / 1e-9): the target's own entry
     # must be skipped by index (0 * inf would otherwise poison its sum); its
